@@ -1,0 +1,65 @@
+// arc_kernels.cuh - launchers of every kernel of the library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include "arc_device.cuh"
+
+namespace arc {
+
+// FP64 data of the reset path (csrc/arc_sim.c:88-110, csrc/arc_phys.c:749-782):
+// forward-kinematics frames, default stance, limits.
+struct ResetModel {
+    int nb, nj, ns;
+    int parent[kMaxJoints], child[kMaxJoints];
+    V3<double> r1[kMaxJoints], r2[kMaxJoints], a1[kMaxJoints];
+    Q4<double> q_rel0[kMaxJoints];
+    double default_angles[kMaxJoints], lo[kMaxJoints], hi[kMaxJoints];
+    double stand_height, footprint;
+};
+
+// ----- stepping
+template <class R>
+cudaError_t launch_step_plain(const DevModel<R>& M, const Worlds<R>& W, const Actuation& A, const int* ids,
+                              int n_ids, cudaStream_t stream);
+
+// Leg-parallel step: four lanes per world, state staged in shared memory.
+// worlds_per_cta is a multiple of 8 (one warp steps eight worlds).
+// spill: per world and lane, spill_per_lane contact records of 8 R beyond
+// the on-chip ones; lane_cap bounds the contacts one lane can record.
+template <class R>
+cudaError_t launch_step_fast(const DevModel<R>& M, const Worlds<R>& W, const Actuation& A, R* spill,
+                             int spill_per_lane, int lane_cap, int worlds_per_cta, cudaStream_t stream);
+
+template <class R> size_t fast_smem_bytes(int stride, int worlds_per_cta);
+constexpr int kFastOnChipContacts = 4;
+
+// ----- outputs of the reference ABI (double precision, any pointer may be null)
+template <class R>
+cudaError_t launch_observe(const DevModel<R>& M, const Worlds<R>& W, double* root, double* rot, double* joints,
+                           double* contacts, int* flags, cudaStream_t stream);
+template <class R>
+cudaError_t launch_heights(const Worlds<R>& W, const double* offsets, int k, double* out, cudaStream_t stream);
+template <class R>
+cudaError_t launch_terrain_at(const Worlds<R>& W, const int* ids, const double* xy, int m, double* out,
+                              cudaStream_t stream);
+
+// ----- snapshots: nb*13 + ns*8 + nj*4 + 2 doubles per world
+template <class R>
+cudaError_t launch_get_state(const DevModel<R>& M, const Worlds<R>& W, const int* ids, int n_ids, double* out,
+                             cudaStream_t stream);
+template <class R>
+cudaError_t launch_set_state(const DevModel<R>& M, const Worlds<R>& W, const int* ids, int n_ids, const double* in,
+                             cudaStream_t stream);
+
+// ----- resets (FP64): seeded terrain + noisy stance (csrc/arc_sim.c:88-121)
+template <class R>
+cudaError_t launch_reset(const ResetModel& RM, const Worlds<R>& W, TerrainGeom<R>* tg, TerrainGeomD* tgd,
+                         const int* ids, int n_ids, const unsigned* seeds, const double* difficulty,
+                         const int* grid_of, double cell, cudaStream_t stream);
+
+// Writes one world's terrain from FP64 heights already on the device.
+template <class R>
+cudaError_t launch_set_terrain(const Worlds<R>& W, TerrainGeom<R>* tg, TerrainGeomD* tgd, int id, int nx, int ny,
+                               double cell, double outside, const double* heights, cudaStream_t stream);
+
+}  // namespace arc

@@ -1,0 +1,859 @@
+// arc_sim.cu - host runtime behind the C ABI of include/arc_sim.h.
+//
+// An arc_sim owns one CUDA stream and all device memory of its worlds
+// (layout in arc_device.cuh). The reference-compatible calls stage the
+// caller's host buffers through device buffers and synchronise before
+// returning, like the reference's synchronous OpenMP calls
+// (csrc/arc_sim.c:112-215). Errors never cross the ABI as exceptions: the
+// void calls record them (arc_sim_last_error) and print them once to stderr.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "arc_model.h"
+#include "../../include/arc_sim.h"
+
+using namespace arc;
+
+struct arc_model {
+    ModelHost m;
+};
+
+namespace {
+
+struct DevBuffer {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+}  // namespace
+
+struct arc_sim {
+    int n = 0, substeps = 0, grid = 0, threads = 1;
+    double dt = 0.0, cell = 0.0;
+    bool fp64 = false;
+    int kernel = ARC_KERNEL_LEGS, wpc = 16;
+    ModelHost model;
+    DevModel<float> mf;
+    DevModel<double> md;
+    ResetModel rm;
+    cudaStream_t stream = nullptr;
+    // device state
+    void* rec = nullptr;
+    int stride = 0, off_sphere = 0, off_joint = 0;
+    uint32_t* sph = nullptr;
+    int* unstable = nullptr;
+    double* time = nullptr;
+    void* th = nullptr;
+    long long* toff = nullptr;
+    void* tg = nullptr;
+    TerrainGeomD* tgd = nullptr;
+    int* grid_of = nullptr;
+    void* spill = nullptr;
+    int spill_per_lane = 0, lane_cap = 0;
+    double spill_cell = 0.0;
+    // staging
+    DevBuffer st_in, st_in2, st_in3, st_out;
+    std::vector<double> host_tmp;
+    arc_world* hworld = nullptr;
+    mutable int err = 0;
+    mutable std::string msg;
+    mutable bool reported = false;
+};
+
+namespace {
+
+int real_size(const arc_sim* s) { return s->fp64 ? 8 : 4; }
+
+int fail(const arc_sim* s, int code, const std::string& what)
+{
+    s->err = code;
+    s->msg = what;
+    if (!s->reported) {
+        std::fprintf(stderr, "arcsim: %s\n", what.c_str());
+        s->reported = true;
+    }
+    return code;
+}
+
+int check(const arc_sim* s, cudaError_t e, const char* where)
+{
+    if (e == cudaSuccess)
+        return ARC_OK;
+    return fail(s, ARC_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+void* grow(const arc_sim* sc, DevBuffer& b, size_t bytes)
+{
+    arc_sim* s = const_cast<arc_sim*>(sc);
+    if (bytes <= b.cap && b.p)
+        return b.p;
+    if (b.p)
+        cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t cap = std::max<size_t>(bytes, 256);
+    if (check(s, cudaMalloc(&b.p, cap), "cudaMalloc(staging)") != ARC_OK)
+        return nullptr;
+    b.cap = cap;
+    return b.p;
+}
+
+template <class R> Worlds<R> view(const arc_sim* s)
+{
+    Worlds<R> w;
+    w.rec = static_cast<R*>(s->rec);
+    w.stride = s->stride;
+    w.off_sphere = s->off_sphere;
+    w.off_joint = s->off_joint;
+    w.sph = s->sph;
+    w.unstable = s->unstable;
+    w.time = s->time;
+    w.th = static_cast<R*>(s->th);
+    w.toff = s->toff;
+    w.tg = static_cast<const TerrainGeom<R>*>(s->tg);
+    w.tgd = s->tgd;
+    w.n = s->n;
+    return w;
+}
+
+void rebuild_models(arc_sim* s)
+{
+    s->model.leaper = is_leaper_topology(s->model);
+    s->mf = make_dev_model<float>(s->model, s->dt, s->substeps, 0.6);
+    s->md = make_dev_model<double>(s->model, s->dt, s->substeps, 0.6);
+    s->rm = make_reset_model(s->model);
+}
+
+// Upper bound of the contacts one lane of the leg-parallel kernel records in
+// a substep: a sphere of radius r touches at most (floor(2r/cell)+2)^2
+// columns, one contact each.
+int lane_contact_bound(const ModelHost& m, double cell)
+{
+    if (!m.leaper)
+        return 0;
+    int worst = 0;
+    for (int leg = 0; leg < kNumLegs; ++leg) {
+        long long sum = 0;
+        for (int it = 0; it < 6; ++it) {
+            int s = it == 0 ? (leg == 0 ? 0 : -1) : 5 * leg + it;
+            if (s < 0)
+                continue;
+            long long per = (long long)std::floor(2.0 * m.s[s].radius / cell) + 2;
+            sum += per * per;
+        }
+        worst = (int)std::max<long long>(worst, std::min<long long>(sum, kMaxContacts));
+    }
+    return worst;
+}
+
+int ensure_spill(arc_sim* s, double cell)
+{
+    if (s->spill && cell >= s->spill_cell)
+        return ARC_OK;
+    const int cap = lane_contact_bound(s->model, cell);
+    const int per = std::max(cap - kFastOnChipContacts, 1);
+    const size_t bytes = (size_t)std::max(s->n, 1) * 4 * per * 8 * real_size(s);
+    void* p = nullptr;
+    if (check(s, cudaMalloc(&p, bytes), "cudaMalloc(contact spill)") != ARC_OK)
+        return ARC_ERR_CUDA;
+    if (s->spill)
+        cudaFree(s->spill);
+    s->spill = p;
+    s->spill_per_lane = per;
+    s->lane_cap = std::max(cap, 0);
+    s->spill_cell = cell;
+    return ARC_OK;
+}
+
+template <class R> void template_record(const arc_sim* s, std::vector<R>& rec)
+{
+    const ModelHost& m = s->model;
+    rec.assign(s->stride, R(0));
+    for (int b = 0; b < m.nb; ++b) {
+        R* r = rec.data() + b * kBodyRec;
+        r[0] = (R)m.b[b].x.x; r[1] = (R)m.b[b].x.y; r[2] = (R)m.b[b].x.z;
+        r[3] = (R)m.b[b].q.w; r[4] = (R)m.b[b].q.x; r[5] = (R)m.b[b].q.y; r[6] = (R)m.b[b].q.z;
+    }
+    for (int j = 0; j < m.nj; ++j) {
+        R* r = rec.data() + s->off_joint + j * kJointRec;
+        r[0] = (R)m.default_angles[j];  // the template's pose sets targets and angles
+        r[1] = (R)m.default_angles[j];
+    }
+}
+
+template <class R> int init_worlds(arc_sim* s)
+{
+    const int n = s->n, g = s->grid;
+    std::vector<R> one;
+    template_record<R>(s, one);
+    std::vector<R> all((size_t)n * s->stride);
+    for (int i = 0; i < n; ++i)
+        std::memcpy(all.data() + (size_t)i * s->stride, one.data(), sizeof(R) * s->stride);
+    if (check(s, cudaMemcpy(s->rec, all.data(), sizeof(R) * all.size(), cudaMemcpyHostToDevice), "init records"))
+        return ARC_ERR_CUDA;
+    // flat terrain, outside at the same height (csrc/arc_sim.c:37: template terrain)
+    std::vector<long long> toff(n);
+    std::vector<TerrainGeom<R>> tg(n);
+    std::vector<TerrainGeomD> tgd(n);
+    std::vector<int> grid_of(n, g);
+    TerrainGeomD gd{g, g, s->cell, -0.5 * g * s->cell, -0.5 * g * s->cell, 0.0};
+    for (int i = 0; i < n; ++i) {
+        toff[i] = (long long)i * kGridMax * kGridMax;
+        tgd[i] = gd;
+        tg[i] = TerrainGeom<R>{g, g, (R)gd.cell, (R)gd.ox, (R)gd.oy, (R)gd.outside};
+    }
+    int rc = ARC_OK;
+    rc |= check(s, cudaMemcpy(s->toff, toff.data(), sizeof(long long) * n, cudaMemcpyHostToDevice), "init toff");
+    rc |= check(s, cudaMemcpy(s->tg, tg.data(), sizeof(TerrainGeom<R>) * n, cudaMemcpyHostToDevice), "init tg");
+    rc |= check(s, cudaMemcpy(s->tgd, tgd.data(), sizeof(TerrainGeomD) * n, cudaMemcpyHostToDevice), "init tgd");
+    rc |= check(s, cudaMemcpy(s->grid_of, grid_of.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "init grid");
+    rc |= check(s, cudaMemset(s->th, 0, sizeof(R) * (size_t)n * kGridMax * kGridMax), "init terrain");
+    rc |= check(s, cudaMemset(s->sph, 0, sizeof(uint32_t) * (size_t)n * std::max(s->model.ns, 1)), "init spheres");
+    rc |= check(s, cudaMemset(s->unstable, 0, sizeof(int) * n), "init flags");
+    rc |= check(s, cudaMemset(s->time, 0, sizeof(double) * n), "init time");
+    return rc ? ARC_ERR_CUDA : ARC_OK;
+}
+
+void free_all(arc_sim* s)
+{
+    void* ps[] = {s->rec, s->sph, s->unstable, s->time, s->th, s->toff, s->tg, s->tgd, s->grid_of, s->spill,
+                  s->st_in.p, s->st_in2.p, s->st_in3.p, s->st_out.p};
+    for (void* p : ps)
+        if (p)
+            cudaFree(p);
+    if (s->stream)
+        cudaStreamDestroy(s->stream);
+    delete s->hworld;
+}
+
+arc_sim* create_with_model(const ModelHost& model, int n, double dt, int substeps, int grid, double cell,
+                           unsigned flags)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        std::fprintf(stderr, "arcsim: no CUDA device available\n");
+        return nullptr;
+    }
+    if (n < 0 || substeps <= 0 || !(cell > 0.0))
+        return nullptr;
+    arc_sim* s = new arc_sim();
+    s->n = n;
+    s->dt = dt;
+    s->substeps = substeps;
+    s->grid = std::max(1, std::min(grid, kGridMax));
+    s->cell = cell;
+    s->fp64 = (flags & ARC_SIM_FP64) != 0;
+    s->model = model;
+    rebuild_models(s);
+    s->kernel = (flags & ARC_SIM_PLAIN) || !s->model.leaper ? ARC_KERNEL_PLAIN : ARC_KERNEL_LEGS;
+    const int rs = real_size(s);
+    s->off_sphere = s->model.nb * kBodyRec;
+    s->off_joint = s->off_sphere + s->model.ns * kSphereRec;
+    const int per16 = 16 / rs;
+    s->stride = (s->off_joint + s->model.nj * kJointRec + per16 - 1) / per16 * per16;
+    const size_t nn = (size_t)std::max(n, 1);
+    bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && cudaMalloc(&s->rec, nn * s->stride * rs) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&s->sph, nn * std::max(s->model.ns, 1) * sizeof(uint32_t)) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&s->unstable, nn * sizeof(int)) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&s->time, nn * sizeof(double)) == cudaSuccess;
+    ok = ok && cudaMalloc(&s->th, nn * kGridMax * kGridMax * rs) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&s->toff, nn * sizeof(long long)) == cudaSuccess;
+    ok = ok && cudaMalloc(&s->tg, nn * (s->fp64 ? sizeof(TerrainGeom<double>) : sizeof(TerrainGeom<float>))) ==
+                   cudaSuccess;
+    ok = ok && cudaMalloc((void**)&s->tgd, nn * sizeof(TerrainGeomD)) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&s->grid_of, nn * sizeof(int)) == cudaSuccess;
+    ok = ok && ensure_spill(s, cell) == ARC_OK;
+    if (ok && n > 0)
+        ok = (s->fp64 ? init_worlds<double>(s) : init_worlds<float>(s)) == ARC_OK;
+    if (!ok) {
+        std::fprintf(stderr, "arcsim: device allocation or initialisation failed for %d worlds\n", n);
+        free_all(s);
+        delete s;
+        cudaGetLastError();
+        return nullptr;
+    }
+    return s;
+}
+
+bool ids_ok(const arc_sim* s, const int* ids, int n_ids)
+{
+    for (int k = 0; k < n_ids; ++k)
+        if (ids[k] < 0 || ids[k] >= s->n)
+            return false;
+    return true;
+}
+
+int sync(const arc_sim* s, const char* where) { return check(s, cudaStreamSynchronize(s->stream), where); }
+
+template <class R> const DevModel<R>& dev_model(const arc_sim* s);
+template <> const DevModel<float>& dev_model<float>(const arc_sim* s) { return s->mf; }
+template <> const DevModel<double>& dev_model<double>(const arc_sim* s) { return s->md; }
+
+template <class R> int step_impl(arc_sim* s, const Actuation& A, cudaStream_t st)
+{
+    const Worlds<R> W = view<R>(s);
+    const DevModel<R>& M = dev_model<R>(s);
+    cudaError_t e;
+    if (s->kernel == ARC_KERNEL_LEGS && M.leaper)
+        e = launch_step_fast<R>(M, W, A, static_cast<R*>(s->spill), s->spill_per_lane, s->lane_cap, s->wpc, st);
+    else
+        e = launch_step_plain<R>(M, W, A, nullptr, s->n, st);
+    return check(s, e, "step kernel");
+}
+
+int step_any(arc_sim* s, const Actuation& A, cudaStream_t st)
+{
+    return s->fp64 ? step_impl<double>(s, A, st) : step_impl<float>(s, A, st);
+}
+
+cudaStream_t stream_of(const arc_sim* s, void* stream) { return stream ? (cudaStream_t)stream : s->stream; }
+
+}  // namespace
+
+// ============================================================================
+// Part 1: the reference API
+
+extern "C" {
+
+arc_sim* arc_sim_create(int n_worlds, double dt, int substeps, int grid, double cell)
+{
+    return arc_sim_create_ex(n_worlds, dt, substeps, grid, cell, 0u);
+}
+
+arc_sim* arc_sim_create_ex(int n_worlds, double dt, int substeps, int grid, double cell, unsigned flags)
+{
+    ModelHost m;
+    build_leaper(m);
+    return create_with_model(m, n_worlds, dt, substeps, grid, cell, flags);
+}
+
+void arc_sim_destroy(arc_sim* s)
+{
+    if (!s)
+        return;
+    if (s->stream)
+        cudaStreamSynchronize(s->stream);
+    free_all(s);
+    delete s;
+}
+
+void arc_sim_set_threads(arc_sim* s, int threads) { s->threads = threads > 0 ? threads : 1; }
+int arc_sim_num_worlds(const arc_sim* s) { return s->n; }
+int arc_sim_num_joints(void) { return kNumJoints; }
+int arc_sim_num_legs(void) { return kNumLegs; }
+
+void arc_sim_robot_info(const arc_sim* s, double* default_angles, double* lo, double* hi, double* misc)
+{
+    const ModelHost& m = s->model;
+    for (int i = 0; i < kNumJoints && i < m.nj; ++i) {
+        if (default_angles)
+            default_angles[i] = m.default_angles[i];
+        if (lo)
+            lo[i] = m.j[i].lo;
+        if (hi)
+            hi[i] = m.j[i].hi;
+    }
+    if (misc) {
+        misc[0] = m.stand_height;
+        misc[1] = m.total_mass;
+    }
+}
+
+void arc_sim_reset(arc_sim* s, const int* ids, int n_ids, const unsigned int* seeds, const double* difficulty)
+{
+    if (n_ids <= 0)
+        return;
+    if (!ids_ok(s, ids, n_ids)) {
+        fail(s, ARC_ERR_ARG, "arc_sim_reset: world index out of range");
+        return;
+    }
+    // one staging block: difficulty (8-byte aligned) first, then ids and seeds
+    char* buf = (char*)grow(s, s->st_in, (size_t)n_ids * (sizeof(double) + sizeof(int) + sizeof(unsigned)));
+    if (!buf)
+        return;
+    double* d_diff = (double*)buf;
+    int* d_ids = (int*)(buf + (size_t)n_ids * sizeof(double));
+    unsigned* d_seeds = (unsigned*)(buf + (size_t)n_ids * (sizeof(double) + sizeof(int)));
+    cudaStream_t st = s->stream;
+    if (check(s, cudaMemcpyAsync(d_ids, ids, sizeof(int) * n_ids, cudaMemcpyHostToDevice, st), "reset ids") ||
+        check(s, cudaMemcpyAsync(d_seeds, seeds, sizeof(unsigned) * n_ids, cudaMemcpyHostToDevice, st), "seeds") ||
+        check(s, cudaMemcpyAsync(d_diff, difficulty, sizeof(double) * n_ids, cudaMemcpyHostToDevice, st), "diff"))
+        return;
+    cudaError_t e;
+    if (s->fp64)
+        e = launch_reset<double>(s->rm, view<double>(s), (TerrainGeom<double>*)s->tg, s->tgd, d_ids, n_ids, d_seeds,
+                                 d_diff, s->grid_of, s->cell, st);
+    else
+        e = launch_reset<float>(s->rm, view<float>(s), (TerrainGeom<float>*)s->tg, s->tgd, d_ids, n_ids, d_seeds,
+                                d_diff, s->grid_of, s->cell, st);
+    if (check(s, e, "reset kernel"))
+        return;
+    sync(s, "arc_sim_reset");
+}
+
+void arc_sim_step(arc_sim* s, const double* targets)
+{
+    if (s->n <= 0)
+        return;
+    const size_t bytes = sizeof(double) * (size_t)s->n * kNumJoints;
+    double* d = (double*)grow(s, s->st_in2, bytes);
+    if (!d)
+        return;
+    if (check(s, cudaMemcpyAsync(d, targets, bytes, cudaMemcpyHostToDevice, s->stream), "step targets"))
+        return;
+    Actuation A{d, nullptr};
+    if (step_any(s, A, s->stream))
+        return;
+    sync(s, "arc_sim_step");
+}
+
+void arc_sim_observe(const arc_sim* s, double* root, double* rot, double* joints, double* contacts, int* flags)
+{
+    if (s->n <= 0)
+        return;
+    const size_t n = (size_t)s->n;
+    const int nch = s->model.n_channels;
+    const size_t sizes[5] = {n * 13, n * 9, n * 3 * s->model.nj, n * nch, n};
+    double* outs[4] = {root, rot, joints, contacts};
+    size_t total = sizes[0] + sizes[1] + sizes[2] + sizes[3] + sizes[4];
+    double* d = (double*)grow(s, const_cast<arc_sim*>(s)->st_out, total * sizeof(double));
+    if (!d)
+        return;
+    double* dr = d;
+    double* drot = dr + sizes[0];
+    double* dj = drot + sizes[1];
+    double* dc = dj + sizes[2];
+    int* df = (int*)(dc + sizes[3]);
+    cudaError_t e;
+    if (s->fp64)
+        e = launch_observe<double>(s->md, view<double>(s), root ? dr : nullptr, rot ? drot : nullptr,
+                                   joints ? dj : nullptr, contacts ? dc : nullptr, flags ? df : nullptr, s->stream);
+    else
+        e = launch_observe<float>(s->mf, view<float>(s), root ? dr : nullptr, rot ? drot : nullptr,
+                                  joints ? dj : nullptr, contacts ? dc : nullptr, flags ? df : nullptr, s->stream);
+    if (check(s, e, "observe kernel"))
+        return;
+    double* devs[4] = {dr, drot, dj, dc};
+    for (int k = 0; k < 4; ++k)
+        if (outs[k] &&
+            check(s, cudaMemcpyAsync(outs[k], devs[k], sizes[k] * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
+                  "observe copy"))
+            return;
+    if (flags && check(s, cudaMemcpyAsync(flags, df, n * sizeof(int), cudaMemcpyDeviceToHost, s->stream), "flags"))
+        return;
+    sync(s, "arc_sim_observe");
+}
+
+void arc_sim_heights(const arc_sim* s, const double* offsets, int k, double* out)
+{
+    if (s->n <= 0 || k <= 0)
+        return;
+    arc_sim* m = const_cast<arc_sim*>(s);
+    double* doff = (double*)grow(s, m->st_in3, sizeof(double) * 2 * k);
+    double* dout = (double*)grow(s, m->st_out, sizeof(double) * (size_t)s->n * k);
+    if (!doff || !dout)
+        return;
+    if (check(s, cudaMemcpyAsync(doff, offsets, sizeof(double) * 2 * k, cudaMemcpyHostToDevice, s->stream), "offs"))
+        return;
+    cudaError_t e = s->fp64 ? launch_heights<double>(view<double>(s), doff, k, dout, s->stream)
+                            : launch_heights<float>(view<float>(s), doff, k, dout, s->stream);
+    if (check(s, e, "heights kernel"))
+        return;
+    if (check(s, cudaMemcpyAsync(out, dout, sizeof(double) * (size_t)s->n * k, cudaMemcpyDeviceToHost, s->stream),
+              "heights copy"))
+        return;
+    sync(s, "arc_sim_heights");
+}
+
+void arc_sim_terrain_at(const arc_sim* s, const int* ids, const double* xy, int m, double* out)
+{
+    if (m <= 0)
+        return;
+    if (!ids_ok(s, ids, m)) {
+        fail(s, ARC_ERR_ARG, "arc_sim_terrain_at: world index out of range");
+        return;
+    }
+    arc_sim* ms = const_cast<arc_sim*>(s);
+    char* buf = (char*)grow(s, ms->st_in3, (size_t)m * (sizeof(int) + 3 * sizeof(double)) + 64);
+    if (!buf)
+        return;
+    double* dxy = (double*)buf;
+    double* dout = dxy + 2 * (size_t)m;
+    int* dids = (int*)(dout + m);
+    if (check(s, cudaMemcpyAsync(dids, ids, sizeof(int) * m, cudaMemcpyHostToDevice, s->stream), "ids") ||
+        check(s, cudaMemcpyAsync(dxy, xy, sizeof(double) * 2 * m, cudaMemcpyHostToDevice, s->stream), "xy"))
+        return;
+    cudaError_t e = s->fp64 ? launch_terrain_at<double>(view<double>(s), dids, dxy, m, dout, s->stream)
+                            : launch_terrain_at<float>(view<float>(s), dids, dxy, m, dout, s->stream);
+    if (check(s, e, "terrain_at kernel"))
+        return;
+    if (check(s, cudaMemcpyAsync(out, dout, sizeof(double) * m, cudaMemcpyDeviceToHost, s->stream), "out"))
+        return;
+    sync(s, "arc_sim_terrain_at");
+}
+
+const arc_world* arc_sim_world(const arc_sim* s, int i)
+{
+    if (i < 0 || i >= s->n) {
+        fail(s, ARC_ERR_ARG, "arc_sim_world: world index out of range");
+        return nullptr;
+    }
+    arc_sim* ms = const_cast<arc_sim*>(s);
+    if (!ms->hworld)
+        ms->hworld = new arc_world();
+    arc_world* w = ms->hworld;
+    std::memset(w, 0, sizeof(*w));
+    const ModelHost& m = s->model;
+    std::vector<double> st(arc_sim_state_size(s));
+    if (arc_sim_get_state(s, &i, 1, st.data()) != ARC_OK)
+        return nullptr;
+    int nxy[2];
+    double geom[4];
+    std::vector<double> h(kGridMax * kGridMax);
+    if (arc_sim_get_terrain(s, i, nxy, geom, h.data()) != ARC_OK)
+        return nullptr;
+    w->gravity = arcw_vec3{m.gravity.x, m.gravity.y, m.gravity.z};
+    w->mu_static = m.mu_s;
+    w->mu_dynamic = m.mu_d;
+    w->n_bodies = m.nb;
+    w->n_joints = m.nj;
+    w->n_spheres = m.ns;
+    const double* p = st.data();
+    for (int b = 0; b < m.nb; ++b, p += 13) {
+        arcw_body& o = w->bodies[b];
+        o.x = o.x_prev = arcw_vec3{p[0], p[1], p[2]};
+        o.q = o.q_prev = arcw_quat{p[3], p[4], p[5], p[6]};
+        o.v = arcw_vec3{p[7], p[8], p[9]};
+        o.w = arcw_vec3{p[10], p[11], p[12]};
+        o.mass = m.b[b].mass;
+        o.inv_mass = m.b[b].inv_mass;
+        o.inertia = arcw_vec3{m.b[b].inertia.x, m.b[b].inertia.y, m.b[b].inertia.z};
+        o.inv_inertia = arcw_vec3{m.b[b].inv_inertia.x, m.b[b].inv_inertia.y, m.b[b].inv_inertia.z};
+        Pose<double> P;
+        P.q = Q4<double>{p[3], p[4], p[5], p[6]};
+        BodyK<double> k{m.b[b].inv_mass, m.b[b].inertia, m.b[b].inv_inertia,
+                        m.b[b].inertia.x == m.b[b].inertia.y && m.b[b].inertia.y == m.b[b].inertia.z};
+        body_sync(P, k);
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 3; ++c)
+                o.rot.m[a][c] = P.rot.m[a][c];
+        double iw[3][3] = {{P.iiw.xx, P.iiw.xy, P.iiw.xz}, {P.iiw.xy, P.iiw.yy, P.iiw.yz},
+                           {P.iiw.xz, P.iiw.yz, P.iiw.zz}};
+        std::memcpy(o.inv_iw.m, iw, sizeof(iw));
+    }
+    for (int sidx = 0; sidx < m.ns; ++sidx, p += 8) {
+        arcw_sphere& o = w->spheres[sidx];
+        o.body = m.s[sidx].body;
+        o.pos = arcw_vec3{m.s[sidx].pos.x, m.s[sidx].pos.y, m.s[sidx].pos.z};
+        o.radius = m.s[sidx].radius;
+        o.anchored = p[0] != 0.0;
+        o.anchor = arcw_vec3{p[1], p[2], p[3]};
+        o.anchor_n = arcw_vec3{p[4], p[5], p[6]};
+        o.touch = (int)p[7];
+    }
+    for (int j = 0; j < m.nj; ++j, p += 4) {
+        arcw_joint& o = w->joints[j];
+        const ModelHost::Joint& t = m.j[j];
+        o.parent = t.parent;
+        o.child = t.child;
+        o.r1 = arcw_vec3{t.r1.x, t.r1.y, t.r1.z};
+        o.r2 = arcw_vec3{t.r2.x, t.r2.y, t.r2.z};
+        o.a1 = arcw_vec3{t.a1.x, t.a1.y, t.a1.z};
+        o.a2 = arcw_vec3{t.a2.x, t.a2.y, t.a2.z};
+        o.b1 = arcw_vec3{t.b1.x, t.b1.y, t.b1.z};
+        o.b2 = arcw_vec3{t.b2.x, t.b2.y, t.b2.z};
+        o.q_rel0 = arcw_quat{t.q_rel0.w, t.q_rel0.x, t.q_rel0.y, t.q_rel0.z};
+        o.lo = t.lo;
+        o.hi = t.hi;
+        o.kp = t.kp;
+        o.kd = t.kd;
+        o.max_torque = t.max_torque;
+        o.target = p[0];
+        o.angle = p[1];
+        o.rate = p[2];
+        o.torque = p[3];
+        o.lim[0] = std::cos(t.lo);
+        o.lim[1] = std::sin(t.lo);
+        o.lim[2] = std::cos(t.hi);
+        o.lim[3] = std::sin(t.hi);
+    }
+    w->unstable = p[0] != 0.0;
+    w->time = p[1];
+    w->terrain.nx = nxy[0];
+    w->terrain.ny = nxy[1];
+    w->terrain.cell = geom[0];
+    w->terrain.ox = geom[1];
+    w->terrain.oy = geom[2];
+    w->terrain.outside = geom[3];
+    std::memcpy(w->terrain.h, h.data(), sizeof(double) * nxy[0] * nxy[1]);
+    return w;
+}
+
+// ============================================================================
+// Part 2: additive API
+
+int arc_sim_last_error(const arc_sim* s) { return s ? s->err : ARC_ERR_ARG; }
+const char* arc_sim_error_message(const arc_sim* s) { return s ? s->msg.c_str() : "null sim"; }
+
+int arc_sim_set_kernel(arc_sim* s, int kernel, int worlds_per_cta)
+{
+    if (kernel == ARC_KERNEL_LEGS) {
+        if (!s->model.leaper)
+            return fail(s, ARC_ERR_UNSUPPORTED, "leg-parallel kernel needs the quadruped's topology");
+        if (worlds_per_cta != 8 && worlds_per_cta != 16 && worlds_per_cta != 32 && worlds_per_cta != 64)
+            return fail(s, ARC_ERR_ARG, "worlds_per_cta must be 8, 16, 32 or 64");
+        const size_t smem = s->fp64 ? fast_smem_bytes<double>(s->stride, worlds_per_cta)
+                                    : fast_smem_bytes<float>(s->stride, worlds_per_cta);
+        if (smem > 227 * 1024)
+            return fail(s, ARC_ERR_UNSUPPORTED, "worlds_per_cta needs more than 227 KB of shared memory");
+        s->wpc = worlds_per_cta;
+    } else if (kernel != ARC_KERNEL_PLAIN) {
+        return fail(s, ARC_ERR_ARG, "unknown kernel");
+    }
+    s->kernel = kernel;
+    return ARC_OK;
+}
+
+int arc_sim_get_kernel(const arc_sim* s, int* kernel, int* worlds_per_cta)
+{
+    if (kernel)
+        *kernel = s->kernel;
+    if (worlds_per_cta)
+        *worlds_per_cta = s->wpc;
+    return ARC_OK;
+}
+
+int arc_sim_real_size(const arc_sim* s) { return real_size(s); }
+
+int arc_sim_state_size(const arc_sim* s)
+{
+    return s->model.nb * 13 + s->model.ns * 8 + s->model.nj * 4 + 2;
+}
+
+int arc_sim_get_state(const arc_sim* s, const int* ids, int n_ids, double* out)
+{
+    if (n_ids <= 0)
+        return ARC_OK;
+    if (!ids_ok(s, ids, n_ids))
+        return fail(s, ARC_ERR_ARG, "arc_sim_get_state: world index out of range");
+    arc_sim* m = const_cast<arc_sim*>(s);
+    const size_t ss = arc_sim_state_size(s);
+    int* dids = (int*)grow(s, m->st_in3, sizeof(int) * n_ids);
+    double* dout = (double*)grow(s, m->st_out, sizeof(double) * ss * n_ids);
+    if (!dids || !dout)
+        return ARC_ERR_CUDA;
+    if (check(s, cudaMemcpyAsync(dids, ids, sizeof(int) * n_ids, cudaMemcpyHostToDevice, s->stream), "ids"))
+        return ARC_ERR_CUDA;
+    cudaError_t e = s->fp64 ? launch_get_state<double>(s->md, view<double>(s), dids, n_ids, dout, s->stream)
+                            : launch_get_state<float>(s->mf, view<float>(s), dids, n_ids, dout, s->stream);
+    if (check(s, e, "get_state kernel") ||
+        check(s, cudaMemcpyAsync(out, dout, sizeof(double) * ss * n_ids, cudaMemcpyDeviceToHost, s->stream), "copy"))
+        return ARC_ERR_CUDA;
+    return sync(s, "arc_sim_get_state");
+}
+
+int arc_sim_set_state(arc_sim* s, const int* ids, int n_ids, const double* in)
+{
+    if (n_ids <= 0)
+        return ARC_OK;
+    if (!ids_ok(s, ids, n_ids))
+        return fail(s, ARC_ERR_ARG, "arc_sim_set_state: world index out of range");
+    const size_t ss = arc_sim_state_size(s);
+    int* dids = (int*)grow(s, s->st_in3, sizeof(int) * n_ids);
+    double* din = (double*)grow(s, s->st_in, sizeof(double) * ss * n_ids);
+    if (!dids || !din)
+        return ARC_ERR_CUDA;
+    if (check(s, cudaMemcpyAsync(dids, ids, sizeof(int) * n_ids, cudaMemcpyHostToDevice, s->stream), "ids") ||
+        check(s, cudaMemcpyAsync(din, in, sizeof(double) * ss * n_ids, cudaMemcpyHostToDevice, s->stream), "in"))
+        return ARC_ERR_CUDA;
+    cudaError_t e = s->fp64 ? launch_set_state<double>(s->md, view<double>(s), dids, n_ids, din, s->stream)
+                            : launch_set_state<float>(s->mf, view<float>(s), dids, n_ids, din, s->stream);
+    if (check(s, e, "set_state kernel"))
+        return ARC_ERR_CUDA;
+    return sync(s, "arc_sim_set_state");
+}
+
+int arc_sim_set_terrain(arc_sim* s, int id, int nx, int ny, double cell, double outside, const double* heights)
+{
+    if (id < 0 || id >= s->n || nx <= 0 || ny <= 0 || nx > kGridMax || ny > kGridMax || !(cell > 0.0))
+        return fail(s, ARC_ERR_ARG, "arc_sim_set_terrain: bad world index or grid size");
+    if (ensure_spill(s, cell) != ARC_OK)
+        return ARC_ERR_CUDA;
+    double* d = (double*)grow(s, s->st_in, sizeof(double) * nx * ny);
+    if (!d)
+        return ARC_ERR_CUDA;
+    if (check(s, cudaMemcpyAsync(d, heights, sizeof(double) * nx * ny, cudaMemcpyHostToDevice, s->stream), "h"))
+        return ARC_ERR_CUDA;
+    cudaError_t e = s->fp64 ? launch_set_terrain<double>(view<double>(s), (TerrainGeom<double>*)s->tg, s->tgd, id,
+                                                         nx, ny, cell, outside, d, s->stream)
+                            : launch_set_terrain<float>(view<float>(s), (TerrainGeom<float>*)s->tg, s->tgd, id, nx,
+                                                        ny, cell, outside, d, s->stream);
+    if (check(s, e, "set_terrain kernel"))
+        return ARC_ERR_CUDA;
+    return sync(s, "arc_sim_set_terrain");
+}
+
+int arc_sim_get_terrain(const arc_sim* s, int id, int* nx_ny, double* geom, double* heights)
+{
+    if (id < 0 || id >= s->n)
+        return fail(s, ARC_ERR_ARG, "arc_sim_get_terrain: world index out of range");
+    TerrainGeomD g;
+    long long off = 0;
+    if (check(s, cudaMemcpyAsync(&g, s->tgd + id, sizeof(g), cudaMemcpyDeviceToHost, s->stream), "geom") ||
+        check(s, cudaMemcpyAsync(&off, s->toff + id, sizeof(off), cudaMemcpyDeviceToHost, s->stream), "off") ||
+        sync(s, "get_terrain"))
+        return ARC_ERR_CUDA;
+    if (nx_ny) {
+        nx_ny[0] = g.nx;
+        nx_ny[1] = g.ny;
+    }
+    if (geom) {
+        geom[0] = g.cell;
+        geom[1] = g.ox;
+        geom[2] = g.oy;
+        geom[3] = g.outside;
+    }
+    if (heights) {
+        const int cnt = g.nx * g.ny;
+        if (s->fp64) {
+            if (check(s, cudaMemcpy(heights, (double*)s->th + off, sizeof(double) * cnt, cudaMemcpyDeviceToHost),
+                      "heights"))
+                return ARC_ERR_CUDA;
+        } else {
+            std::vector<float> tmp(cnt);
+            if (check(s, cudaMemcpy(tmp.data(), (float*)s->th + off, sizeof(float) * cnt, cudaMemcpyDeviceToHost),
+                      "heights"))
+                return ARC_ERR_CUDA;
+            for (int c = 0; c < cnt; ++c)
+                heights[c] = tmp[c];
+        }
+    }
+    return ARC_OK;
+}
+
+int arc_sim_set_world_params(arc_sim* s, const double* gravity, double mu_static, double mu_dynamic)
+{
+    if (gravity)
+        s->model.gravity = V3<double>{gravity[0], gravity[1], gravity[2]};
+    s->model.mu_s = mu_static;
+    s->model.mu_d = mu_dynamic;
+    rebuild_models(s);
+    return ARC_OK;
+}
+
+int arc_sim_set_joint(arc_sim* s, int j, double lo, double hi, double kp, double kd, double max_torque)
+{
+    if (j < 0 || j >= s->model.nj)
+        return fail(s, ARC_ERR_ARG, "arc_sim_set_joint: joint index out of range");
+    ModelHost::Joint& t = s->model.j[j];
+    t.lo = lo;
+    t.hi = hi;
+    t.kp = kp;
+    t.kd = kd;
+    t.max_torque = max_torque;
+    rebuild_models(s);
+    return ARC_OK;
+}
+
+arc_model* arc_model_create(void)
+{
+    arc_model* m = new arc_model();
+    m->m.n_channels = 1;
+    return m;
+}
+
+void arc_model_destroy(arc_model* m) { delete m; }
+
+int arc_model_add_body(arc_model* m, double mass, const double* inertia, const double* pos, const double* q)
+{
+    return m->m.add_body(mass, V3<double>{inertia[0], inertia[1], inertia[2]}, V3<double>{pos[0], pos[1], pos[2]},
+                         Q4<double>{q[0], q[1], q[2], q[3]});
+}
+
+int arc_model_add_sphere(arc_model* m, int body, const double* local_pos, double radius)
+{
+    if (body < 0 || body >= m->m.nb)
+        return -1;
+    return m->m.add_sphere(body, V3<double>{local_pos[0], local_pos[1], local_pos[2]}, radius);
+}
+
+int arc_model_add_hinge(arc_model* m, int parent, int child, const double* anchor, const double* axis)
+{
+    if (child < 0 || child >= m->m.nb || parent >= m->m.nb)
+        return -1;
+    return m->m.add_hinge(parent, child, V3<double>{anchor[0], anchor[1], anchor[2]},
+                          V3<double>{axis[0], axis[1], axis[2]});
+}
+
+arc_sim* arc_sim_create_model(const arc_model* m, int n_worlds, double dt, int substeps, int grid, double cell,
+                              unsigned flags)
+{
+    if (!m || m->m.nb <= 0)
+        return nullptr;
+    ModelHost model = m->m;
+    for (int j = 0; j < model.nj; ++j)
+        model.default_angles[j] = 0.0;
+    return create_with_model(model, n_worlds, dt, substeps, grid, cell, flags | ARC_SIM_PLAIN);
+}
+
+int arc_sim_set_pose(arc_sim* s, int id, const double* pos, const double* q, const double* angles)
+{
+    if (id < 0 || id >= s->n)
+        return fail(s, ARC_ERR_ARG, "arc_sim_set_pose: world index out of range");
+    const ModelHost& m = s->model;
+    std::vector<double> st(arc_sim_state_size(s));
+    int rc = arc_sim_get_state(s, &id, 1, st.data());
+    if (rc != ARC_OK)
+        return rc;
+    V3<double> xs[kMaxBodies];
+    Q4<double> qs[kMaxBodies];
+    std::vector<double> zero(kMaxJoints, 0.0);
+    const double* ang = angles ? angles : zero.data();
+    m.pose(V3<double>{pos[0], pos[1], pos[2]}, Q4<double>{q[0], q[1], q[2], q[3]}, ang, xs, qs);
+    double* p = st.data();
+    for (int b = 0; b < m.nb; ++b, p += 13) {
+        p[0] = xs[b].x; p[1] = xs[b].y; p[2] = xs[b].z;
+        p[3] = qs[b].w; p[4] = qs[b].x; p[5] = qs[b].y; p[6] = qs[b].z;
+        for (int c = 7; c < 13; ++c)
+            p[c] = 0.0;
+    }
+    for (int sidx = 0; sidx < m.ns; ++sidx, p += 8) {
+        p[0] = 0.0;  // anchored
+        p[7] = 0.0;  // touch
+    }
+    for (int j = 0; j < m.nj; ++j, p += 4) {
+        p[0] = ang[j];
+        p[1] = ang[j];
+        p[2] = 0.0;
+        p[3] = 0.0;
+    }
+    p[0] = 0.0;  // unstable; time is kept
+    return arc_sim_set_state(s, &id, 1, st.data());
+}
+
+void* arc_sim_stream(const arc_sim* s) { return (void*)s->stream; }
+
+int arc_sim_step_device(arc_sim* s, const double* d_targets, void* stream)
+{
+    Actuation A{d_targets, nullptr};
+    return step_any(s, A, stream_of(s, stream));
+}
+
+int arc_sim_observe_device(const arc_sim* s, double* root, double* rot, double* joints, double* contacts, int* flags,
+                           void* stream)
+{
+    cudaStream_t st = stream_of(s, stream);
+    cudaError_t e = s->fp64 ? launch_observe<double>(s->md, view<double>(s), root, rot, joints, contacts, flags, st)
+                            : launch_observe<float>(s->mf, view<float>(s), root, rot, joints, contacts, flags, st);
+    return check(s, e, "observe kernel");
+}
+
+int arc_sim_synchronize(const arc_sim* s) { return sync(s, "arc_sim_synchronize"); }
+
+}  // extern "C"

@@ -1,0 +1,291 @@
+"""ctypes binding of libarcsim.so, the B200 batched world step.
+
+`Sim` has the reference binding's constructor, attributes and methods
+(arc/native.py:73-157): the same float64 output buffers, reused by
+`observe()`, the same argument checks. It adds what the GPU library offers
+beyond the reference: precision and kernel choice, state snapshots,
+per-world terrain, custom models and device-pointer calls.
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+usable, construction raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import functools
+import re
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libarcsim.so"
+HEADER = HERE.parent / "include" / "arc_sim.h"
+
+_f64 = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_u32 = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_vp = ctypes.c_void_p
+_int, _uint, _dbl = ctypes.c_int, ctypes.c_uint, ctypes.c_double
+
+ROOT_SIZE = 13  # pos(3) quat wxyz(4) linvel(3) angvel(3)
+FP64 = 1
+PLAIN = 2
+KERNEL_PLAIN = 0
+KERNEL_LEGS = 1
+
+
+class ArcSimError(RuntimeError):
+    pass
+
+
+def _declare(lib, name, restype, *argtypes):
+    fn = getattr(lib, name)
+    fn.restype = restype
+    fn.argtypes = list(argtypes)
+
+
+@functools.cache
+def sim_lib() -> ctypes.CDLL:
+    if not LIB_PATH.exists():
+        raise OSError(f"{LIB_PATH} not found: build it with `python -m arc_demo_b200.build`")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    d = functools.partial(_declare, lib)
+    # the reference's symbols (csrc/arc_sim.h:25-56), declared as arc/native.py:38-55 does
+    d("arc_sim_create", _vp, _int, _dbl, _int, _int, _dbl)
+    d("arc_sim_destroy", None, _vp)
+    d("arc_sim_set_threads", None, _vp, _int)
+    d("arc_sim_num_worlds", _int, _vp)
+    d("arc_sim_num_joints", _int)
+    d("arc_sim_num_legs", _int)
+    d("arc_sim_robot_info", None, _vp, _f64, _f64, _f64, _f64)
+    d("arc_sim_reset", None, _vp, _i32, _int, _u32, _f64)
+    d("arc_sim_step", None, _vp, _vp)
+    d("arc_sim_observe", None, _vp, _vp, _vp, _vp, _vp, _vp)
+    d("arc_sim_heights", None, _vp, _vp, _int, _vp)
+    d("arc_sim_terrain_at", None, _vp, _i32, _f64, _int, _f64)
+    d("arc_sim_world", _vp, _vp, _int)
+    # additive
+    d("arc_sim_create_ex", _vp, _int, _dbl, _int, _int, _dbl, _uint)
+    d("arc_sim_last_error", _int, _vp)
+    d("arc_sim_error_message", ctypes.c_char_p, _vp)
+    d("arc_sim_set_kernel", _int, _vp, _int, _int)
+    d("arc_sim_get_kernel", _int, _vp, ctypes.POINTER(_int), ctypes.POINTER(_int))
+    d("arc_sim_real_size", _int, _vp)
+    d("arc_sim_state_size", _int, _vp)
+    d("arc_sim_get_state", _int, _vp, _i32, _int, _f64)
+    d("arc_sim_set_state", _int, _vp, _i32, _int, _f64)
+    d("arc_sim_set_terrain", _int, _vp, _int, _int, _int, _dbl, _dbl, _f64)
+    d("arc_sim_get_terrain", _int, _vp, _int, _i32, _f64, _f64)
+    d("arc_sim_set_world_params", _int, _vp, _f64, _dbl, _dbl)
+    d("arc_sim_set_joint", _int, _vp, _int, _dbl, _dbl, _dbl, _dbl, _dbl)
+    d("arc_model_create", _vp)
+    d("arc_model_destroy", None, _vp)
+    d("arc_model_add_body", _int, _vp, _dbl, _f64, _f64, _f64)
+    d("arc_model_add_sphere", _int, _vp, _int, _f64, _dbl)
+    d("arc_model_add_hinge", _int, _vp, _int, _int, _f64, _f64)
+    d("arc_sim_create_model", _vp, _vp, _int, _dbl, _int, _int, _dbl, _uint)
+    d("arc_sim_set_pose", _int, _vp, _int, _f64, _f64, _vp)
+    d("arc_sim_stream", _vp, _vp)
+    d("arc_sim_step_device", _int, _vp, _vp, _vp)
+    d("arc_sim_observe_device", _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp)
+    d("arc_sim_synchronize", _int, _vp)
+    return lib
+
+
+def header_symbols() -> list[str]:
+    """Every function declared in include/arc_sim.h."""
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    return sorted(set(re.findall(r"\b(arc_\w+)\s*\(", text)))
+
+
+class Model:
+    """A custom model (bodies, hinges, spheres), as with csrc/arc_phys.h's builders."""
+
+    def __init__(self):
+        self._lib = sim_lib()
+        self.ptr = self._lib.arc_model_create()
+
+    def add_body(self, mass, inertia, pos, q=(1.0, 0.0, 0.0, 0.0)) -> int:
+        return self._lib.arc_model_add_body(self.ptr, mass, _vec(inertia), _vec(pos), _vec(q))
+
+    def add_sphere(self, body, pos, radius) -> int:
+        return self._lib.arc_model_add_sphere(self.ptr, body, _vec(pos), radius)
+
+    def add_hinge(self, parent, child, anchor, axis) -> int:
+        return self._lib.arc_model_add_hinge(self.ptr, parent, child, _vec(anchor), _vec(axis))
+
+    def close(self):
+        if self.ptr:
+            self._lib.arc_model_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        self.close()
+
+
+def _vec(v) -> np.ndarray:
+    return np.ascontiguousarray(v, dtype=np.float64)
+
+
+class Sim:
+    """N independent worlds, each with the quadruped on its own terrain."""
+
+    def __init__(self, num_worlds: int, dt: float = 1.0 / 30.0, substeps: int = 20,
+                 grid: int = 64, cell: float = 0.4, threads: int = 1, *, fp64: bool = False,
+                 plain: bool = False, model: Model | None = None):
+        self._lib = sim_lib()
+        self.num_worlds = num_worlds
+        self.grid = min(grid, 64)
+        self.cell = cell
+        self.dt, self.substeps = dt, substeps
+        self.num_joints = self._lib.arc_sim_num_joints()
+        self.num_legs = self._lib.arc_sim_num_legs()
+        flags = (FP64 if fp64 else 0) | (PLAIN if plain else 0)
+        if model is not None:
+            self._ptr = self._lib.arc_sim_create_model(model.ptr, num_worlds, dt, substeps, grid, cell, flags)
+        else:
+            self._ptr = self._lib.arc_sim_create_ex(num_worlds, dt, substeps, grid, cell, flags)
+        if not self._ptr:
+            raise MemoryError("arc_sim_create failed (no CUDA device, or out of memory)")
+        self._lib.arc_sim_set_threads(self._ptr, int(threads))
+
+        nj = self.num_joints
+        self.default_angles = np.zeros(nj)
+        self.lo, self.hi, misc = np.zeros(nj), np.zeros(nj), np.zeros(2)
+        self._lib.arc_sim_robot_info(self._ptr, self.default_angles, self.lo, self.hi, misc)
+        self.stand_height = float(misc[0])
+        self.total_mass = float(misc[1])
+        self.state_size = self._lib.arc_sim_state_size(self._ptr)
+
+        # output buffers, reused by observe()
+        self.root = np.zeros((num_worlds, ROOT_SIZE))
+        self.rot = np.zeros((num_worlds, 3, 3))
+        self.joints = np.zeros((num_worlds, 3 * nj))
+        self.contacts = np.zeros((num_worlds, self.num_legs + 2))
+        self.flags = np.zeros(num_worlds, dtype=np.int32)
+        self._observe_args = (self._ptr, self.root.ctypes.data, self.rot.ctypes.data,
+                              self.joints.ctypes.data, self.contacts.ctypes.data,
+                              self.flags.ctypes.data)
+
+    # -- errors ---------------------------------------------------------------
+
+    def _check(self, rc: int | None = None) -> None:
+        err = self._lib.arc_sim_last_error(self._ptr) if rc is None else rc
+        if err:
+            msg = self._lib.arc_sim_error_message(self._ptr).decode()
+            raise ArcSimError(f"libarcsim error {err}: {msg}")
+
+    # -- the reference's interface (arc/native.py:73-157) ---------------------
+
+    @property
+    def ptr(self) -> int:
+        return self._ptr
+
+    @property
+    def half_extent(self) -> float:
+        return 0.5 * self.grid * self.cell
+
+    def reset(self, ids: np.ndarray, seeds: np.ndarray, difficulty: np.ndarray) -> None:
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
+        difficulty = np.ascontiguousarray(difficulty, dtype=np.float64)
+        assert len(ids) == len(seeds) == len(difficulty)
+        if len(ids):
+            self._lib.arc_sim_reset(self._ptr, ids, len(ids), seeds, difficulty)
+            self._check()
+
+    def step(self, targets: np.ndarray) -> None:
+        targets = np.ascontiguousarray(targets, dtype=np.float64)
+        assert targets.shape == (self.num_worlds, self.num_joints)
+        self._lib.arc_sim_step(self._ptr, targets.ctypes.data)
+        self._check()
+
+    def observe(self) -> tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
+        """root (N, 13), joints (N, 3*J), contacts (N, legs + 2), flags (N,);
+        also refreshes rot (N, 3, 3)."""
+        self._lib.arc_sim_observe(*self._observe_args)
+        self._check()
+        return self.root, self.joints, self.contacts, self.flags
+
+    def heights(self, offsets: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+        offsets = np.ascontiguousarray(offsets, dtype=np.float64)
+        if out is None:
+            out = np.empty((self.num_worlds, len(offsets)))
+        assert out.shape == (self.num_worlds, len(offsets)) and out.dtype == np.float64
+        assert out.flags.c_contiguous
+        self._lib.arc_sim_heights(self._ptr, offsets.ctypes.data, len(offsets), out.ctypes.data)
+        self._check()
+        return out
+
+    def terrain_at(self, ids: np.ndarray, xy: np.ndarray) -> np.ndarray:
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        xy = np.ascontiguousarray(xy, dtype=np.float64)
+        out = np.zeros(len(ids))
+        if len(ids):
+            self._lib.arc_sim_terrain_at(self._ptr, ids, xy, len(ids), out)
+            self._check()
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_ptr", None):
+            self._lib.arc_sim_destroy(self._ptr)
+            self._ptr = None
+
+    def __del__(self):
+        self.close()
+
+    # -- additive -------------------------------------------------------------
+
+    def set_kernel(self, kernel: int, worlds_per_cta: int = 16) -> None:
+        self._check(self._lib.arc_sim_set_kernel(self._ptr, kernel, worlds_per_cta))
+
+    def kernel(self) -> tuple[int, int]:
+        k, w = _int(), _int()
+        self._lib.arc_sim_get_kernel(self._ptr, ctypes.byref(k), ctypes.byref(w))
+        return k.value, w.value
+
+    @property
+    def real_size(self) -> int:
+        return self._lib.arc_sim_real_size(self._ptr)
+
+    def get_state(self, ids=None) -> np.ndarray:
+        ids = np.arange(self.num_worlds) if ids is None else ids
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        out = np.zeros((len(ids), self.state_size))
+        self._check(self._lib.arc_sim_get_state(self._ptr, ids, len(ids), out))
+        return out
+
+    def set_state(self, state, ids=None) -> None:
+        ids = np.arange(self.num_worlds) if ids is None else ids
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        st = np.ascontiguousarray(state, dtype=np.float64).reshape(len(ids), self.state_size)
+        self._check(self._lib.arc_sim_set_state(self._ptr, ids, len(ids), st))
+
+    def set_terrain(self, i: int, heights: np.ndarray, cell: float, outside: float = -100.0) -> None:
+        h = np.ascontiguousarray(heights, dtype=np.float64)
+        ny, nx = h.shape
+        self._check(self._lib.arc_sim_set_terrain(self._ptr, int(i), nx, ny, cell, outside, h.ravel()))
+
+    def get_terrain(self, i: int):
+        nxy = np.zeros(2, dtype=np.int32)
+        geom = np.zeros(4)
+        h = np.zeros(64 * 64)
+        self._check(self._lib.arc_sim_get_terrain(self._ptr, int(i), nxy, geom, h))
+        nx, ny = int(nxy[0]), int(nxy[1])
+        return h[: nx * ny].reshape(ny, nx), geom
+
+    def set_world_params(self, gravity=(0.0, 0.0, -9.81), mu_static=1.0, mu_dynamic=0.8) -> None:
+        self._check(self._lib.arc_sim_set_world_params(self._ptr, _vec(gravity), mu_static, mu_dynamic))
+
+    def set_joint(self, j, lo, hi, kp, kd, max_torque) -> None:
+        self._check(self._lib.arc_sim_set_joint(self._ptr, j, lo, hi, kp, kd, max_torque))
+
+    def set_pose(self, i, pos, q=(1.0, 0.0, 0.0, 0.0), angles=None) -> None:
+        a = None if angles is None else _vec(angles)
+        self._check(self._lib.arc_sim_set_pose(self._ptr, int(i), _vec(pos), _vec(q),
+                                               None if a is None else a.ctypes.data))
+
+    def synchronize(self) -> None:
+        self._check(self._lib.arc_sim_synchronize(self._ptr))

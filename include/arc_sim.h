@@ -1,0 +1,166 @@
+/*
+ * arc_sim.h - C ABI of the B200 batched world step (libarcsim.so).
+ *
+ * Part 1 is the reference's batched API, symbol for symbol, so that the
+ * reference's ctypes binding (arc/native.py:38-55) and its C callers load
+ * this library unchanged. Every call there keeps the reference's contract:
+ * host float64 / int32 buffers, synchronous (results are in the caller's
+ * buffers when the call returns), void returns, NULL only from create.
+ *
+ * Part 2 is additive: status codes, precision and kernel selection, state
+ * snapshots, per-world terrain, custom models for the analytic scenes, and
+ * the device-resident path (device pointers, an explicit CUDA stream).
+ *
+ * All functions have C linkage and plain pointer/size arguments; none takes
+ * a PyTorch or CUDA runtime type (streams are passed as void *).
+ */
+#ifndef ARC_SIM_H
+#define ARC_SIM_H
+
+#include "arc_world.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct arc_sim arc_sim;
+
+/* Sizes of the per-world blocks of arc_sim_observe (csrc/arc_sim.h:17-21). */
+#define ARC_SIM_ROOT_SIZE 13    /* pos(3) quat wxyz(4) linvel(3) angvel(3), world frame */
+#define ARC_SIM_ROT_SIZE 9      /* torso rotation matrix (body to world), row-major */
+#define ARC_SIM_JOINT_SIZE 36   /* angles, rates, torques */
+#define ARC_SIM_CONTACT_SIZE 6  /* feet, torso, other leg parts */
+
+/* ======================================================================
+ * Part 1: the reference API (csrc/arc_sim.h:25-56)
+ * ====================================================================== */
+
+/* Replaces csrc/arc_sim.h:25 (csrc/arc_sim.c:26-54). n_worlds worlds of
+ * the quadruped on flat grid x grid terrain; grid is clamped to 64.
+ * Returns NULL if no CUDA device is usable or memory runs out. Steps in
+ * FP32 with the leg-parallel kernel (see arc_sim_create_ex). */
+arc_sim *arc_sim_create(int n_worlds, double dt, int substeps, int grid, double cell);
+
+/* Replaces csrc/arc_sim.h:26. NULL-safe. */
+void arc_sim_destroy(arc_sim *s);
+
+/* Replaces csrc/arc_sim.h:27: stored (<= 0 -> 1); the GPU ignores it. */
+void arc_sim_set_threads(arc_sim *s, int threads);
+
+/* Replace csrc/arc_sim.h:28-30. */
+int arc_sim_num_worlds(const arc_sim *s);
+int arc_sim_num_joints(void);
+int arc_sim_num_legs(void);
+
+/* Replaces csrc/arc_sim.h:33: default_angles, lo, hi are 12 doubles each,
+ * misc = {stand height, total mass}; any pointer may be NULL. */
+void arc_sim_robot_info(const arc_sim *s, double *default_angles, double *lo, double *hi, double *misc);
+
+/* Replaces csrc/arc_sim.h:38: regenerates the listed worlds' terrain from
+ * (seed, difficulty) and drops the robot in a noisy default stance with a
+ * random yaw, exactly as the reference's RNG stream dictates. */
+void arc_sim_reset(arc_sim *s, const int *ids, int n_ids, const unsigned int *seeds, const double *difficulty);
+
+/* Replaces csrc/arc_sim.h:42: targets is N x 12 drive targets (rad),
+ * clamped to the joint limits; unstable worlds are not stepped. */
+void arc_sim_step(arc_sim *s, const double *targets);
+
+/* Replaces csrc/arc_sim.h:46: root N x 13, rot N x 9, joints N x 36,
+ * contacts N x 6, flags N; any pointer may be NULL. */
+void arc_sim_observe(const arc_sim *s, double *root, double *rot, double *joints, double *contacts, int *flags);
+
+/* Replaces csrc/arc_sim.h:51: heights at k (forward, left) offsets in each
+ * torso's heading frame; out is N x k. */
+void arc_sim_heights(const arc_sim *s, const double *offsets, int k, double *out);
+
+/* Replaces csrc/arc_sim.h:54: height at point i (xy[2i], xy[2i+1]) of world ids[i]. */
+void arc_sim_terrain_at(const arc_sim *s, const int *ids, const double *xy, int m, double *out);
+
+/* Replaces csrc/arc_sim.h:56: a host FP64 copy of world i in the
+ * reference's arc_world layout (arc_world.h), refreshed from the device by
+ * this call and valid until the next arc_sim_world call on the same sim.
+ * Render-only visuals and the last substep's contact list are not kept on
+ * the device: n_visuals and n_contacts are 0. */
+const arc_world *arc_sim_world(const arc_sim *s, int i);
+
+/* ======================================================================
+ * Part 2: additive API (no counterpart in the reference)
+ * ====================================================================== */
+
+/* status codes */
+#define ARC_OK 0
+#define ARC_ERR_CUDA (-1)       /* a CUDA call failed; see arc_sim_error_message */
+#define ARC_ERR_ARG (-2)        /* bad argument (index, size, pointer) */
+#define ARC_ERR_UNSUPPORTED (-3) /* e.g. leg-parallel kernel on a non-quadruped model */
+
+/* create flags */
+#define ARC_SIM_FP64 1u         /* step in FP64 instead of FP32 */
+#define ARC_SIM_PLAIN 2u        /* start with the plain per-world kernel */
+
+/* kernels */
+#define ARC_KERNEL_PLAIN 0      /* one thread per world */
+#define ARC_KERNEL_LEGS 1       /* four lanes per world (one per leg), shared-memory staging */
+
+arc_sim *arc_sim_create_ex(int n_worlds, double dt, int substeps, int grid, double cell, unsigned flags);
+
+/* Last error of any call on s (0 if none) and its message; clears nothing. */
+int arc_sim_last_error(const arc_sim *s);
+const char *arc_sim_error_message(const arc_sim *s);
+
+/* Kernel choice; worlds_per_cta in {8, 16, 32, 64} for ARC_KERNEL_LEGS. */
+int arc_sim_set_kernel(arc_sim *s, int kernel, int worlds_per_cta);
+int arc_sim_get_kernel(const arc_sim *s, int *kernel, int *worlds_per_cta);
+/* 4 for FP32, 8 for FP64 */
+int arc_sim_real_size(const arc_sim *s);
+
+/* World-state snapshots, host FP64 buffers of arc_sim_state_size doubles per
+ * world: bodies (x3 q4 v3 w3) x nb, spheres (anchored, anchor3, anchor_n3,
+ * touch) x ns, joints (target, angle, rate, torque) x nj, unstable, time. */
+int arc_sim_state_size(const arc_sim *s);
+int arc_sim_get_state(const arc_sim *s, const int *ids, int n_ids, double *out);
+int arc_sim_set_state(arc_sim *s, const int *ids, int n_ids, const double *in);
+
+/* Terrain of one world: nx x ny columns (heights[ix + iy * nx], FP64),
+ * centred on the origin, `outside` beyond the grid; nx, ny <= the grid the
+ * sim was created with. geom = {cell, ox, oy, outside}. */
+int arc_sim_set_terrain(arc_sim *s, int id, int nx, int ny, double cell, double outside, const double *heights);
+int arc_sim_get_terrain(const arc_sim *s, int id, int *nx_ny, double *geom, double *heights);
+
+/* Gravity and friction coefficients of every world (csrc/arc_phys.c:32-39). */
+int arc_sim_set_world_params(arc_sim *s, const double *gravity, double mu_static, double mu_dynamic);
+
+/* Drive and limit parameters of joint j (lo > hi disables the limits). */
+int arc_sim_set_joint(arc_sim *s, int j, double lo, double hi, double kp, double kd, double max_torque);
+
+/* ---- custom models (csrc/arc_phys.h:114-144 builders), for scenes other
+ * than the quadruped; they step with ARC_KERNEL_PLAIN. */
+typedef struct arc_model arc_model;
+arc_model *arc_model_create(void);
+void arc_model_destroy(arc_model *m);
+/* inertia: principal moments; q: w, x, y, z. Returns the index or -1. */
+int arc_model_add_body(arc_model *m, double mass, const double *inertia, const double *pos, const double *q);
+int arc_model_add_sphere(arc_model *m, int body, const double *local_pos, double radius);
+int arc_model_add_hinge(arc_model *m, int parent, int child, const double *anchor, const double *axis);
+arc_sim *arc_sim_create_model(const arc_model *m, int n_worlds, double dt, int substeps, int grid, double cell,
+                              unsigned flags);
+/* Places body 0 at (pos, q) and the others by forward kinematics from the
+ * joint angles, zeroing velocities and setting drive targets to the angles
+ * (csrc/arc_phys.c:749-782). */
+int arc_sim_set_pose(arc_sim *s, int id, const double *pos, const double *q, const double *angles);
+
+/* ---- device-resident path. Pointers are CUDA device pointers; stream is a
+ * cudaStream_t (NULL: the sim's own stream). Calls are asynchronous on that
+ * stream. */
+void *arc_sim_stream(const arc_sim *s);
+/* targets: N x 12 FP64 on the device */
+int arc_sim_step_device(arc_sim *s, const double *d_targets, void *stream);
+/* observe into device FP64 buffers (any may be NULL) */
+int arc_sim_observe_device(const arc_sim *s, double *root, double *rot, double *joints, double *contacts, int *flags,
+                           void *stream);
+int arc_sim_synchronize(const arc_sim *s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

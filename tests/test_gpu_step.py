@@ -1,0 +1,251 @@
+"""Parity of the CUDA step (both kernels, FP32 and FP64) with the CPU checkers.
+
+Checkers: the reference's own csrc/ built from its sources (oracle/_ref,
+FP64 as shipped) and the C restatement (oracle/, FP64 and FP32).
+
+Tolerances (the parity contract):
+- FP64 kernels vs the reference, teacher-forced one control step (20
+  substeps) from the same state: body positions within 1e-9 m at the 99th
+  percentile, sphere touch counts equal in >= 99.9% of world-steps. The
+  only differences are FMA contraction and libm ulps.
+- FP32 kernels vs the FP64 reference, teacher-forced one control step: body
+  position error p99 <= 1e-5 m and quaternion error p99 <= 1e-5, relative to
+  unit quaternions; the maximum is reported. FP32 cannot meet a bound on
+  every world-step: threshold events (contact on/off, friction anchor reset,
+  limit activation) flip on differences far below FP32 resolution, so the
+  touch-count mismatch rate is bounded (<= 1%) and reported instead.
+- The two kernels (plain, leg-parallel) run the same solver in the same
+  per-body order, so they agree to within rounding of FMA placement.
+"""
+
+import numpy as np
+import pytest
+
+from arc_demo_b200.native import KERNEL_LEGS, KERNEL_PLAIN, Sim
+from oracle.oracle import NB, NS, OracleSim, RefSim, ref_available
+
+pytestmark = pytest.mark.gpu
+
+N = 64
+
+
+def seeds_diffs(n, seed=0):
+    rng = np.random.default_rng(seed)
+    return (rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32),
+            np.round(rng.uniform(0, 1, n), 1))
+
+
+def body_errors(a, b):
+    """Max over bodies of position and (sign-aligned) quaternion error per world."""
+    xa = a[:, : NB * 13].reshape(len(a), NB, 13)
+    xb = b[:, : NB * 13].reshape(len(b), NB, 13)
+    dx = np.linalg.norm(xa[..., :3] - xb[..., :3], axis=2).max(1)
+    qa, qb = xa[..., 3:7], xb[..., 3:7]
+    dq = np.minimum(np.linalg.norm(qa - qb, axis=2), np.linalg.norm(qa + qb, axis=2)).max(1)
+    return dx, dq
+
+
+def touches(s):
+    return s[:, NB * 13: NB * 13 + NS * 8].reshape(len(s), NS, 8)[:, :, 7]
+
+
+def diverse_states(n, steps=40, seed=0):
+    """FP64 reference states after some random-action steps on mixed terrain."""
+    ref = RefSim(n)
+    seeds, diffs = seeds_diffs(n, seed)
+    ref.reset(np.arange(n), seeds, diffs)
+    rng = np.random.default_rng(seed + 1)
+    for _ in range(steps):
+        ref.step(ref.default_angles + 0.6 * rng.uniform(-1, 1, (n, 12)))
+    return ref, seeds, diffs, rng
+
+
+def copy_terrain(dst, src, n):
+    for i in range(n):
+        h, geom = src.get_terrain(i)
+        dst.set_terrain(i, h, geom[0], geom[3])
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_reset_matches_oracle(fp64):
+    n = 48
+    seeds, diffs = seeds_diffs(n, 3)
+    g = Sim(n, fp64=fp64)
+    o = OracleSim(n, bits=64 if fp64 else 32)
+    g.reset(np.arange(n), seeds, diffs)
+    o.reset(np.arange(n), seeds, diffs)
+    for i in range(n):
+        hg, gg = g.get_terrain(i)
+        ho, go = o.get_terrain(i)
+        assert np.array_equal(hg, ho), f"terrain of world {i} differs"
+        # the FP32 oracle keeps its grid geometry in FP32
+        assert np.allclose(gg, go, rtol=0, atol=1e-12 if fp64 else 1e-6)
+    sg, so = g.get_state(), o.get_state()
+    tol = 1e-12 if fp64 else 3e-7
+    assert np.allclose(sg, so, rtol=tol, atol=tol)
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("kernel", [KERNEL_PLAIN, KERNEL_LEGS])
+def test_fp64_teacher_forced_vs_reference(kernel):
+    ref, seeds, diffs, rng = diverse_states(N)
+    g = Sim(N, fp64=True)
+    g.set_kernel(kernel, 16)
+    g.reset(np.arange(N), seeds, diffs)
+    dxs, mism = [], 0
+    for _ in range(10):
+        s0 = ref.get_state()
+        g.set_state(s0)
+        t = ref.default_angles + 0.6 * rng.uniform(-1, 1, (N, 12))
+        ref.step(t)
+        g.step(t)
+        a, b = ref.get_state(), g.get_state()
+        dx, _ = body_errors(a, b)
+        dxs.append(dx)
+        mism += int((touches(a) != touches(b)).any(1).sum())
+    dx = np.concatenate(dxs)
+    print(f"fp64 kernel {kernel}: |dx| p50 {np.median(dx):.2e} p99 {np.percentile(dx, 99):.2e} "
+          f"max {dx.max():.2e}; touch mismatches {mism}/{len(dx)}")
+    assert np.percentile(dx, 99) <= 1e-9
+    assert mism <= 0.001 * len(dx) + 1
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("kernel", [KERNEL_PLAIN, KERNEL_LEGS])
+def test_fp32_teacher_forced_vs_reference(kernel):
+    ref, seeds, diffs, rng = diverse_states(N, seed=5)
+    g = Sim(N)
+    g.set_kernel(kernel, 16)
+    g.reset(np.arange(N), seeds, diffs)
+    dxs, dqs, mism = [], [], 0
+    for _ in range(20):
+        s0 = ref.get_state()
+        g.set_state(s0)
+        t = ref.default_angles + 0.6 * rng.uniform(-1, 1, (N, 12))
+        ref.step(t)
+        g.step(t)
+        a, b = ref.get_state(), g.get_state()
+        dx, dq = body_errors(a, b)
+        dxs.append(dx)
+        dqs.append(dq)
+        mism += int((touches(a) != touches(b)).any(1).sum())
+    dx, dq = np.concatenate(dxs), np.concatenate(dqs)
+    print(f"fp32 kernel {kernel}: |dx| p50 {np.median(dx):.2e} p99 {np.percentile(dx, 99):.2e} "
+          f"max {dx.max():.2e}; |dq| p99 {np.percentile(dq, 99):.2e}; touch mismatches {mism}/{len(dx)}")
+    assert np.percentile(dx, 99) <= 1e-5
+    assert np.percentile(dq, 99) <= 1e-5
+    assert mism <= 0.01 * len(dx)
+
+
+def test_fp32_teacher_forced_vs_fp32_oracle():
+    n = N
+    seeds, diffs = seeds_diffs(n, 11)
+    o = OracleSim(n, bits=32)
+    g = Sim(n)
+    o.reset(np.arange(n), seeds, diffs)
+    g.reset(np.arange(n), seeds, diffs)
+    rng = np.random.default_rng(2)
+    for _ in range(30):
+        o.step(o.default_angles + 0.6 * rng.uniform(-1, 1, (n, 12)))
+    dxs, mism = [], 0
+    for _ in range(10):
+        g.set_state(o.get_state())
+        t = o.default_angles + 0.6 * rng.uniform(-1, 1, (n, 12))
+        o.step(t)
+        g.step(t)
+        a, b = o.get_state(), g.get_state()
+        dxs.append(body_errors(a, b)[0])
+        mism += int((touches(a) != touches(b)).any(1).sum())
+    dx = np.concatenate(dxs)
+    print(f"fp32 vs fp32 oracle: |dx| p50 {np.median(dx):.2e} p99 {np.percentile(dx, 99):.2e} max {dx.max():.2e}")
+    assert np.percentile(dx, 99) <= 1e-5
+    assert mism <= 0.01 * len(dx)
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_plain_and_leg_parallel_kernels_agree(fp64):
+    n = 96
+    seeds, diffs = seeds_diffs(n, 21)
+    a, b = Sim(n, fp64=fp64), Sim(n, fp64=fp64)
+    a.set_kernel(KERNEL_PLAIN)
+    b.set_kernel(KERNEL_LEGS, 32)
+    for s in (a, b):
+        s.reset(np.arange(n), seeds, diffs)
+    rng = np.random.default_rng(9)
+    worst = 0.0
+    for _ in range(5):
+        t = a.default_angles + 0.6 * rng.uniform(-1, 1, (n, 12))
+        b.set_state(a.get_state())
+        a.step(t)
+        b.step(t)
+        worst = max(worst, float(np.abs(a.get_state() - b.get_state()).max()))
+    print(f"plain vs legs ({'fp64' if fp64 else 'fp32'}): max abs state difference {worst:.2e}")
+    assert worst <= (1e-10 if fp64 else 1e-4)
+
+
+@pytest.mark.parametrize("wpc", [8, 16, 32, 64])
+def test_worlds_per_cta_and_ragged_batches(wpc):
+    """Any worlds-per-CTA and a world count that is not a multiple of it."""
+    n = 2 * wpc + 5
+    seeds, diffs = seeds_diffs(n, 4)
+    a, b = Sim(n), Sim(n)
+    a.set_kernel(KERNEL_LEGS, wpc)
+    b.set_kernel(KERNEL_PLAIN)
+    for s in (a, b):
+        s.reset(np.arange(n), seeds, diffs)
+    t = a.default_angles + 0.3
+    t = np.broadcast_to(t, (n, 12))
+    a.step(t)
+    b.step(t)
+    assert np.abs(a.get_state() - b.get_state()).max() <= 1e-4
+
+
+def test_observe_heights_terrain_at_match_oracle():
+    n = 40
+    seeds, diffs = seeds_diffs(n, 8)
+    g, o = Sim(n), OracleSim(n, bits=32)
+    g.reset(np.arange(n), seeds, diffs)
+    o.reset(np.arange(n), seeds, diffs)
+    rng = np.random.default_rng(3)
+    for _ in range(15):
+        t = g.default_angles + 0.6 * rng.uniform(-1, 1, (n, 12))
+        g.step(t)
+    o.set_state(g.get_state())
+    rg, jg, cg, fg = (x.copy() for x in g.observe())
+    ro, jo, co, fo = o.observe()
+    assert np.array_equal(rg, ro)
+    assert np.array_equal(jg, jo)
+    assert np.array_equal(cg, co)
+    assert np.array_equal(fg, fo)
+    assert np.allclose(g.rot, o.rot, rtol=0, atol=1e-15)
+    offs = np.array([(f, l) for f in np.arange(-1.0, 1.41, 0.2) for l in np.arange(-1.0, 1.01, 0.2)])
+    hg, ho = g.heights(offs), o.heights(offs)
+    mism = np.mean(hg != ho)
+    print(f"heights mismatch fraction {mism:.2e}")
+    assert mism <= 1e-3
+    ids = rng.integers(0, n, 500).astype(np.int32)
+    xy = rng.uniform(-14, 14, (500, 2))
+    assert np.array_equal(g.terrain_at(ids, xy), o.terrain_at(ids, xy))
+
+
+def test_unstable_worlds_are_flagged_and_skipped():
+    """csrc/arc_phys.c:689-705 and csrc/arc_sim.c:135: NaN / huge / fast states
+    are flagged; flagged worlds keep their state; targets are still clamped."""
+    n = 16
+    g = Sim(n)
+    g.reset(np.arange(n), np.arange(n, dtype=np.uint32), np.zeros(n))
+    st = g.get_state()
+    st[1, 0] = np.nan        # torso x
+    st[2, 0] = 1e12          # far away
+    st[3, 7] = 1000.0        # torso vx far above 60 m/s
+    g.set_state(st)
+    g.step(np.broadcast_to(g.default_angles, (n, 12)))
+    _, _, _, flags = g.observe()
+    assert list(flags[:4]) == [0, 1, 1, 1]
+    assert not flags[4:].any()
+    before = g.get_state()
+    g.step(np.full((n, 12), 10.0))
+    after = g.get_state()
+    assert np.array_equal(before[1:4, : NB * 13], after[1:4, : NB * 13], equal_nan=True)
+    tgt = after[:, NB * 13 + NS * 8:: 4][:, :12]
+    assert np.allclose(tgt[1], g.hi.astype(np.float32), atol=1e-6)
