@@ -96,7 +96,9 @@ ARC_HD R actuate(const DevModel<R>& M, const Actuation& A, int i, int j)
     } else {
         t = A.targets64[(size_t)i * M.nj + j];
     }
-    return r_clamp((R)t, M.lo[j], M.hi[j]);
+    // csrc/arc_sim.c:132-134 clamps to the limits; a joint whose limits are
+    // off (lo > hi, csrc/arc_phys.c:140-141) takes the target as given
+    return M.lo[j] <= M.hi[j] ? r_clamp((R)t, M.lo[j], M.hi[j]) : (R)t;
 }
 
 // Contacts that do not fit in a kernel's on-chip list go to this per-world

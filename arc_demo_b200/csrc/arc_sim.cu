@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "arc_model.h"
+#include "arc_task.cuh"
 #include "../../include/arc_sim.h"
 
 using namespace arc;
@@ -60,6 +61,17 @@ struct arc_sim {
     DevBuffer st_in, st_in2, st_in3, st_out;
     std::vector<double> host_tmp;
     arc_world* hworld = nullptr;
+    // task layer (arc_env_*)
+    bool env = false;
+    TaskParams tp;
+    TaskState ts{};
+    TaskOut to{};
+    float* actions = nullptr;
+    std::vector<void*> env_allocs;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaStream_t graph_stream = nullptr;
+    int graph_kernel = -1, graph_wpc = -1;
     mutable int err = 0;
     mutable std::string msg;
     mutable bool reported = false;
@@ -221,6 +233,12 @@ template <class R> int init_worlds(arc_sim* s)
 
 void free_all(arc_sim* s)
 {
+    if (s->graph_exec)
+        cudaGraphExecDestroy(s->graph_exec);
+    if (s->graph)
+        cudaGraphDestroy(s->graph);
+    for (void* p : s->env_allocs)
+        cudaFree(p);
     void* ps[] = {s->rec, s->sph, s->unstable, s->time, s->th, s->toff, s->tg, s->tgd, s->grid_of, s->spill,
                   s->st_in.p, s->st_in2.p, s->st_in3.p, s->st_out.p};
     for (void* p : ps)
@@ -387,11 +405,11 @@ void arc_sim_reset(arc_sim* s, const int* ids, int n_ids, const unsigned int* se
         return;
     cudaError_t e;
     if (s->fp64)
-        e = launch_reset<double>(s->rm, view<double>(s), (TerrainGeom<double>*)s->tg, s->tgd, d_ids, n_ids, d_seeds,
-                                 d_diff, s->grid_of, s->cell, st);
+        e = launch_reset_warp<double>(s->rm, view<double>(s), (TerrainGeom<double>*)s->tg, s->tgd, d_ids, n_ids,
+                                      d_seeds, d_diff, s->grid_of, s->cell, st);
     else
-        e = launch_reset<float>(s->rm, view<float>(s), (TerrainGeom<float>*)s->tg, s->tgd, d_ids, n_ids, d_seeds,
-                                d_diff, s->grid_of, s->cell, st);
+        e = launch_reset_warp<float>(s->rm, view<float>(s), (TerrainGeom<float>*)s->tg, s->tgd, d_ids, n_ids,
+                                     d_seeds, d_diff, s->grid_of, s->cell, st);
     if (check(s, e, "reset kernel"))
         return;
     sync(s, "arc_sim_reset");
@@ -631,6 +649,19 @@ int arc_sim_get_kernel(const arc_sim* s, int* kernel, int* worlds_per_cta)
 
 int arc_sim_real_size(const arc_sim* s) { return real_size(s); }
 
+int arc_sim_model_info(const arc_sim* s, int* n_bodies, int* n_joints, int* n_spheres, int* n_channels)
+{
+    if (n_bodies)
+        *n_bodies = s->model.nb;
+    if (n_joints)
+        *n_joints = s->model.nj;
+    if (n_spheres)
+        *n_spheres = s->model.ns;
+    if (n_channels)
+        *n_channels = s->model.n_channels;
+    return ARC_OK;
+}
+
 int arc_sim_state_size(const arc_sim* s)
 {
     return s->model.nb * 13 + s->model.ns * 8 + s->model.nj * 4 + 2;
@@ -845,6 +876,12 @@ int arc_sim_step_device(arc_sim* s, const double* d_targets, void* stream)
     return step_any(s, A, stream_of(s, stream));
 }
 
+int arc_sim_step_actions(arc_sim* s, const float* d_actions, void* stream)
+{
+    Actuation A{nullptr, d_actions};
+    return step_any(s, A, stream_of(s, stream));
+}
+
 int arc_sim_observe_device(const arc_sim* s, double* root, double* rot, double* joints, double* contacts, int* flags,
                            void* stream)
 {
@@ -855,5 +892,530 @@ int arc_sim_observe_device(const arc_sim* s, double* root, double* rot, double* 
 }
 
 int arc_sim_synchronize(const arc_sim* s) { return sync(s, "arc_sim_synchronize"); }
+
+
+// ============================================================================
+// the task layer on the device
+
+void arc_task_config_default(arc_task_config* c)
+{
+    // arc/task.py:17-66
+    c->dt = 1.0 / 30.0;
+    c->max_steps = 1000;
+    c->action_scale = 0.6;
+    c->checkpoint_radius = 0.5;
+    c->checkpoint_min_dist = 3.0;
+    c->checkpoint_max_dist = 6.0;
+    c->border = 1.5;
+    c->w_progress = 10.0;
+    c->max_speed = 1.2;
+    c->fov = 45.0;
+    c->w_turn = 1.0;
+    c->w_checkpoint = 10.0;
+    c->w_time = 0.05;
+    c->w_fall = 20.0;
+    c->w_energy = 0.002;
+    c->w_action_rate = 0.005;
+    c->w_body_contact = 0.02;
+    c->w_torso_contact = 0.5;
+    c->w_body_rate = 0.01;
+    c->w_bounce = 0.05;
+    c->flip_up_z = 0.3;
+    c->beached_steps = 30;
+    c->void_z = -2.0;
+    c->curriculum = 1;
+    c->difficulty = 0.0;
+    c->max_difficulty = 1.0;
+    c->level_step = 0.1;
+    c->level_up_checkpoints = 3;
+    c->level_down_steps = 300;
+}
+
+}  // extern "C"
+
+namespace {
+
+template <class T> T* env_alloc(arc_sim* s, size_t count, bool& ok)
+{
+    void* p = nullptr;
+    if (!ok || cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) {
+        ok = false;
+        return nullptr;
+    }
+    cudaMemset(p, 0, std::max<size_t>(count, 1) * sizeof(T));
+    s->env_allocs.push_back(p);
+    return static_cast<T*>(p);
+}
+
+int env_check(const arc_sim* s)
+{
+    if (!s->env)
+        return fail(s, ARC_ERR_ARG, "arc_env_* needs arc_env_init first");
+    if (!s->model.leaper)
+        return fail(s, ARC_ERR_UNSUPPORTED, "the task layer needs the quadruped model");
+    return ARC_OK;
+}
+
+template <class R> int env_task_step(arc_sim* s, const float* actions, bool write_obs, cudaStream_t st)
+{
+    const Worlds<R> W = view<R>(s);
+    if (check(s, cudaMemsetAsync(s->to.done_count, 0, sizeof(int), st), "memset done_count"))
+        return ARC_ERR_CUDA;
+    return check(s, launch_task_step<R>(dev_model<R>(s), W, s->tp, s->ts, s->to, actions, write_obs ? 1 : 0, st),
+                  "task step kernel");
+}
+
+template <class R> int env_reset_done(arc_sim* s, cudaStream_t st)
+{
+    return check(s,
+                 launch_task_reset<R>(dev_model<R>(s), s->rm, view<R>(s), (TerrainGeom<R>*)s->tg, s->tgd, s->grid_of,
+                                      s->cell, s->tp, s->ts, s->to.obs, s->to.done_list, s->to.done_count, s->n, st),
+                 "task reset kernel");
+}
+
+// the whole control step of ArcVecEnv.step_wait, as launched into `st`
+int env_step_launches(arc_sim* s, const float* actions, cudaStream_t st)
+{
+    Actuation A{nullptr, actions};
+    int rc = step_any(s, A, st);
+    if (rc)
+        return rc;
+    rc = s->fp64 ? env_task_step<double>(s, actions, true, st) : env_task_step<float>(s, actions, true, st);
+    if (rc)
+        return rc;
+    return s->fp64 ? env_reset_done<double>(s, st) : env_reset_done<float>(s, st);
+}
+
+}  // namespace
+
+extern "C" {
+
+int arc_env_init(arc_sim* s, const arc_task_config* cfg, unsigned long long seed)
+{
+    if (!s->model.leaper)
+        return fail(s, ARC_ERR_UNSUPPORTED, "the task layer needs the quadruped model");
+    if (s->env)
+        return ARC_OK;
+    arc_task_config c;
+    if (cfg)
+        c = *cfg;
+    else
+        arc_task_config_default(&c);
+    TaskParams& P = s->tp;
+    std::memset(&P, 0, sizeof(P));
+    P.dt = c.dt;
+    P.max_steps = c.max_steps;
+    P.action_scale = c.action_scale;
+    P.checkpoint_radius = c.checkpoint_radius;
+    P.checkpoint_min_dist = c.checkpoint_min_dist;
+    P.checkpoint_max_dist = c.checkpoint_max_dist;
+    P.border = c.border;
+    P.w_progress = c.w_progress;
+    P.max_speed = c.max_speed;
+    P.fov = c.fov;
+    P.w_turn = c.w_turn;
+    P.w_checkpoint = c.w_checkpoint;
+    P.w_time = c.w_time;
+    P.w_fall = c.w_fall;
+    P.w_energy = c.w_energy;
+    P.w_action_rate = c.w_action_rate;
+    P.w_body_contact = c.w_body_contact;
+    P.w_torso_contact = c.w_torso_contact;
+    P.w_body_rate = c.w_body_rate;
+    P.w_bounce = c.w_bounce;
+    P.flip_up_z = c.flip_up_z;
+    P.beached_steps = c.beached_steps;
+    P.void_z = c.void_z;
+    P.curriculum = c.curriculum;
+    P.difficulty = c.difficulty;
+    P.max_difficulty = c.max_difficulty;
+    P.level_step = c.level_step;
+    P.level_up_checkpoints = c.level_up_checkpoints;
+    P.level_down_steps = c.level_down_steps;
+    P.fov_rad = c.fov * (kPi / 180.0);  // np.radians multiplies by pi/180
+    P.cos_fov = std::cos(P.fov_rad);
+    P.half_extent = 0.5 * s->grid * s->cell;
+    P.stand_height = s->model.stand_height;
+    for (int j = 0; j < kNumJoints; ++j)
+        P.default_angles[j] = s->model.default_angles[j];
+    // arc/task.py:74-76: np.arange(-1.0, 1.41, 0.2) x np.arange(-1.0, 1.01, 0.2)
+    int k = 0;
+    for (int a = 0; a < 13; ++a)
+        for (int b = 0; b < 11; ++b, ++k) {
+            P.offsets[k][0] = -1.0 + a * 0.2;
+            P.offsets[k][1] = -1.0 + b * 0.2;
+        }
+    P.seed = seed;
+    // the action scale of the actuation follows the task config
+    s->mf.action_scale = c.action_scale;
+    s->md.action_scale = c.action_scale;
+
+    const size_t n = (size_t)std::max(s->n, 1);
+    bool ok = true;
+    TaskState& S = s->ts;
+    S.target = env_alloc<double>(s, 2 * n, ok);
+    S.target_z = env_alloc<double>(s, n, ok);
+    S.prev_dist = env_alloc<double>(s, n, ok);
+    S.prev_gaze = env_alloc<double>(s, n, ok);
+    S.prev_action = env_alloc<float>(s, n * kNumJoints, ok);
+    S.torso_steps = env_alloc<int>(s, n, ok);
+    S.steps = env_alloc<int>(s, n, ok);
+    S.checkpoints = env_alloc<int>(s, n, ok);
+    S.level = env_alloc<double>(s, n, ok);
+    S.difficulty = env_alloc<double>(s, n, ok);
+    S.in_view = env_alloc<unsigned char>(s, n, ok);
+    S.episode = env_alloc<unsigned>(s, n, ok);
+    S.draws = env_alloc<unsigned>(s, n, ok);
+    TaskOut& O = s->to;
+    O.obs = env_alloc<float>(s, n * kObsSize, ok);
+    O.terminal_obs = env_alloc<float>(s, n * kObsSize, ok);
+    O.reward = env_alloc<float>(s, n, ok);
+    O.terminated = env_alloc<unsigned char>(s, n, ok);
+    O.truncated = env_alloc<unsigned char>(s, n, ok);
+    O.cause = env_alloc<signed char>(s, n, ok);
+    O.ended_checkpoints = env_alloc<int>(s, n, ok);
+    O.ended_difficulty = env_alloc<double>(s, n, ok);
+    O.ended_steps = env_alloc<int>(s, n, ok);
+    O.done_list = env_alloc<int>(s, n, ok);
+    O.done_count = env_alloc<int>(s, 1, ok);
+    s->actions = env_alloc<float>(s, n * kNumJoints, ok);
+    if (!ok)
+        return fail(s, ARC_ERR_CUDA, "arc_env_init: device allocation failed");
+    // initial level / difficulty (arc/task.py:107-108)
+    std::vector<double> lvl(n, c.curriculum ? 0.0 : c.difficulty);
+    if (check(s, cudaMemcpy(S.level, lvl.data(), n * sizeof(double), cudaMemcpyHostToDevice), "level") ||
+        check(s, cudaMemcpy(S.difficulty, lvl.data(), n * sizeof(double), cudaMemcpyHostToDevice), "difficulty"))
+        return ARC_ERR_CUDA;
+    s->env = true;
+    return ARC_OK;
+}
+
+int arc_env_reset(arc_sim* s, const int* ids, int n_ids, void* stream)
+{
+    if (int rc = env_check(s))
+        return rc;
+    cudaStream_t st = stream_of(s, stream);
+    std::vector<int> all;
+    if (!ids || n_ids < 0) {
+        all.resize(s->n);
+        for (int i = 0; i < s->n; ++i)
+            all[i] = i;
+        ids = all.data();
+        n_ids = s->n;
+    }
+    if (n_ids == 0)
+        return ARC_OK;
+    if (!ids_ok(s, ids, n_ids))
+        return fail(s, ARC_ERR_ARG, "arc_env_reset: world index out of range");
+    int* d = (int*)grow(s, s->st_in3, sizeof(int) * n_ids);
+    if (!d)
+        return ARC_ERR_CUDA;
+    if (check(s, cudaMemcpyAsync(d, ids, sizeof(int) * n_ids, cudaMemcpyHostToDevice, st), "reset ids"))
+        return ARC_ERR_CUDA;
+    cudaError_t e =
+        s->fp64 ? launch_task_reset<double>(s->md, s->rm, view<double>(s), (TerrainGeom<double>*)s->tg, s->tgd,
+                                            s->grid_of, s->cell, s->tp, s->ts, s->to.obs, d, nullptr, n_ids, st)
+                : launch_task_reset<float>(s->mf, s->rm, view<float>(s), (TerrainGeom<float>*)s->tg, s->tgd,
+                                           s->grid_of, s->cell, s->tp, s->ts, s->to.obs, d, nullptr, n_ids, st);
+    if (check(s, e, "task reset kernel"))
+        return ARC_ERR_CUDA;
+    return check(s, cudaStreamSynchronize(st), "arc_env_reset");
+}
+
+int arc_env_step(arc_sim* s, const float* d_actions, void* stream)
+{
+    if (int rc = env_check(s))
+        return rc;
+    cudaStream_t st = stream_of(s, stream);
+    if (d_actions)
+        return env_step_launches(s, d_actions, st);
+    // graph of the whole control step over the ARC_ENV_ACTIONS buffer
+    if (s->graph_exec && (s->graph_kernel != s->kernel || s->graph_wpc != s->wpc)) {
+        cudaGraphExecDestroy(s->graph_exec);
+        cudaGraphDestroy(s->graph);
+        s->graph_exec = nullptr;
+        s->graph = nullptr;
+    }
+    if (!s->graph_exec) {
+        // one eager step first: kernels configure their attributes outside capture
+        // (this step is real work on the current actions, like every other step)
+        if (int rc = env_step_launches(s, s->actions, st))
+            return rc;
+        if (!s->graph_stream &&
+            check(s, cudaStreamCreateWithFlags(&s->graph_stream, cudaStreamNonBlocking), "graph stream"))
+            return ARC_ERR_CUDA;
+        if (check(s, cudaStreamSynchronize(st), "pre-capture sync") ||
+            check(s, cudaStreamBeginCapture(s->graph_stream, cudaStreamCaptureModeThreadLocal), "begin capture"))
+            return ARC_ERR_CUDA;
+        int rc = env_step_launches(s, s->actions, s->graph_stream);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(s->graph_stream, &g);
+        if (rc)
+            return rc;
+        if (check(s, e, "end capture") || check(s, cudaGraphInstantiate(&s->graph_exec, g, 0), "instantiate"))
+            return ARC_ERR_CUDA;
+        s->graph = g;
+        s->graph_kernel = s->kernel;
+        s->graph_wpc = s->wpc;
+        return ARC_OK;
+    }
+    return check(s, cudaGraphLaunch(s->graph_exec, st), "graph launch");
+}
+
+int arc_env_task_step(arc_sim* s, const float* d_actions, void* stream)
+{
+    if (int rc = env_check(s))
+        return rc;
+    cudaStream_t st = stream_of(s, stream);
+    const float* a = d_actions ? d_actions : s->actions;
+    Actuation A{nullptr, a};
+    if (int rc = step_any(s, A, st))
+        return rc;
+    return s->fp64 ? env_task_step<double>(s, a, false, st) : env_task_step<float>(s, a, false, st);
+}
+
+int arc_env_observe(arc_sim* s, void* stream)
+{
+    if (int rc = env_check(s))
+        return rc;
+    cudaStream_t st = stream_of(s, stream);
+    cudaError_t e = s->fp64 ? launch_task_observe<double>(s->md, view<double>(s), s->tp, s->ts, s->to.obs, nullptr,
+                                                          s->n, st)
+                            : launch_task_observe<float>(s->mf, view<float>(s), s->tp, s->ts, s->to.obs, nullptr,
+                                                         s->n, st);
+    return check(s, e, "task observe kernel");
+}
+
+int arc_env_buffer(const arc_sim* s, int which, void** ptr, long long* shape, int* ndim, int* code, int* bits)
+{
+    if (int rc = env_check(s))
+        return rc;
+    const long long n = s->n;
+    void* p = nullptr;
+    long long sh[2] = {n, 1};
+    int nd = 1, c = 2, b = 32;
+    switch (which) {
+    case ARC_ENV_OBS: p = s->to.obs; sh[1] = kObsSize; nd = 2; break;
+    case ARC_ENV_TERMINAL_OBS: p = s->to.terminal_obs; sh[1] = kObsSize; nd = 2; break;
+    case ARC_ENV_REWARD: p = s->to.reward; break;
+    case ARC_ENV_TERMINATED: p = s->to.terminated; c = 1; b = 8; break;
+    case ARC_ENV_TRUNCATED: p = s->to.truncated; c = 1; b = 8; break;
+    case ARC_ENV_CAUSE: p = s->to.cause; c = 0; b = 8; break;
+    case ARC_ENV_DONE_LIST: p = s->to.done_list; c = 0; break;
+    case ARC_ENV_DONE_COUNT: p = s->to.done_count; c = 0; sh[0] = 1; break;
+    case ARC_ENV_ACTIONS: p = s->actions; sh[1] = kNumJoints; nd = 2; break;
+    case ARC_ENV_ENDED_CHECKPOINTS: p = s->to.ended_checkpoints; c = 0; break;
+    case ARC_ENV_ENDED_STEPS: p = s->to.ended_steps; c = 0; break;
+    case ARC_ENV_ENDED_DIFFICULTY: p = s->to.ended_difficulty; b = 64; break;
+    default: return fail(s, ARC_ERR_ARG, "arc_env_buffer: unknown buffer");
+    }
+    if (ptr)
+        *ptr = p;
+    if (shape) {
+        shape[0] = sh[0];
+        shape[1] = sh[1];
+    }
+    if (ndim)
+        *ndim = nd;
+    if (code)
+        *code = c;
+    if (bits)
+        *bits = b;
+    return ARC_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// DLPack v0.8 ABI (dlpack.h): the exchange format torch.from_dlpack reads.
+struct DLDevice_ {
+    int32_t device_type;  // kDLCUDA = 2
+    int32_t device_id;
+};
+struct DLDataType_ {
+    uint8_t code, bits;
+    uint16_t lanes;
+};
+struct DLTensor_ {
+    void* data;
+    DLDevice_ device;
+    int32_t ndim;
+    DLDataType_ dtype;
+    int64_t* shape;
+    int64_t* strides;
+    uint64_t byte_offset;
+};
+struct DLManagedTensor_ {
+    DLTensor_ dl_tensor;
+    void* manager_ctx;
+    void (*deleter)(DLManagedTensor_*);
+};
+struct DLPackHolder {
+    DLManagedTensor_ t;
+    int64_t shape[2];
+};
+
+void dlpack_delete(DLManagedTensor_* t) { delete reinterpret_cast<DLPackHolder*>(t->manager_ctx); }
+
+}  // namespace
+
+extern "C" {
+
+int arc_env_dlpack(const arc_sim* s, int which, void** managed)
+{
+    void* p;
+    long long shape[2];
+    int nd, code, bits;
+    if (int rc = arc_env_buffer(s, which, &p, shape, &nd, &code, &bits))
+        return rc;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    DLPackHolder* h = new DLPackHolder();
+    h->shape[0] = shape[0];
+    h->shape[1] = shape[1];
+    h->t.dl_tensor.data = p;
+    h->t.dl_tensor.device = DLDevice_{2, dev};
+    h->t.dl_tensor.ndim = nd;
+    h->t.dl_tensor.dtype = DLDataType_{(uint8_t)code, (uint8_t)bits, 1};
+    h->t.dl_tensor.shape = h->shape;
+    h->t.dl_tensor.strides = nullptr;  // compact row-major
+    h->t.dl_tensor.byte_offset = 0;
+    h->t.manager_ctx = h;
+    h->t.deleter = dlpack_delete;
+    *managed = &h->t;
+    return ARC_OK;
+}
+
+static int env_copy(const arc_sim* s, int which, void* host, bool down)
+{
+    void* p;
+    long long shape[2];
+    int nd, code, bits;
+    if (int rc = arc_env_buffer(s, which, &p, shape, &nd, &code, &bits))
+        return rc;
+    const size_t bytes = (size_t)shape[0] * (nd == 2 ? shape[1] : 1) * (bits / 8);
+    if (sync(s, "env copy"))
+        return ARC_ERR_CUDA;
+    return check(s, cudaMemcpy(down ? host : p, down ? p : host, bytes,
+                               down ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice),
+                 "env copy");
+}
+
+int arc_env_download(const arc_sim* s, int which, void* host) { return env_copy(s, which, host, true); }
+int arc_env_upload(arc_sim* s, int which, const void* host) { return env_copy(s, which, (void*)host, false); }
+
+int arc_env_get_task_state(const arc_sim* s, const int* ids, int n_ids, double* out)
+{
+    if (int rc = env_check(s))
+        return rc;
+    if (!ids_ok(s, ids, n_ids))
+        return fail(s, ARC_ERR_ARG, "arc_env_get_task_state: world index out of range");
+    if (sync(s, "task state"))
+        return ARC_ERR_CUDA;
+    const size_t n = s->n;
+    std::vector<double> tgt(2 * n), tz(n), pd(n), pg(n), lvl(n), dif(n);
+    std::vector<float> pa(n * kNumJoints);
+    std::vector<int> ts(n), st(n), cp(n);
+    std::vector<unsigned char> iv(n);
+    std::vector<unsigned> ep(n), dr(n);
+    const TaskState& S = s->ts;
+    bool ok = cudaMemcpy(tgt.data(), S.target, 2 * n * 8, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(tz.data(), S.target_z, n * 8, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(pd.data(), S.prev_dist, n * 8, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(pg.data(), S.prev_gaze, n * 8, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(pa.data(), S.prev_action, n * kNumJoints * 4, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(ts.data(), S.torso_steps, n * 4, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(st.data(), S.steps, n * 4, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(cp.data(), S.checkpoints, n * 4, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(lvl.data(), S.level, n * 8, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(dif.data(), S.difficulty, n * 8, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(iv.data(), S.in_view, n, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(ep.data(), S.episode, n * 4, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(dr.data(), S.draws, n * 4, cudaMemcpyDeviceToHost) == cudaSuccess;
+    if (!ok)
+        return check(s, cudaGetLastError(), "task state copy");
+    for (int k = 0; k < n_ids; ++k) {
+        const int i = ids[k];
+        double* o = out + (size_t)k * ARC_TASK_STATE_SIZE;
+        o[0] = tgt[2 * i];
+        o[1] = tgt[2 * i + 1];
+        o[2] = tz[i];
+        o[3] = pd[i];
+        o[4] = pg[i];
+        for (int j = 0; j < kNumJoints; ++j)
+            o[5 + j] = pa[(size_t)i * kNumJoints + j];
+        o[17] = ts[i];
+        o[18] = st[i];
+        o[19] = cp[i];
+        o[20] = lvl[i];
+        o[21] = dif[i];
+        o[22] = iv[i];
+        o[23] = ep[i];
+        o[24] = dr[i];
+    }
+    return ARC_OK;
+}
+
+int arc_env_set_task_state(arc_sim* s, const int* ids, int n_ids, const double* in)
+{
+    if (int rc = env_check(s))
+        return rc;
+    if (!ids_ok(s, ids, n_ids))
+        return fail(s, ARC_ERR_ARG, "arc_env_set_task_state: world index out of range");
+    if (sync(s, "task state"))
+        return ARC_ERR_CUDA;
+    const TaskState& S = s->ts;
+    for (int k = 0; k < n_ids; ++k) {
+        const int i = ids[k];
+        const double* p = in + (size_t)k * ARC_TASK_STATE_SIZE;
+        float pa[kNumJoints];
+        for (int j = 0; j < kNumJoints; ++j)
+            pa[j] = (float)p[5 + j];
+        int ints[3] = {(int)p[17], (int)p[18], (int)p[19]};
+        unsigned char iv = p[22] != 0.0;
+        unsigned ep = (unsigned)p[23], dr = (unsigned)p[24];
+        bool ok = cudaMemcpy(S.target + 2 * i, p, 16, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(S.target_z + i, p + 2, 8, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(S.prev_dist + i, p + 3, 8, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(S.prev_gaze + i, p + 4, 8, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(S.prev_action + (size_t)i * kNumJoints, pa, sizeof(pa), cudaMemcpyHostToDevice) ==
+                      cudaSuccess &&
+                  cudaMemcpy(S.torso_steps + i, &ints[0], 4, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(S.steps + i, &ints[1], 4, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(S.checkpoints + i, &ints[2], 4, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(S.level + i, p + 20, 8, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(S.difficulty + i, p + 21, 8, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(S.in_view + i, &iv, 1, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(S.episode + i, &ep, 4, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(S.draws + i, &dr, 4, cudaMemcpyHostToDevice) == cudaSuccess;
+        if (!ok)
+            return check(s, cudaGetLastError(), "task state copy");
+    }
+    return ARC_OK;
+}
+
+int arc_env_set_targets(arc_sim* s, const int* ids, int n_ids, const double* xy)
+{
+    if (int rc = env_check(s))
+        return rc;
+    if (n_ids <= 0)
+        return ARC_OK;
+    if (!ids_ok(s, ids, n_ids))
+        return fail(s, ARC_ERR_ARG, "arc_env_set_targets: world index out of range");
+    char* buf = (char*)grow(s, s->st_in3, (size_t)n_ids * (2 * sizeof(double) + sizeof(int)));
+    if (!buf)
+        return ARC_ERR_CUDA;
+    double* dxy = (double*)buf;
+    int* dids = (int*)(buf + (size_t)n_ids * 2 * sizeof(double));
+    if (check(s, cudaMemcpyAsync(dxy, xy, sizeof(double) * 2 * n_ids, cudaMemcpyHostToDevice, s->stream), "xy") ||
+        check(s, cudaMemcpyAsync(dids, ids, sizeof(int) * n_ids, cudaMemcpyHostToDevice, s->stream), "ids"))
+        return ARC_ERR_CUDA;
+    cudaError_t e = s->fp64 ? launch_task_set_targets<double>(view<double>(s), s->tp, s->ts, dids, dxy, n_ids, s->stream)
+                            : launch_task_set_targets<float>(view<float>(s), s->tp, s->ts, dids, dxy, n_ids, s->stream);
+    if (check(s, e, "set targets kernel"))
+        return ARC_ERR_CUDA;
+    return sync(s, "arc_env_set_targets");
+}
 
 }  // extern "C"

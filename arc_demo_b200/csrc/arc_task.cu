@@ -1,0 +1,681 @@
+// arc_task.cu - task layer kernels (arc/task.py on the device) and the
+// warp-cooperative world reset (csrc/arc_sim.c:88-110).
+#include "arc_task.cuh"
+
+namespace arc {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// reference RNG (csrc/arc_rng.h:14-53), integer exact
+
+struct Xorshift {
+    uint32_t s[4];
+    __device__ __forceinline__ uint32_t next()
+    {
+        uint32_t t = s[3], v = s[0];
+        s[3] = s[2];
+        s[2] = s[1];
+        s[1] = v;
+        t = t ^ (t << 11);
+        t ^= t >> 8;
+        s[0] = t ^ v ^ (v >> 19);
+        return s[0];
+    }
+    __device__ __forceinline__ void seed(uint32_t seed)
+    {
+        for (int i = 0; i < 4; ++i) {
+            uint32_t x = seed + 0x9e3779b9U * (uint32_t)(i + 1);
+            x = (x ^ (x >> 16)) * 0x7feb352dU;
+            x = (x ^ (x >> 15)) * 0x846ca68bU;
+            seed = x ^ (x >> 16);
+            s[i] = seed ? seed : 1U;
+        }
+    }
+};
+
+// rng_range(lo, hi) of a raw draw u (csrc/arc_rng.h:45-53)
+__device__ __forceinline__ double range_of(uint32_t u, double lo, double hi)
+{
+    return lo + (hi - lo) * (u * (1.0 / 4294967296.0));
+}
+
+// ---------------------------------------------------------------------------
+// device RNG of the task layer (checkpoints, reset seeds): a counter-based
+// splitmix64 stream per (seed, world, kind). The reference draws these from
+// numpy's PCG64 on the host (arc/task.py:117,138-139); the device cannot
+// reproduce that stream, so it draws the same distributions from its own.
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+__device__ __forceinline__ uint64_t stream_u64(uint64_t seed, int world, uint32_t kind, uint32_t counter)
+{
+    return splitmix64(splitmix64(seed ^ (((uint64_t)(uint32_t)world << 32) | kind)) + counter);
+}
+
+__device__ __forceinline__ double unit(uint64_t x) { return (double)(x >> 11) * (1.0 / 9007199254740992.0); }
+
+// ---------------------------------------------------------------------------
+// world read-out in FP64 (what arc_sim_observe returns, csrc/arc_sim.c:140-183)
+
+struct Obs64 {
+    V3<double> x, v, w;
+    Q4<double> q;
+    M3<double> rot;
+    double angle[kNumJoints], rate[kNumJoints], torque[kNumJoints];
+    double contact[kNumLegs + 2];
+    int unstable;
+};
+
+template <class R>
+__device__ void read_world(const DevModel<R>& M, const Worlds<R>& W, int i, Obs64& o)
+{
+    const R* rec = W.rec + (size_t)i * W.stride;
+    o.x = V3<double>{(double)rec[0], (double)rec[1], (double)rec[2]};
+    o.q = Q4<double>{(double)rec[3], (double)rec[4], (double)rec[5], (double)rec[6]};
+    o.v = V3<double>{(double)rec[7], (double)rec[8], (double)rec[9]};
+    o.w = V3<double>{(double)rec[10], (double)rec[11], (double)rec[12]};
+    o.rot = m3_from_quat(o.q);
+    const R* jr = rec + W.off_joint;
+    for (int j = 0; j < kNumJoints; ++j) {
+        o.angle[j] = (double)jr[j * kJointRec + 1];
+        o.rate[j] = (double)jr[j * kJointRec + 2];
+        o.torque[j] = (double)jr[j * kJointRec + 3];
+    }
+    const uint32_t* sph = W.sph + (size_t)i * M.ns;
+    const double inv = 1.0 / M.substeps;
+    for (int c = 0; c < kNumLegs + 2; ++c)
+        o.contact[c] = 0.0;
+    for (int s = 0; s < M.ns; ++s) {
+        double v = (int)(sph[s] & 0xffffu) * inv;
+        double& c = o.contact[M.channel[s]];
+        c = c > v ? c : v;
+    }
+    o.unstable = W.unstable[i];
+}
+
+template <class R> __device__ __forceinline__ double height_at(const Worlds<R>& W, int i, double x, double y)
+{
+    const TerrainGeomD g = W.tgd[i];
+    double fx = floor((x - g.ox) / g.cell), fy = floor((y - g.oy) / g.cell);
+    if (!(fx >= 0.0 && fy >= 0.0 && fx < g.nx && fy < g.ny))
+        return g.outside;
+    return (double)W.th[W.toff[i] + (int)fx + (int)fy * g.nx];
+}
+
+// |angle| between the gaze (body +x on the ground) and the target (arc/task.py:79-85)
+__device__ __forceinline__ double gaze_error(const M3<double>& rot, V3<double> pos, const double* target)
+{
+    double fx = rot.m[0][0], fy = rot.m[1][0];
+    double dx = target[0] - pos.x, dy = target[1] - pos.y;
+    return fabs(atan2(fx * dy - fy * dx, fx * dx + fy * dy));
+}
+
+// R^T a, summed like numpy's a @ R for a row vector
+__device__ __forceinline__ V3<double> rt_mul(const M3<double>& r, V3<double> a)
+{
+    return V3<double>{a.x * r.m[0][0] + a.y * r.m[1][0] + a.z * r.m[2][0],
+                      a.x * r.m[0][1] + a.y * r.m[1][1] + a.z * r.m[2][1],
+                      a.x * r.m[0][2] + a.y * r.m[1][2] + a.z * r.m[2][2]};
+}
+
+__device__ __forceinline__ float obs_value(double v)
+{
+    float f = (float)v;
+    return isfinite(f) ? f : 0.0f;
+}
+
+// arc/task.py:231-259: writes the 195 observation values of world i
+template <class R>
+__device__ void write_obs(const TaskParams& P, const Worlds<R>& W, const TaskState& S, int i, const Obs64& o,
+                          float* dst)
+{
+    const M3<double>& r = o.rot;
+    int k = 0;
+    dst[k++] = obs_value(-r.m[2][0]);
+    dst[k++] = obs_value(-r.m[2][1]);
+    dst[k++] = obs_value(-r.m[2][2]);
+    V3<double> lin = rt_mul(r, o.v), ang = rt_mul(r, o.w);
+    dst[k++] = obs_value(lin.x);
+    dst[k++] = obs_value(lin.y);
+    dst[k++] = obs_value(lin.z);
+    dst[k++] = obs_value(0.25 * ang.x);
+    dst[k++] = obs_value(0.25 * ang.y);
+    dst[k++] = obs_value(0.25 * ang.z);
+    for (int j = 0; j < kNumJoints; ++j)
+        dst[k++] = obs_value(o.angle[j] - P.default_angles[j]);
+    for (int j = 0; j < kNumJoints; ++j)
+        dst[k++] = obs_value(0.1 * o.rate[j]);
+    for (int j = 0; j < kNumJoints; ++j)
+        dst[k++] = obs_value((double)S.prev_action[(size_t)i * kNumJoints + j]);
+    const double heading = atan2(r.m[1][0], r.m[0][0]);
+    const double dx = S.target[2 * i] - o.x.x, dy = S.target[2 * i + 1] - o.x.y;
+    const double c = cos(heading), s = sin(heading);
+    const double fwd = c * dx + s * dy, left = -s * dx + c * dy;
+    double dist = hypot(fwd, left);
+    dist = dist > 1e-6 ? dist : 1e-6;
+    dst[k++] = obs_value(fwd / dist);
+    dst[k++] = obs_value(left / dist);
+    dst[k++] = obs_value((dist < 6.0 ? dist : 6.0) / 6.0);
+    // heights in the heading frame (csrc/arc_sim.c:185-203)
+    V3<double> f = qrotate(o.q, V3<double>{1.0, 0.0, 0.0});
+    const double yaw = atan2(f.y, f.x), cy = cos(yaw), sy = sin(yaw);
+    for (int m = 0; m < kNumOffsets; ++m) {
+        const double fo = P.offsets[m][0], lo = P.offsets[m][1];
+        double h = height_at(W, i, o.x.x + cy * fo - sy * lo, o.x.y + sy * fo + cy * lo);
+        double rel = o.x.z - P.stand_height - h;
+        rel = rel < -1.0 ? -1.0 : (rel > 1.0 ? 1.0 : rel);
+        dst[k++] = obs_value(rel);
+    }
+    for (int l = 0; l < kNumLegs; ++l)
+        dst[k++] = obs_value(o.contact[l]);
+}
+
+// Checkpoint 3-6 m away inside the terrain (arc/task.py:127-151), drawn
+// from the device stream; also refreshes target_z, prev_dist, prev_gaze.
+template <class R>
+__device__ void place_target(const TaskParams& P, const Worlds<R>& W, const TaskState& S, int i, V3<double> pos,
+                             const M3<double>& rot)
+{
+    const double limit = P.half_extent - P.border;
+    double tx = 0.5 * pos.x, ty = 0.5 * pos.y;
+    for (int t = 0; t < 20; ++t) {
+        const unsigned k = S.draws[i]++;
+        const double ang = -kPi + 2.0 * kPi * unit(stream_u64(P.seed, i, 1u, 2u * k));
+        const double dist = P.checkpoint_min_dist +
+                            (P.checkpoint_max_dist - P.checkpoint_min_dist) * unit(stream_u64(P.seed, i, 1u, 2u * k + 1u));
+        const double cx = pos.x + dist * cos(ang), cy = pos.y + dist * sin(ang);
+        if (fabs(cx) < limit && fabs(cy) < limit) {
+            tx = cx;
+            ty = cy;
+            break;
+        }
+    }
+    S.target[2 * i] = tx;
+    S.target[2 * i + 1] = ty;
+    S.target_z[i] = height_at(W, i, tx, ty);
+    const double dx = tx - pos.x, dy = ty - pos.y;
+    S.prev_dist[i] = sqrt(dx * dx + dy * dy);
+    S.prev_gaze[i] = gaze_error(rot, pos, S.target + 2 * i);
+    S.in_view[i] = S.prev_gaze[i] < P.fov_rad;
+}
+
+// ---------------------------------------------------------------------------
+// arc/task.py:155-220 (+ 231-259 for the observation): one thread per world
+
+template <class R>
+__global__ void k_task_step(const __grid_constant__ DevModel<R> M, Worlds<R> W, const __grid_constant__ TaskParams P,
+                            TaskState S, TaskOut O, const float* __restrict__ actions, int write_obs_rows)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W.n)
+        return;
+    Obs64 o;
+    read_world(M, W, i, o);
+    const int steps = S.steps[i] + 1;
+    S.steps[i] = steps;
+    const double* tgt = S.target + 2 * i;
+    const double dist = hypot(tgt[0] - o.x.x, tgt[1] - o.x.y);
+    const double gaze = gaze_error(o.rot, o.x, tgt);
+    double view = (cos(gaze) - P.cos_fov) / (1.0 - P.cos_fov);
+    view = view < 0.0 ? 0.0 : (view > 1.0 ? 1.0 : view);
+    const bool in_view = gaze < P.fov_rad;
+    double progress = S.prev_dist[i] - dist;
+    progress = progress < P.max_speed * P.dt ? progress : P.max_speed * P.dt;
+    if (progress > 0)
+        progress = progress * view;
+    const double turn = S.prev_gaze[i] - gaze;
+    const bool reached = dist < P.checkpoint_radius && in_view;
+    const V3<double> br = rt_mul(o.rot, o.w);
+    const bool torso = o.contact[kNumLegs] > 0;
+    const int torso_steps = torso ? S.torso_steps[i] + 1 : 0;
+    S.torso_steps[i] = torso_steps;
+    double power = 0.0, rate = 0.0;
+    float* pa = S.prev_action + (size_t)i * kNumJoints;
+    for (int j = 0; j < kNumJoints; ++j) {
+        power += fabs(o.rate[j] * o.torque[j]);
+        double a = (double)actions[(size_t)i * kNumJoints + j];
+        a = a < -1.0 ? -1.0 : (a > 1.0 ? 1.0 : a);
+        const double d = a - (double)pa[j];
+        rate += d * d;
+        pa[j] = (float)a;
+    }
+    double reward = P.w_progress * progress + P.w_turn * turn + P.w_checkpoint * (reached ? 1.0 : 0.0) - P.w_time -
+                    P.w_energy * power * P.dt - P.w_action_rate * rate -
+                    P.w_body_contact * (o.contact[kNumLegs + 1] > 0 ? 1.0 : 0.0) -
+                    P.w_torso_contact * (torso ? 1.0 : 0.0) - P.w_body_rate * (br.x * br.x + br.y * br.y) -
+                    P.w_bounce * (o.v.z * o.v.z);
+    bool finite = true;
+    {
+        const double r13[13] = {o.x.x, o.x.y, o.x.z, o.q.w, o.q.x, o.q.y, o.q.z,
+                                o.v.x, o.v.y, o.v.z, o.w.x, o.w.y, o.w.z};
+        for (int c = 0; c < 13; ++c)
+            finite = finite && isfinite(r13[c]);
+    }
+    const bool bad = o.unstable != 0 || !finite;
+    const bool vd = fabs(o.x.x) > P.half_extent || fabs(o.x.y) > P.half_extent || o.x.z < P.void_z;
+    const bool flip = o.rot.m[2][2] < P.flip_up_z;
+    const bool beached = torso_steps > P.beached_steps;
+    const bool fell = flip || beached || vd || bad;
+    const int cause = bad ? 1 : (vd ? 2 : (flip ? 3 : (beached ? 4 : 0)));
+    if (fell)
+        reward = reward - P.w_fall;
+    if (bad)
+        reward = -P.w_fall;
+    S.prev_dist[i] = dist;
+    S.prev_gaze[i] = gaze;
+    S.in_view[i] = in_view;
+    const int checkpoints = S.checkpoints[i] + (reached ? 1 : 0);
+    S.checkpoints[i] = checkpoints;
+    if (reached && !fell)
+        place_target(P, W, S, i, o.x, o.rot);
+    const bool truncated = steps >= P.max_steps && !fell;
+    O.reward[i] = (float)reward;
+    O.terminated[i] = fell;
+    O.truncated[i] = truncated;
+    O.cause[i] = (signed char)cause;
+    const bool done = fell || truncated;
+    if (done) {
+        O.ended_checkpoints[i] = checkpoints;
+        O.ended_difficulty[i] = S.difficulty[i];
+        O.ended_steps[i] = steps;
+        if (P.curriculum) {
+            // arc/task.py:222-227
+            const bool up = checkpoints >= P.level_up_checkpoints;
+            const bool down = fell && checkpoints == 0 && steps < P.level_down_steps;
+            double lvl = S.level[i] + P.level_step * ((up ? 1.0 : 0.0) - (down ? 1.0 : 0.0));
+            lvl = rint(lvl * 1e6) / 1e6;
+            S.level[i] = lvl < 0.0 ? 0.0 : (lvl > P.max_difficulty ? P.max_difficulty : lvl);
+        }
+        if (O.done_list)
+            O.done_list[atomicAdd(O.done_count, 1)] = i;
+    }
+    if (write_obs_rows && O.obs) {
+        float* row = O.obs + (size_t)i * kObsSize;
+        write_obs(P, W, S, i, o, row);
+        if (done && O.terminal_obs) {
+            float* t = O.terminal_obs + (size_t)i * kObsSize;
+            for (int k = 0; k < kObsSize; ++k)
+                t[k] = row[k];
+        }
+    }
+}
+
+template <class R>
+__global__ void k_task_observe(const __grid_constant__ DevModel<R> M, Worlds<R> W, const __grid_constant__ TaskParams P,
+                               TaskState S, float* obs, const int* __restrict__ ids, int n)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    const int i = ids ? ids[k] : k;
+    Obs64 o;
+    read_world(M, W, i, o);
+    write_obs(P, W, S, i, o, obs + (size_t)i * kObsSize);
+}
+
+// ---------------------------------------------------------------------------
+// warp-cooperative reset (csrc/arc_sim.c:88-110, csrc/arc_terrain.c:35-71):
+// lane 0 draws the world's RNG stream into shared memory, all lanes build
+// the terrain columns, lane 0 poses the robot.
+
+constexpr int kLat1 = (kGridMax / 8 + 2) * (kGridMax / 8 + 2);   // 100
+constexpr int kLat2 = (kGridMax / 3 + 2) * (kGridMax / 3 + 2);   // 529
+constexpr int kMaxDraws = kLat1 + kLat2 + kGridMax * kGridMax + kMaxJoints + 1;
+
+struct ResetSmem {
+    uint32_t draws[kMaxDraws];
+    double lat[kLat1 + kLat2];
+};
+
+// The generator's arithmetic is written with explicitly rounded FP64
+// operations (no FMA contraction): the quantisation to 0.03 m steps and the
+// base shift must see the reference's roundings bit for bit
+// (csrc/arc_terrain.c:84-123 evaluates each operation separately).
+__device__ __forceinline__ double smooth(double t)
+{
+    return __dmul_rn(__dmul_rn(t, t), __dsub_rn(3.0, __dmul_rn(2.0, t)));
+}
+
+__device__ __forceinline__ double noise_at(const double* lat, int m, int spacing, int ix, int iy)
+{
+    double fx = __ddiv_rn((double)ix, (double)spacing), fy = __ddiv_rn((double)iy, (double)spacing);
+    int gx = (int)fx, gy = (int)fy;
+    double tx = smooth(__dsub_rn(fx, (double)gx)), ty = smooth(__dsub_rn(fy, (double)gy));
+    double a = lat[gx + gy * m], b = lat[gx + 1 + gy * m];
+    double c = lat[gx + (gy + 1) * m], d = lat[gx + 1 + (gy + 1) * m];
+    double top = __dadd_rn(a, __dmul_rn(__dsub_rn(b, a), tx));
+    double bot = __dadd_rn(c, __dmul_rn(__dsub_rn(d, c), tx));
+    return __dadd_rn(__dmul_rn(top, __dsub_rn(1.0, ty)), __dmul_rn(bot, ty));
+}
+
+// one column: hills + bumps + jitter, quantised (csrc/arc_terrain.c:93-118)
+__device__ __forceinline__ double column_height(const double* lat1, int m1, const double* lat2, int m2, int ix,
+                                                int iy, double amp1, double amp2, double ampj, uint32_t draw)
+{
+    double v = __dadd_rn(0.0, __dmul_rn(amp1, noise_at(lat1, m1, 8, ix, iy)));
+    v = __dadd_rn(v, __dmul_rn(amp2, noise_at(lat2, m2, 3, ix, iy)));
+    const double u = __dmul_rn((double)draw, 1.0 / 4294967296.0);
+    const double jitter = __dadd_rn(-1.0, __dmul_rn(2.0, u));
+    const double hj = __dadd_rn(v, __dmul_rn(ampj, jitter));
+    return __dmul_rn(0.03, floor(__dadd_rn(__ddiv_rn(hj, 0.03), 0.5)));
+}
+
+__device__ __forceinline__ unsigned long long scan_cells(double reach, double step, double o, double cell, int n,
+                                                         bool& outside)
+{
+    unsigned long long mask = 0;
+    for (double x = -reach; x <= reach; x += step) {
+        double f = floor((x - o) / cell);
+        if (f >= 0.0 && f < n)
+            mask |= 1ull << (int)f;
+        else
+            outside = true;
+    }
+    return mask;
+}
+
+template <class R>
+__device__ void reset_world_warp(ResetSmem& sm, const ResetModel& RM, const Worlds<R>& W, TerrainGeom<R>* tg,
+                                 TerrainGeomD* tgd, int i, uint32_t seed, double diff, int n, double cell)
+{
+    const int lane = threadIdx.x & 31;
+    n = n < kGridMax ? n : kGridMax;
+    const bool rough = diff > 0.0;
+    const int m1 = n / 8 + 2, m2 = n / 3 + 2;
+    const int L = rough ? m1 * m1 + m2 * m2 : 0;
+    const int J = rough ? n * n : 0;
+    const int total = L + J + RM.nj + 1;
+    if (lane == 0) {
+        Xorshift rng;
+        rng.seed(seed);
+        for (int k = 0; k < total; ++k)
+            sm.draws[k] = rng.next();
+    }
+    __syncwarp();
+    for (int k = lane; k < L; k += 32)
+        sm.lat[k] = __dadd_rn(-1.0, __dmul_rn(2.0, __dmul_rn((double)sm.draws[k], 1.0 / 4294967296.0)));
+    __syncwarp();
+
+    TerrainGeomD g;
+    g.nx = g.ny = n;
+    g.cell = cell;
+    g.ox = -0.5 * n * cell;
+    g.oy = -0.5 * n * cell;
+    g.outside = -100.0;
+    if (lane == 0) {
+        tgd[i] = g;
+        tg[i] = TerrainGeom<R>{n, n, (R)g.cell, (R)g.ox, (R)g.oy, (R)g.outside};
+    }
+    R* h = W.th + W.toff[i];
+    const double reach = RM.footprint + 0.1, step = 0.5 * cell;
+    bool out_x = false, out_y = false;
+    const unsigned long long mx = scan_cells(reach, step, g.ox, cell, n, out_x);
+    const unsigned long long my = scan_cells(reach, step, g.oy, cell, n, out_y);
+    double ground = (out_x || out_y) ? g.outside : -1e30;
+    if (!rough) {
+        for (int c = lane; c < n * n; c += 32)
+            h[c] = R(0);
+        if (mx && my)
+            ground = ground > 0.0 ? ground : 0.0;
+    } else {
+        const double amp1 = __dmul_rn(0.45, diff), amp2 = __dmul_rn(0.12, diff), ampj = __dmul_rn(0.06, diff);
+        const double* lat1 = sm.lat;
+        const double* lat2 = sm.lat + m1 * m1;
+        const double f0x = floor((0.0 - g.ox) / g.cell), f0y = floor((0.0 - g.oy) / g.cell);
+        double base = g.outside;
+        if (f0x >= 0.0 && f0y >= 0.0 && f0x < n && f0y < n) {
+            const int ix = (int)f0x, iy = (int)f0y;
+            base = column_height(lat1, m1, lat2, m2, ix, iy, amp1, amp2, ampj, sm.draws[L + ix + iy * n]);
+        }
+        double gmax = -1e300;
+        for (int c = lane; c < n * n; c += 32) {
+            const int ix = c % n, iy = c / n;
+            const double hf =
+                __dsub_rn(column_height(lat1, m1, lat2, m2, ix, iy, amp1, amp2, ampj, sm.draws[L + c]), base);
+            h[c] = (R)hf;
+            if (((mx >> ix) & 1) && ((my >> iy) & 1))
+                gmax = gmax > hf ? gmax : hf;
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            double o = __shfl_xor_sync(0xffffffffu, gmax, off);
+            gmax = gmax > o ? gmax : o;
+        }
+        if (mx && my)
+            ground = ground > gmax ? ground : gmax;
+    }
+    if (lane != 0)
+        return;
+
+    // noisy stance, yaw, forward kinematics (csrc/arc_sim.c:99-109, csrc/arc_phys.c:749-782)
+    double angles[kMaxJoints];
+    for (int j = 0; j < RM.nj; ++j) {
+        double a = RM.default_angles[j] + range_of(sm.draws[L + J + j], -0.1, 0.1);
+        angles[j] = a < RM.lo[j] ? RM.lo[j] : (a > RM.hi[j] ? RM.hi[j] : a);
+    }
+    const double yaw = range_of(sm.draws[L + J + RM.nj], -kPi, kPi);
+    V3<double> xs[kMaxBodies];
+    Q4<double> qs[kMaxBodies];
+    const double sy = sin(0.5 * yaw), cyw = cos(0.5 * yaw);
+    xs[0] = V3<double>{0.0, 0.0, ground + RM.stand_height + 0.03};
+    qs[0] = qnormalize(Q4<double>{cyw, 0.0 * sy, 0.0 * sy, 1.0 * sy});
+    for (int j = 0; j < RM.nj; ++j) {
+        const int p = RM.parent[j], c = RM.child[j];
+        V3<double> xp = p >= 0 ? xs[p] : V3<double>{0.0, 0.0, 0.0};
+        Q4<double> qp = p >= 0 ? qs[p] : q_identity<double>();
+        V3<double> anchor = xp + qrotate(qp, RM.r1[j]);
+        const double s = sin(0.5 * angles[j]), ca = cos(0.5 * angles[j]);
+        Q4<double> qa{ca, RM.a1[j].x * s, RM.a1[j].y * s, RM.a1[j].z * s};
+        qs[c] = qnormalize(qmul(qp, qmul(qa, RM.q_rel0[j])));
+        xs[c] = anchor - qrotate(qs[c], RM.r2[j]);
+    }
+    R* rec = W.rec + (size_t)i * W.stride;
+    for (int b = 0; b < RM.nb; ++b) {
+        R* r = rec + b * kBodyRec;
+        r[0] = (R)xs[b].x; r[1] = (R)xs[b].y; r[2] = (R)xs[b].z;
+        r[3] = (R)qs[b].w; r[4] = (R)qs[b].x; r[5] = (R)qs[b].y; r[6] = (R)qs[b].z;
+        for (int c = 7; c < 13; ++c)
+            r[c] = R(0);
+    }
+    R* sr = rec + W.off_sphere;
+    uint32_t* sph = W.sph + (size_t)i * RM.ns;
+    for (int s = 0; s < RM.ns; ++s) {
+        for (int c = 0; c < kSphereRec; ++c)
+            sr[s * kSphereRec + c] = R(0);
+        sph[s] = 0;
+    }
+    R* jr = rec + W.off_joint;
+    for (int j = 0; j < RM.nj; ++j) {
+        jr[j * kJointRec + 0] = (R)angles[j];
+        jr[j * kJointRec + 1] = (R)angles[j];
+        jr[j * kJointRec + 2] = R(0);
+        jr[j * kJointRec + 3] = R(0);
+    }
+    W.unstable[i] = 0;
+    W.time[i] = 0.0;
+}
+
+template <class R>
+__global__ void __launch_bounds__(32)
+k_reset_warp(const __grid_constant__ ResetModel RM, Worlds<R> W, TerrainGeom<R>* tg, TerrainGeomD* tgd,
+             const int* __restrict__ ids, int n_ids, const unsigned* __restrict__ seeds,
+             const double* __restrict__ difficulty, const int* __restrict__ grid_of, double cell)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ResetSmem& sm = *reinterpret_cast<ResetSmem*>(smem_raw);
+    for (int k = blockIdx.x; k < n_ids; k += gridDim.x) {
+        const int i = ids[k];
+        reset_world_warp(sm, RM, W, tg, tgd, i, seeds[k], difficulty[k], grid_of ? grid_of[i] : kGridMax, cell);
+        __syncwarp();
+    }
+}
+
+// ArcTask.reset (arc/task.py:113-125) + the observation of the new episode
+template <class R>
+__global__ void __launch_bounds__(32)
+k_task_reset(const __grid_constant__ DevModel<R> M, const __grid_constant__ ResetModel RM, Worlds<R> W,
+             TerrainGeom<R>* tg, TerrainGeomD* tgd, const int* __restrict__ grid_of, double cell,
+             const __grid_constant__ TaskParams P, TaskState S, float* obs, const int* __restrict__ ids,
+             const int* __restrict__ count_dev, int max_n)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ResetSmem& sm = *reinterpret_cast<ResetSmem*>(smem_raw);
+    const int n = count_dev ? min(*count_dev, max_n) : max_n;
+    const int lane = threadIdx.x & 31;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int i = ids[k];
+        uint32_t seed = 0;
+        if (lane == 0) {
+            const unsigned e = S.episode[i]++;
+            seed = (uint32_t)stream_u64(P.seed, i, 2u, e);
+            S.difficulty[i] = S.level[i];
+        }
+        seed = __shfl_sync(0xffffffffu, seed, 0);
+        __syncwarp();
+        reset_world_warp(sm, RM, W, tg, tgd, i, seed, S.difficulty[i], grid_of ? grid_of[i] : kGridMax, cell);
+        __syncwarp();
+        if (lane == 0) {
+            for (int j = 0; j < kNumJoints; ++j)
+                S.prev_action[(size_t)i * kNumJoints + j] = 0.0f;
+            S.torso_steps[i] = 0;
+            S.steps[i] = 0;
+            S.checkpoints[i] = 0;
+            Obs64 o;
+            read_world(M, W, i, o);
+            place_target(P, W, S, i, o.x, o.rot);
+            if (obs)
+                write_obs(P, W, S, i, o, obs + (size_t)i * kObsSize);
+        }
+        __syncwarp();
+    }
+}
+
+template <class R>
+__global__ void k_task_set_targets(Worlds<R> W, const __grid_constant__ TaskParams P, TaskState S,
+                                   const int* __restrict__ ids, const double* __restrict__ xy, int n)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    const int i = ids[k];
+    const R* rec = W.rec + (size_t)i * W.stride;
+    V3<double> pos{(double)rec[0], (double)rec[1], (double)rec[2]};
+    Q4<double> q{(double)rec[3], (double)rec[4], (double)rec[5], (double)rec[6]};
+    M3<double> rot = m3_from_quat(q);
+    const double tx = xy[2 * k], ty = xy[2 * k + 1];
+    S.target[2 * i] = tx;
+    S.target[2 * i + 1] = ty;
+    S.target_z[i] = height_at(W, i, tx, ty);
+    const double dx = tx - pos.x, dy = ty - pos.y;
+    S.prev_dist[i] = sqrt(dx * dx + dy * dy);
+    S.prev_gaze[i] = gaze_error(rot, pos, S.target + 2 * i);
+    S.in_view[i] = S.prev_gaze[i] < P.fov_rad;
+}
+
+int reset_grid(int n)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int cap = sms * 8;
+    return n < cap ? (n > 0 ? n : 1) : cap;
+}
+
+}  // namespace
+
+template <class R>
+cudaError_t launch_task_step(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskState& S,
+                             const TaskOut& O, const float* actions, int write_obs_rows, cudaStream_t stream)
+{
+    if (W.n <= 0)
+        return cudaSuccess;
+    k_task_step<R><<<(W.n + 127) / 128, 128, 0, stream>>>(M, W, P, S, O, actions, write_obs_rows);
+    return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t launch_task_observe(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskState& S,
+                                float* obs, const int* ids, int n_ids, cudaStream_t stream)
+{
+    if (n_ids <= 0)
+        return cudaSuccess;
+    k_task_observe<R><<<(n_ids + 127) / 128, 128, 0, stream>>>(M, W, P, S, obs, ids, n_ids);
+    return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t launch_task_reset(const DevModel<R>& M, const ResetModel& RM, const Worlds<R>& W, TerrainGeom<R>* tg,
+                              TerrainGeomD* tgd, const int* grid_of, double cell, const TaskParams& P,
+                              const TaskState& S, float* obs, const int* ids, const int* count_dev, int max_n,
+                              cudaStream_t stream)
+{
+    if (max_n <= 0)
+        return cudaSuccess;
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_task_reset<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sizeof(ResetSmem));
+        if (e != cudaSuccess)
+            return e;
+        configured = true;
+    }
+    k_task_reset<R><<<reset_grid(max_n), 32, sizeof(ResetSmem), stream>>>(M, RM, W, tg, tgd, grid_of, cell, P, S, obs,
+                                                                       ids, count_dev, max_n);
+    return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t launch_task_set_targets(const Worlds<R>& W, const TaskParams& P, const TaskState& S, const int* ids,
+                                    const double* xy, int n, cudaStream_t stream)
+{
+    if (n <= 0)
+        return cudaSuccess;
+    k_task_set_targets<R><<<(n + 127) / 128, 128, 0, stream>>>(W, P, S, ids, xy, n);
+    return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t launch_reset_warp(const ResetModel& RM, const Worlds<R>& W, TerrainGeom<R>* tg, TerrainGeomD* tgd,
+                              const int* ids, int n_ids, const unsigned* seeds, const double* difficulty,
+                              const int* grid_of, double cell, cudaStream_t stream)
+{
+    if (n_ids <= 0)
+        return cudaSuccess;
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_reset_warp<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sizeof(ResetSmem));
+        if (e != cudaSuccess)
+            return e;
+        configured = true;
+    }
+    k_reset_warp<R><<<reset_grid(n_ids), 32, sizeof(ResetSmem), stream>>>(RM, W, tg, tgd, ids, n_ids, seeds,
+                                                                        difficulty, grid_of, cell);
+    return cudaGetLastError();
+}
+
+#define ARC_INSTANTIATE_TASK(R)                                                                                    \
+    template cudaError_t launch_task_step<R>(const DevModel<R>&, const Worlds<R>&, const TaskParams&,            \
+                                             const TaskState&, const TaskOut&, const float*, int, cudaStream_t); \
+    template cudaError_t launch_task_observe<R>(const DevModel<R>&, const Worlds<R>&, const TaskParams&,         \
+                                                const TaskState&, float*, const int*, int, cudaStream_t);        \
+    template cudaError_t launch_task_reset<R>(const DevModel<R>&, const ResetModel&, const Worlds<R>&,           \
+                                              TerrainGeom<R>*, TerrainGeomD*, const int*, double,                \
+                                              const TaskParams&, const TaskState&, float*, const int*,           \
+                                              const int*, int, cudaStream_t);                                    \
+    template cudaError_t launch_task_set_targets<R>(const Worlds<R>&, const TaskParams&, const TaskState&,       \
+                                                    const int*, const double*, int, cudaStream_t);               \
+    template cudaError_t launch_reset_warp<R>(const ResetModel&, const Worlds<R>&, TerrainGeom<R>*,              \
+                                              TerrainGeomD*, const int*, int, const unsigned*, const double*,    \
+                                              const int*, double, cudaStream_t);
+
+ARC_INSTANTIATE_TASK(float)
+ARC_INSTANTIATE_TASK(double)
+
+}  // namespace arc

@@ -1,0 +1,93 @@
+// arc_task.cuh - the task layer on the device: observations, rewards,
+// terminations, checkpoints and the terrain curriculum of the reference's
+// arc/task.py (ArcTask), computed in FP64 from the step-precision state.
+#pragma once
+
+#include "arc_kernels.cuh"
+
+namespace arc {
+
+constexpr int kNumOffsets = 143;                 // arc/task.py:74-76: 13 forward x 11 left
+constexpr int kObsSize = 9 + 3 * kNumJoints + 3 + kNumOffsets + kNumLegs;  // 195
+
+// TaskConfig (arc/task.py:17-66) plus derived constants.
+struct TaskParams {
+    double dt;
+    int max_steps;
+    double action_scale, checkpoint_radius, checkpoint_min_dist, checkpoint_max_dist, border;
+    double w_progress, max_speed, fov, w_turn, w_checkpoint, w_time, w_fall, w_energy, w_action_rate;
+    double w_body_contact, w_torso_contact, w_body_rate, w_bounce;
+    double flip_up_z;
+    int beached_steps;
+    double void_z;
+    int curriculum;
+    double difficulty, max_difficulty, level_step;
+    int level_up_checkpoints, level_down_steps;
+    // derived
+    double cos_fov, fov_rad, half_extent, stand_height;
+    double default_angles[kNumJoints];
+    double offsets[kNumOffsets][2];
+    unsigned long long seed;  // device RNG stream of resets and checkpoint draws
+};
+
+// Per-world task state (the ArcTask arrays, arc/task.py:96-109), device arrays.
+struct TaskState {
+    double* target;       // [N][2]
+    double* target_z;     // [N]
+    double* prev_dist;    // [N]
+    double* prev_gaze;    // [N]
+    float* prev_action;   // [N][12] (clipped float32 actions: exact in float)
+    int* torso_steps;     // [N]
+    int* steps;           // [N]
+    int* checkpoints;     // [N]
+    double* level;        // [N]
+    double* difficulty;   // [N]
+    unsigned char* in_view;  // [N]
+    unsigned* episode;    // [N] resets so far (device RNG counter)
+    unsigned* draws;      // [N] checkpoint draws so far (device RNG counter)
+};
+
+// Outputs of one env step, device arrays.
+struct TaskOut {
+    float* obs;            // [N][195]
+    float* terminal_obs;   // [N][195], rows of worlds that ended this step
+    float* reward;         // [N]
+    unsigned char* terminated, *truncated;  // [N]
+    signed char* cause;    // [N] index into ("", unstable, void, flip, beached)
+    int* ended_checkpoints;   // [N] episode stats of worlds that ended this step
+    double* ended_difficulty; // [N]
+    int* ended_steps;         // [N]
+    int* done_list;        // [N] worlds that ended this step
+    int* done_count;       // [1]
+};
+
+template <class R>
+cudaError_t launch_task_step(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskState& S,
+                             const TaskOut& O, const float* actions, int write_obs, cudaStream_t stream);
+
+template <class R>
+cudaError_t launch_task_observe(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskState& S,
+                                float* obs, const int* ids, int n_ids, cudaStream_t stream);
+
+// Task reset of worlds (arc/task.py:113-125): device-drawn seeds, terrain,
+// pose, task state, a checkpoint, and their observations. ids == nullptr
+// with count_dev != nullptr: the worlds listed in done_list[0..*count_dev).
+template <class R>
+cudaError_t launch_task_reset(const DevModel<R>& M, const ResetModel& RM, const Worlds<R>& W, TerrainGeom<R>* tg,
+                              TerrainGeomD* tgd, const int* grid_of, double cell, const TaskParams& P,
+                              const TaskState& S, float* obs, const int* ids, const int* count_dev, int max_n,
+                              cudaStream_t stream);
+
+// Checkpoints at given points (host-injected; parity tests and callers that
+// draw their own): target, target_z, prev_dist, prev_gaze, in_view.
+template <class R>
+cudaError_t launch_task_set_targets(const Worlds<R>& W, const TaskParams& P, const TaskState& S, const int* ids,
+                                    const double* xy, int n, cudaStream_t stream);
+
+// Warp-cooperative reset used by arc_sim_reset: seeds and difficulties given.
+template <class R>
+cudaError_t launch_reset_warp(const ResetModel& RM, const Worlds<R>& W, TerrainGeom<R>* tg, TerrainGeomD* tgd,
+                              const int* ids, int n_ids, const unsigned* seeds, const double* difficulty,
+                              const int* grid_of, double cell, cudaStream_t stream);
+
+}  // namespace arc

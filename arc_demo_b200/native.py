@@ -73,6 +73,8 @@ def sim_lib() -> ctypes.CDLL:
     d("arc_sim_set_kernel", _int, _vp, _int, _int)
     d("arc_sim_get_kernel", _int, _vp, ctypes.POINTER(_int), ctypes.POINTER(_int))
     d("arc_sim_real_size", _int, _vp)
+    d("arc_sim_model_info", _int, _vp, ctypes.POINTER(_int), ctypes.POINTER(_int), ctypes.POINTER(_int),
+      ctypes.POINTER(_int))
     d("arc_sim_state_size", _int, _vp)
     d("arc_sim_get_state", _int, _vp, _i32, _int, _f64)
     d("arc_sim_set_state", _int, _vp, _i32, _int, _f64)
@@ -89,6 +91,7 @@ def sim_lib() -> ctypes.CDLL:
     d("arc_sim_set_pose", _int, _vp, _int, _f64, _f64, _vp)
     d("arc_sim_stream", _vp, _vp)
     d("arc_sim_step_device", _int, _vp, _vp, _vp)
+    d("arc_sim_step_actions", _int, _vp, _vp, _vp)
     d("arc_sim_observe_device", _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp)
     d("arc_sim_synchronize", _int, _vp)
     return lib
@@ -150,11 +153,18 @@ class Sim:
         if not self._ptr:
             raise MemoryError("arc_sim_create failed (no CUDA device, or out of memory)")
         self._lib.arc_sim_set_threads(self._ptr, int(threads))
+        nb, nj_, ns, nch = _int(), _int(), _int(), _int()
+        self._lib.arc_sim_model_info(self._ptr, ctypes.byref(nb), ctypes.byref(nj_), ctypes.byref(ns),
+                                     ctypes.byref(nch))
+        self.num_bodies, self.num_spheres, self.num_channels = nb.value, ns.value, nch.value
+        if model is not None:
+            self.num_joints = nj_.value
 
         nj = self.num_joints
-        self.default_angles = np.zeros(nj)
-        self.lo, self.hi, misc = np.zeros(nj), np.zeros(nj), np.zeros(2)
+        self.default_angles = np.zeros(max(nj, 12))
+        self.lo, self.hi, misc = np.zeros(max(nj, 12)), np.zeros(max(nj, 12)), np.zeros(2)
         self._lib.arc_sim_robot_info(self._ptr, self.default_angles, self.lo, self.hi, misc)
+        self.default_angles, self.lo, self.hi = self.default_angles[:nj], self.lo[:nj], self.hi[:nj]
         self.stand_height = float(misc[0])
         self.total_mass = float(misc[1])
         self.state_size = self._lib.arc_sim_state_size(self._ptr)
@@ -163,7 +173,7 @@ class Sim:
         self.root = np.zeros((num_worlds, ROOT_SIZE))
         self.rot = np.zeros((num_worlds, 3, 3))
         self.joints = np.zeros((num_worlds, 3 * nj))
-        self.contacts = np.zeros((num_worlds, self.num_legs + 2))
+        self.contacts = np.zeros((num_worlds, self.num_channels if model is not None else self.num_legs + 2))
         self.flags = np.zeros(num_worlds, dtype=np.int32)
         self._observe_args = (self._ptr, self.root.ctypes.data, self.rot.ctypes.data,
                               self.joints.ctypes.data, self.contacts.ctypes.data,

@@ -1,0 +1,97 @@
+"""Device-resident vectorised env over libarcsim.so, for PyTorch training loops.
+
+`DeviceVecEnv` runs ArcVecEnv.step_wait's work (arc/env.py:99-117) on the GPU:
+actuation, physics, rewards, terminations, checkpoints, curriculum,
+observations and the auto-reset of ended worlds, in one CUDA graph per
+control step. Observations, rewards and done flags are torch tensors that
+alias the library's device buffers through DLPack: no copies, no host
+round trip. Torch is only the consumer here; the step itself is the
+library's CUDA kernels.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from .native import Sim
+from .task import (ACTIONS, CAUSE, DONE_COUNT, DONE_LIST, ENDED_CHECKPOINTS, ENDED_DIFFICULTY, ENDED_STEPS, OBS,
+                   REWARD, TERMINAL_OBS, TERMINATED, TRUNCATED, GpuTask, TaskConfig)
+
+_capsule_new = ctypes.pythonapi.PyCapsule_New
+_capsule_new.restype = ctypes.py_object
+_capsule_new.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
+
+CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: torch's default stream has handle 0
+
+
+def stream_handle(stream: torch.cuda.Stream | None = None) -> int:
+    s = (stream or torch.cuda.current_stream()).cuda_stream
+    return s if s else CUDA_STREAM_LEGACY
+
+
+def dlpack_tensor(gpu: GpuTask, which: int) -> torch.Tensor:
+    """A torch tensor aliasing one of the library's device buffers."""
+    p = ctypes.c_void_p()
+    gpu.sim._check(gpu.lib.arc_env_dlpack(gpu.sim.ptr, which, ctypes.byref(p)))
+    return torch.utils.dlpack.from_dlpack(_capsule_new(p, b"dltensor", None))
+
+
+class DeviceVecEnv:
+    def __init__(self, num_envs: int, config: TaskConfig | None = None, seed: int = 0, *, fp64: bool = False,
+                 kernel: int | None = None, worlds_per_cta: int = 16):
+        self.cfg = cfg = config or TaskConfig()
+        self.num_envs = num_envs
+        self.sim = Sim(num_envs, cfg.dt, cfg.substeps, cfg.grid, cfg.cell, fp64=fp64)
+        if kernel is not None:
+            self.sim.set_kernel(kernel, worlds_per_cta)
+        self.gpu = GpuTask(self.sim, cfg, seed)
+        self.obs = dlpack_tensor(self.gpu, OBS)
+        self.terminal_obs = dlpack_tensor(self.gpu, TERMINAL_OBS)
+        self.reward = dlpack_tensor(self.gpu, REWARD)
+        self.terminated = dlpack_tensor(self.gpu, TERMINATED)
+        self.truncated = dlpack_tensor(self.gpu, TRUNCATED)
+        self.cause = dlpack_tensor(self.gpu, CAUSE)
+        self.actions = dlpack_tensor(self.gpu, ACTIONS)
+        self.done_list = dlpack_tensor(self.gpu, DONE_LIST)
+        self.done_count = dlpack_tensor(self.gpu, DONE_COUNT)
+        self.ended_checkpoints = dlpack_tensor(self.gpu, ENDED_CHECKPOINTS)
+        self.ended_steps = dlpack_tensor(self.gpu, ENDED_STEPS)
+        self.ended_difficulty = dlpack_tensor(self.gpu, ENDED_DIFFICULTY)
+
+    def set_kernel(self, kernel: int, worlds_per_cta: int = 16) -> None:
+        self.sim.set_kernel(kernel, worlds_per_cta)
+
+    def set_levels(self, levels) -> None:
+        """Per-world terrain difficulty levels (the curriculum state)."""
+        import numpy as np
+        st = self.gpu.get_state()
+        st[:, 20] = np.asarray(levels, dtype=np.float64)
+        st[:, 21] = st[:, 20]
+        self.gpu.set_state(st)
+
+    def reset(self) -> torch.Tensor:
+        self.sim._check(self.gpu.lib.arc_env_reset(self.sim.ptr, None, -1, ctypes.c_void_p(stream_handle())))
+        return self.obs
+
+    def step(self, actions: torch.Tensor | None = None, *, graph: bool = True):
+        """One control step of every world on the current torch stream.
+
+        actions: N x 12 float32 on the device, or None when the policy
+        already wrote `self.actions`. Returns (obs, reward, terminated,
+        truncated) views; ended worlds are already reset, their last
+        observation is in `terminal_obs`."""
+        st = ctypes.c_void_p(stream_handle())
+        if graph:
+            if actions is not None:
+                self.actions.copy_(actions)
+            rc = self.gpu.lib.arc_env_step(self.sim.ptr, None, st)
+        else:
+            a = self.actions if actions is None else actions.contiguous()
+            rc = self.gpu.lib.arc_env_step(self.sim.ptr, ctypes.c_void_p(a.data_ptr()), st)
+        self.sim._check(rc)
+        return self.obs, self.reward, self.terminated, self.truncated
+
+    def close(self) -> None:
+        self.sim.close()

@@ -1,0 +1,454 @@
+#!/usr/bin/env python
+"""Throughput of the B200 batched world step (arc-demo's quadruped task).
+
+Workload (the configuration the headline metric is quoted on): 65,536
+worlds of the quadruped, terrain difficulty uniform in {0, 0.1, ..., 1.0}
+per world, seeded synthetic terrain from the reference's generator,
+checkpoints drawn as the reference draws them, auto-reset on termination or
+after 1,000 steps, actions from a random-init MLP policy (195 -> 256 -> 256
+-> 12, tanh, FP32) that reads the observations in place. One step = one
+control step (20 XPBD substeps of 1/600 s) of every world: actuation,
+physics, rewards, terminations, checkpoints, curriculum bookkeeping,
+observations, resets; plus the policy forward that produces its actions.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). `value` is device-resident throughput (the
+step is a CUDA graph of the library's kernels on a stream shared with the
+policy); `e2e` is the same loop through the host-buffer API (actions copied
+in, observations/rewards/dones copied out every step). `--impl reference`
+times the reference's own CPU path (its csrc/ built by oracle/Makefile, run
+with OpenMP on every host core) plus the task layer, on a bounded sample.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "env-steps/s at 65536 worlds vs plain GPU kernel and OpenMP; p50/p99 step lat"
+WORLDS = 65536
+FLOP_PER_ENV_STEP = 415.6e3   # scalar FP ops of one control step, counted on the reference
+HBM_BYTES_PER_ENV_STEP = 3.9e3  # algorithmic HBM traffic of one env-step (state, actions, obs)
+
+
+def parse():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=300)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--worlds", type=int, default=WORLDS)
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--wpc", type=int, default=0, help="worlds per CTA (0: autotune)")
+    p.add_argument("--no-plain", action="store_true")
+    return p.parse_args()
+
+
+def levels_for(n: int, seed: int) -> np.ndarray:
+    """Difficulty uniform in {0, 0.1, ..., 1.0} per world."""
+    return np.random.default_rng(seed).integers(0, 11, n) / 10.0
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1])]
+        loaded = [v for v, r in zip(sm, rows) if (num(r[3]) or 0) > 300] or sm
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip().lower() == "active"})
+        return {"sm_mhz": float(np.median(loaded)) if loaded else None,
+                "sm_max_mhz": num(rows[0][2]), "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+
+def make_policy(torch, seed: int):
+    g = torch.Generator(device="cpu").manual_seed(seed)
+
+    def lin(i, o):
+        bound = 1.0 / np.sqrt(i)
+        w = (torch.rand(o, i, generator=g) * 2 - 1) * bound
+        b = (torch.rand(o, generator=g) * 2 - 1) * bound
+        return w.cuda().contiguous(), b.cuda().contiguous()
+    return [lin(195, 256), lin(256, 256), lin(256, 12)]
+
+
+def policy_forward(torch, params, obs, out):
+    """MLP 195-256-256-12 with tanh, FP32; writes the actions into `out`."""
+    (w1, b1), (w2, b2), (w3, b3) = params
+    h = torch.tanh(torch.addmm(b1, obs, w1.t()))
+    h = torch.tanh(torch.addmm(b2, h, w2.t()))
+    torch.addmm(b3, h, w3.t(), out=out)
+
+
+def autotune(env, torch, stream, candidates=(8, 16, 32), steps=4):
+    """Worlds-per-CTA of the leg-parallel kernel, by timing the step kernel."""
+    from arc_demo_b200.native import KERNEL_LEGS
+    lib, ptr = env.sim._lib, env.sim.ptr
+    best, table = None, {}
+    for wpc in candidates:
+        env.set_kernel(KERNEL_LEGS, wpc)
+        a = ctypes.c_void_p(env.actions.data_ptr())
+        st = ctypes.c_void_p(stream.cuda_stream)
+        for _ in range(2):
+            lib.arc_sim_step_actions(ptr, a, st)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            lib.arc_sim_step_actions(ptr, a, st)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        table[wpc] = round(ms, 4)
+        if best is None or ms < table[best]:
+            best = wpc
+    env.set_kernel(KERNEL_LEGS, best)
+    return best, table
+
+
+def run_ours(args) -> dict | None:
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    torch.backends.cuda.matmul.allow_tf32 = False
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from arc_demo_b200.native import KERNEL_LEGS, KERNEL_PLAIN, sim_lib
+    from arc_demo_b200.task import TaskConfig
+    from arc_demo_b200.torch_env import DeviceVecEnv
+
+    n = args.worlds
+    cfg = TaskConfig(curriculum=False)
+    env = DeviceVecEnv(n, cfg, seed=1000 + rank)
+    env.set_levels(levels_for(n, 17 + rank))
+    stream = torch.cuda.Stream()
+    params = make_policy(torch, 1234)
+    with torch.cuda.stream(stream):
+        env.reset()
+        torch.nn.init.uniform_(env.actions, -1.0, 1.0)
+        if args.wpc:
+            env.set_kernel(KERNEL_LEGS, args.wpc)
+            best_wpc, tune = args.wpc, None
+        else:
+            best_wpc, tune = autotune(env, torch, stream)
+        env.reset()
+
+        def one_step():
+            policy_forward(torch, params, env.obs, env.actions)
+            env.step()
+
+        for _ in range(max(args.warmup, 3)):
+            one_step()
+        stream.synchronize()
+        if dist:
+            dist.barrier()
+        K = args.steps
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        with ClockSampler(local) as clocks:
+            torch.cuda.synchronize()
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for k in range(K):
+                starts[k].record(stream)
+                one_step()
+                ends[k].record(stream)
+            t1.record(stream)
+            t1.synchronize()
+            torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ms_total = t0.elapsed_time(t1)
+        if dist:
+            t = torch.tensor([ms_total], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_total = float(t.item())
+        lat = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
+        clock = clocks.summary()
+        ended = int(env.done_count.item())
+
+        # the dominant kernel alone: the leg-parallel step, same stream
+        lib, ptr = env.sim._lib, env.sim.ptr
+        a = ctypes.c_void_p(env.actions.data_ptr())
+        st = ctypes.c_void_p(stream.cuda_stream)
+        M = 10
+        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k0.record(stream)
+        for _ in range(M):
+            lib.arc_sim_step_actions(ptr, a, st)
+        k1.record(stream)
+        k1.synchronize()
+        step_kernel_ms = k0.elapsed_time(k1) / M
+
+        # the plain per-world kernel on the same loop (the baseline form)
+        plain = None
+        if rank == 0 and not args.no_plain:
+            env.set_kernel(KERNEL_PLAIN)
+            for _ in range(2):
+                one_step()
+            Kp = max(3, min(10, K))
+            p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            p0.record(stream)
+            for _ in range(Kp):
+                one_step()
+            p1.record(stream)
+            p1.synchronize()
+            plain_ms = p0.elapsed_time(p1) / Kp
+            q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            q0.record(stream)
+            for _ in range(3):
+                lib.arc_sim_step_actions(ptr, a, st)
+            q1.record(stream)
+            q1.synchronize()
+            plain_kernel_ms = q0.elapsed_time(q1) / 3
+            plain = {"ms_per_step": round(plain_ms, 3), "env_steps_per_s": round(n / plain_ms * 1e3),
+                     "step_kernel_ms": round(plain_kernel_ms, 3)}
+            env.set_kernel(KERNEL_LEGS, best_wpc)
+
+        e2e = None if args.no_e2e else run_e2e(torch, env, params, stream, max(3, min(K, 50)))
+
+    peak = ctypes.c_double(0.0)
+    sim_lib().arc_probe_fp32_peak(ctypes.byref(peak), None)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+
+    value = world * n * K / (ms_total * 1e-3)
+    achieved = n * FLOP_PER_ENV_STEP / (step_kernel_ms * 1e-3)
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": "env-steps/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": round(ms_total / K, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{n} worlds of the quadruped per GPU, difficulty uniform in {{0,...,1.0}}, "
+                               "checkpoints, auto-reset, random-init MLP policy 195-256-256-12 tanh FP32 in the loop",
+                   "worlds_per_gpu": n, "substeps": 20, "dt": 1 / 30, "kernel": "leg-parallel",
+                   "worlds_per_cta": best_wpc, "autotune_step_kernel_ms": tune,
+                   "l2": "inputs larger than L2 (world records + 64x64 terrains: ~1.2 GB per GPU)"},
+        "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 4),
+                       "p99": round(float(np.percentile(lat, 99)), 4), "max": round(float(lat.max()), 4)},
+        "plain_kernel": plain,
+        "speedup_vs_plain": round(plain["ms_per_step"] / (ms_total / K), 2) if plain else None,
+        "roofline": {"bound": "fp32", "achieved": round(achieved / 1e12, 3),
+                     "peak": round(peak.value / 1e12, 3), "unit": "TFLOP/s",
+                     "frac": round(achieved / peak.value, 4) if peak.value else None,
+                     "traffic": None,
+                     "kernel": "leg-parallel step", "kernel_ms": round(step_kernel_ms, 4),
+                     "flop_per_env_step": FLOP_PER_ENV_STEP,
+                     "peak_source": "measured FP32 FMA probe (arc_probe_fp32_peak) on this GPU",
+                     "hbm_gbs_algorithmic": round(n * HBM_BYTES_PER_ENV_STEP / (step_kernel_ms * 1e-3) / 1e9, 1)},
+        "gpu_launches": 3 * K,
+        "ended_in_last_step": ended,
+        "clocks": clock,
+    }
+    if e2e:
+        out["e2e"] = e2e
+    if world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(args.cpu_seconds, n)
+    return out
+
+
+def run_e2e(torch, env, params, stream, K) -> dict:
+    """The same loop through host buffers: actions from pinned host memory in,
+    observations / rewards / dones out to pinned host memory, every step."""
+    n = env.num_envs
+    host_act = torch.empty((n, 12), dtype=torch.float32, pin_memory=True)
+    host_obs = torch.empty((n, 195), dtype=torch.float32, pin_memory=True)
+    host_rew = torch.empty(n, dtype=torch.float32, pin_memory=True)
+    host_term = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    host_trunc = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    # the host-side policy's actions: the device policy's output, staged on the host
+    policy_forward(torch, params, env.obs, env.actions)
+    host_act.copy_(env.actions)
+    stream.synchronize()
+
+    def one():
+        env.actions.copy_(host_act, non_blocking=True)
+        env.step()
+        host_obs.copy_(env.obs, non_blocking=True)
+        host_rew.copy_(env.reward, non_blocking=True)
+        host_term.copy_(env.terminated, non_blocking=True)
+        host_trunc.copy_(env.truncated, non_blocking=True)
+        stream.synchronize()
+
+    for _ in range(2):
+        one()
+    t = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(K):
+        one()
+    e1.record(stream)
+    e1.synchronize()
+    wall = time.perf_counter() - t
+    ms = e0.elapsed_time(e1) / K
+    h2d = n * 12 * 4
+    d2h = n * 195 * 4 + n * 4 + 2 * n
+    return {"value": round(n / (ms * 1e-3), 1), "unit": "env-steps/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": round(ms, 4), "wall_ms_per_step": round(wall / K * 1e3, 4),
+            "path": "arc_env_step through DeviceVecEnv with pinned host buffers, synchronised every step"}
+
+
+# ---------------------------------------------------------------------------
+# the reference's CPU path
+
+def reference_loop(n: int, seconds: float | None, steps: int | None, warmup: int, threads: int) -> dict:
+    """The reference's OpenMP step/observe/heights (its csrc/, oracle/_ref) with
+    the task layer (obs, reward, done, auto-reset) in numpy, over n worlds of
+    the workload, the same MLP policy on the host (torch, all threads)."""
+    import torch
+    from oracle.oracle import RefSim, ref_available
+    from oracle.task_oracle import TaskConfig, TaskOracle
+    if not ref_available():
+        raise RuntimeError("oracle/_ref/libarcsim_ref.so not built")
+    torch.set_num_threads(threads)
+    sim = RefSim(n, threads=threads)
+    task = TaskOracle(sim, TaskConfig(curriculum=False), seed=5)
+    task.level[:] = levels_for(n, 17)
+    task.reset(np.arange(n))
+    obs = task.observe()
+    g = torch.Generator().manual_seed(1234)
+
+    def lin(i, o):
+        bound = 1.0 / np.sqrt(i)
+        return (torch.rand(o, i, generator=g) * 2 - 1) * bound, (torch.rand(o, generator=g) * 2 - 1) * bound
+    (w1, b1), (w2, b2), (w3, b3) = lin(195, 256), lin(256, 256), lin(256, 12)
+
+    def one(obs):
+        with torch.no_grad():
+            x = torch.from_numpy(obs)
+            a = torch.addmm(b3, torch.tanh(torch.addmm(b2, torch.tanh(torch.addmm(b1, x, w1.t())), w2.t())), w3.t())
+        _, te, tr, _ = task.step(a.numpy())
+        obs = task.observe()
+        ended = np.flatnonzero(te | tr)
+        if len(ended):
+            task.reset(ended)
+            obs[ended] = task.observe()[ended]
+        return obs
+
+    for _ in range(warmup):
+        obs = one(obs)
+    lat = []
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        s = time.perf_counter()
+        obs = one(obs)
+        lat.append(time.perf_counter() - s)
+        k += 1
+        el = time.perf_counter() - t0
+        if (steps is not None and k >= steps) or (seconds is not None and el >= seconds):
+            break
+    sim.close()
+    return {"value": n * k / el, "steps": k, "seconds": el, "lat": np.array(lat) * 1e3}
+
+
+def cpu_baseline(seconds: float, full_n: int) -> dict:
+    threads = os.cpu_count() or 1
+    sample_n = 4096
+    r = reference_loop(sample_n, seconds, None, 2, threads)
+    return {"value": round(r["value"], 1), "unit": "env-steps/s", "cores": threads, "kind": "reference",
+            "sample": f"{sample_n} of the {full_n} worlds (same difficulty mix), {r['steps']} control steps "
+                      f"in {r['seconds']:.1f} s: reference csrc/ step+observe+heights with OpenMP x{threads}, "
+                      "numpy task layer with auto-reset, MLP policy in torch on the host"}
+
+
+def run_reference(args) -> dict | None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    threads = os.cpu_count() or 1
+    sample_n = 4096
+    r = reference_loop(sample_n, None, max(args.steps, 1), max(args.warmup, 0), threads)
+    cpu = {"value": round(r["value"], 1), "unit": "env-steps/s", "cores": threads, "kind": "reference",
+           "sample": f"{sample_n} of the {args.worlds} worlds per step (same difficulty mix)"}
+    return {"metric": METRIC, "value": round(r["value"], 1), "unit": "env-steps/s", "impl": "reference",
+            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": r["steps"], "warmup": args.warmup,
+            "ms_per_step": round(float(r["lat"].mean()), 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{sample_n}-world sample of the {args.worlds}-world quadruped workload, "
+                                   "difficulty uniform in {0,...,1.0}, checkpoints, auto-reset, MLP policy",
+                       "threads": threads},
+            "latency_ms": {"p50": round(float(np.percentile(r["lat"], 50)), 3),
+                           "p99": round(float(np.percentile(r["lat"], 99)), 3)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(r["value"], 1), "unit": "env-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -112,6 +112,9 @@ int arc_sim_set_kernel(arc_sim *s, int kernel, int worlds_per_cta);
 int arc_sim_get_kernel(const arc_sim *s, int *kernel, int *worlds_per_cta);
 /* 4 for FP32, 8 for FP64 */
 int arc_sim_real_size(const arc_sim *s);
+/* Counts of the simulated model: bodies, joints, spheres, contact channels
+ * (the quadruped: 13, 12, 21, 6); any pointer may be NULL. */
+int arc_sim_model_info(const arc_sim *s, int *n_bodies, int *n_joints, int *n_spheres, int *n_channels);
 
 /* World-state snapshots, host FP64 buffers of arc_sim_state_size doubles per
  * world: bodies (x3 q4 v3 w3) x nb, spheres (anchored, anchor3, anchor_n3,
@@ -154,10 +157,96 @@ int arc_sim_set_pose(arc_sim *s, int id, const double *pos, const double *q, con
 void *arc_sim_stream(const arc_sim *s);
 /* targets: N x 12 FP64 on the device */
 int arc_sim_step_device(arc_sim *s, const double *d_targets, void *stream);
+/* actions: N x 12 FP32 policy actions on the device; targets are
+ * default + action_scale * clip(a, -1, 1) (arc/task.py:159-160), clamped */
+int arc_sim_step_actions(arc_sim *s, const float *d_actions, void *stream);
 /* observe into device FP64 buffers (any may be NULL) */
 int arc_sim_observe_device(const arc_sim *s, double *root, double *rot, double *joints, double *contacts, int *flags,
                            void *stream);
 int arc_sim_synchronize(const arc_sim *s);
+
+/* Measured FP32 FMA throughput of the current device (FLOP/s, an FMA
+ * counted as 2): the roofline denominator of the step kernels. */
+int arc_probe_fp32_peak(double *flops_per_s, double *seconds);
+
+/* ---- the task layer on the device (arc/task.py ArcTask and the auto-reset
+ * of arc/env.py ArcVecEnv.step_wait), so a training loop keeps observations,
+ * rewards and done flags in device memory. */
+
+/* TaskConfig (arc/task.py:17-66); arc_task_config_default fills its defaults. */
+typedef struct arc_task_config {
+    double dt;
+    int max_steps;
+    double action_scale, checkpoint_radius, checkpoint_min_dist, checkpoint_max_dist, border;
+    double w_progress, max_speed, fov, w_turn, w_checkpoint, w_time, w_fall, w_energy, w_action_rate;
+    double w_body_contact, w_torso_contact, w_body_rate, w_bounce;
+    double flip_up_z;
+    int beached_steps;
+    double void_z;
+    int curriculum;
+    double difficulty, max_difficulty, level_step;
+    int level_up_checkpoints, level_down_steps;
+} arc_task_config;
+
+void arc_task_config_default(arc_task_config *c);
+
+/* Attaches task state and output buffers to s. seed starts the device
+ * random stream of reset seeds and checkpoint draws (the reference draws
+ * them from numpy's PCG64 on the host; the distributions are the same). */
+int arc_env_init(arc_sim *s, const arc_task_config *cfg, unsigned long long seed);
+
+/* ArcTask.reset (arc/task.py:113-125) of the listed worlds (host ids; NULL
+ * and n_ids < 0: all), writing their observations. */
+int arc_env_reset(arc_sim *s, const int *ids, int n_ids, void *stream);
+
+/* One control step of ArcVecEnv.step_wait (arc/env.py:99-117) on the device:
+ * actuation from d_actions (N x 12 float32, clipped to [-1, 1]), physics,
+ * rewards, terminations, checkpoints, curriculum, observations, and the
+ * reset of every world that ended (their pre-reset observation goes to
+ * ARC_ENV_TERMINAL_OBS). d_actions == NULL: the ARC_ENV_ACTIONS buffer,
+ * through a CUDA graph of the whole step captured on first use. */
+int arc_env_step(arc_sim *s, const float *d_actions, void *stream);
+
+/* ArcTask.step alone (arc/task.py:155-220): no observation, no reset. */
+int arc_env_task_step(arc_sim *s, const float *d_actions, void *stream);
+/* ArcTask.observe (arc/task.py:231-259) of every world into ARC_ENV_OBS. */
+int arc_env_observe(arc_sim *s, void *stream);
+
+/* device buffers of the task layer */
+#define ARC_ENV_OBS 0               /* float32 N x 195 */
+#define ARC_ENV_TERMINAL_OBS 1      /* float32 N x 195 (rows of worlds that ended) */
+#define ARC_ENV_REWARD 2            /* float32 N */
+#define ARC_ENV_TERMINATED 3        /* uint8 N */
+#define ARC_ENV_TRUNCATED 4         /* uint8 N */
+#define ARC_ENV_CAUSE 5             /* int8 N: "", unstable, void, flip, beached */
+#define ARC_ENV_DONE_LIST 6         /* int32 N: worlds that ended in the last step */
+#define ARC_ENV_DONE_COUNT 7        /* int32 1 */
+#define ARC_ENV_ACTIONS 8           /* float32 N x 12: input of arc_env_step(s, NULL, ...) */
+#define ARC_ENV_ENDED_CHECKPOINTS 9 /* int32 N: episode stats of worlds that ended */
+#define ARC_ENV_ENDED_STEPS 10      /* int32 N */
+#define ARC_ENV_ENDED_DIFFICULTY 11 /* float64 N */
+#define ARC_ENV_NUM_BUFFERS 12
+
+/* Device pointer, shape (up to 2 dims) and dtype (DLPack codes: 0 int,
+ * 1 uint, 2 float; bits) of a buffer. */
+int arc_env_buffer(const arc_sim *s, int which, void **ptr, long long *shape, int *ndim, int *dtype_code,
+                   int *dtype_bits);
+/* Synchronous copies between a task-layer buffer and host memory of the
+ * buffer's full size (the reference's host-buffer style). */
+int arc_env_download(const arc_sim *s, int which, void *host);
+int arc_env_upload(arc_sim *s, int which, const void *host);
+/* The same buffer as a DLPack DLManagedTensor (caller hands it to a DLPack
+ * consumer, which calls its deleter). The memory stays owned by s. */
+int arc_env_dlpack(const arc_sim *s, int which, void **managed);
+
+/* Per-world task state, host FP64, ARC_TASK_STATE_SIZE values per world:
+ * target x y, target_z, prev_dist, prev_gaze, prev_action x12, torso_steps,
+ * steps, checkpoints, level, difficulty, in_view, episode, draws. */
+#define ARC_TASK_STATE_SIZE 25
+int arc_env_get_task_state(const arc_sim *s, const int *ids, int n_ids, double *out);
+int arc_env_set_task_state(arc_sim *s, const int *ids, int n_ids, const double *in);
+/* Places checkpoints at given points (target_z, prev_dist, prev_gaze follow). */
+int arc_env_set_targets(arc_sim *s, const int *ids, int n_ids, const double *xy);
 
 #ifdef __cplusplus
 }

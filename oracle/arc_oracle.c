@@ -1104,6 +1104,7 @@ typedef struct {
     int channel[MAXS];
     oworld tmpl;
     oworld *worlds;
+    double (*geom64)[4];  /* per world: cell, ox, oy, outside in FP64 */
 } osim;
 
 /* Copies the FP64 model (bodies as built, flat terrain) into a step world. */
@@ -1161,7 +1162,7 @@ static void load_terrain(oterrain *t, const dterrain *d)
 
 /* csrc/arc_sim.c:88-110: seeded terrain, noisy stance, random yaw, drop
  * height from the footprint; all in FP64, rounded into the world. */
-static void reset_world(const osim *s, oworld *w, uint32_t seed, double difficulty)
+static void reset_world(const osim *s, oworld *w, double *geom, uint32_t seed, double difficulty)
 {
     const tmodel *m = &s->model;
     orng rng;
@@ -1188,6 +1189,10 @@ static void reset_world(const osim *s, oworld *w, uint32_t seed, double difficul
     /* template copy (everything but the terrain), then the pose */
     memcpy(w, &s->tmpl, offsetof(oworld, t));
     load_terrain(&w->t, &t);
+    geom[0] = t.cell;
+    geom[1] = t.ox;
+    geom[2] = t.oy;
+    geom[3] = t.outside;
     for (i = 0; i < m->nb; ++i) {
         obody *b = &w->b[i];
         b->x = b->x_prev = to_r3(xs[i]);
@@ -1224,7 +1229,10 @@ EXPORT osim *ORC_EXPORT(create)(int n, double dt, int substeps, int grid, double
     s->grid = grid < GRID_MAX ? grid : GRID_MAX;
     s->cell = cell;
     s->worlds = (oworld *)malloc(sizeof(oworld) * (size_t)(n > 0 ? n : 1));
-    if (!s->worlds) {
+    s->geom64 = (double (*)[4])malloc(sizeof(double[4]) * (size_t)(n > 0 ? n : 1));
+    if (!s->worlds || !s->geom64) {
+        free(s->worlds);
+        free(s->geom64);
         free(s);
         return 0;
     }
@@ -1245,8 +1253,13 @@ EXPORT osim *ORC_EXPORT(create)(int n, double dt, int substeps, int grid, double
         s->tmpl.j[i].target = s->tmpl.j[i].angle = (real)s->model.default_angles[i];
     terrain_flat(&flat, s->grid, s->grid, cell, 0.0);
     load_terrain(&s->tmpl.t, &flat);
-    for (i = 0; i < n; ++i)
+    for (i = 0; i < n; ++i) {
         memcpy(&s->worlds[i], &s->tmpl, sizeof(oworld));
+        s->geom64[i][0] = flat.cell;
+        s->geom64[i][1] = flat.ox;
+        s->geom64[i][2] = flat.oy;
+        s->geom64[i][3] = flat.outside;
+    }
     return s;
 }
 
@@ -1255,6 +1268,7 @@ EXPORT void ORC_EXPORT(destroy)(osim *s)
     if (!s)
         return;
     free(s->worlds);
+    free(s->geom64);
     free(s);
 }
 
@@ -1282,7 +1296,7 @@ EXPORT void ORC_EXPORT(reset)(osim *s, const int *ids, int n_ids, const unsigned
     int k;
 #pragma omp parallel for schedule(static)
     for (k = 0; k < n_ids; ++k)
-        reset_world(s, &s->worlds[ids[k]], seeds[k], difficulty[k]);
+        reset_world(s, &s->worlds[ids[k]], s->geom64[ids[k]], seeds[k], difficulty[k]);
 }
 
 EXPORT void ORC_EXPORT(step)(osim *s, const double *targets)
@@ -1332,12 +1346,17 @@ EXPORT void ORC_EXPORT(observe)(const osim *s, double *root, double *rot, double
             r[10] = b->w.x; r[11] = b->w.y; r[12] = b->w.z;
         }
         if (rot) {
-            m3r m;
-            int a, c;
-            m3_from_quat(&m, b->q);
-            for (a = 0; a < 3; ++a)
-                for (c = 0; c < 3; ++c)
-                    rot[(size_t)i * 9 + a * 3 + c] = m.m[a][c];
+            /* FP64 from the state, as the reference's read-out (csrc/arc_sim.c:158-162) */
+            double qw = b->q.w, qx = b->q.x, qy = b->q.y, qz = b->q.z;
+            double k = 2.0 / (qw * qw + qx * qx + qy * qy + qz * qz);
+            double x2 = qx * k, y2 = qy * k, z2 = qz * k;
+            double xx = qx * x2, yy = qy * y2, zz = qz * z2;
+            double xy = qx * y2, xz = qx * z2, yz = qy * z2;
+            double wx = qw * x2, wy = qw * y2, wz = qw * z2;
+            double *o = rot + (size_t)i * 9;
+            o[0] = 1.0 - (yy + zz); o[1] = xy - wz;         o[2] = xz + wy;
+            o[3] = xy + wz;         o[4] = 1.0 - (xx + zz); o[5] = yz - wx;
+            o[6] = xz - wy;         o[7] = yz + wx;         o[8] = 1.0 - (xx + yy);
         }
         if (joints) {
             double *o = joints + (size_t)i * 3 * NJ;
@@ -1361,8 +1380,18 @@ EXPORT void ORC_EXPORT(observe)(const osim *s, double *root, double *rot, double
     }
 }
 
-/* csrc/arc_sim.c:185-203: the heading and sample points are in step
- * precision, like the CUDA path. */
+/* Height of the column under (x, y) in FP64 (csrc/arc_terrain.h:42-50),
+ * over the step-precision heights. */
+static double height64(const oterrain *t, const double *geom, double x, double y)
+{
+    double fx = floor((x - geom[1]) / geom[0]), fy = floor((y - geom[2]) / geom[0]);
+    if (!(fx >= 0.0 && fy >= 0.0 && fx < t->nx && fy < t->ny))
+        return geom[3];
+    return t->h[(int)fx + (int)fy * t->nx];
+}
+
+/* csrc/arc_sim.c:185-203, in FP64 from the step-precision state (the
+ * reference's read-out arithmetic; the CUDA path does the same). */
 EXPORT void ORC_EXPORT(heights)(const osim *s, const double *offsets, int k, double *out)
 {
     int i;
@@ -1370,18 +1399,13 @@ EXPORT void ORC_EXPORT(heights)(const osim *s, const double *offsets, int k, dou
     for (i = 0; i < s->n; ++i) {
         const oworld *w = &s->worlds[i];
         const obody *b = &w->b[0];
-        v3r fwd = q_rotate(b->q, v3(K(1.0), K(0.0), K(0.0)));
-        real yaw = R_ATAN2(fwd.y, fwd.x);
-#ifdef ORC_FP32
-        real c = cosf(yaw), sn = sinf(yaw);
-#else
-        real c = cos(yaw), sn = sin(yaw);
-#endif
+        d3 fwd = dq_rotate(dqv(b->q.w, b->q.x, b->q.y, b->q.z), d3v(1.0, 0.0, 0.0));
+        double yaw = atan2(fwd.y, fwd.x), c = cos(yaw), sn = sin(yaw);
+        double px = b->x.x, py = b->x.y;
         int j;
         for (j = 0; j < k; ++j) {
-            real f = (real)offsets[2 * j], l = (real)offsets[2 * j + 1];
-            out[(size_t)i * k + j] = terrain_height(&w->t, b->x.x + c * f - sn * l,
-                                                    b->x.y + sn * f + c * l);
+            double f = offsets[2 * j], l = offsets[2 * j + 1];
+            out[(size_t)i * k + j] = height64(&w->t, s->geom64[i], px + c * f - sn * l, py + sn * f + c * l);
         }
     }
 }
@@ -1391,7 +1415,7 @@ EXPORT void ORC_EXPORT(terrain_at)(const osim *s, const int *ids, const double *
 {
     int i;
     for (i = 0; i < m; ++i)
-        out[i] = terrain_height(&s->worlds[ids[i]].t, (real)xy[2 * i], (real)xy[2 * i + 1]);
+        out[i] = height64(&s->worlds[ids[i]].t, s->geom64[ids[i]], xy[2 * i], xy[2 * i + 1]);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1486,6 +1510,10 @@ EXPORT void ORC_EXPORT(set_terrain)(osim *s, int id, int nx, int ny, double cell
     for (i = 0; i < t.nx * t.ny; ++i)
         t.h[i] = heights[i];
     load_terrain(&s->worlds[id].t, &t);
+    s->geom64[id][0] = t.cell;
+    s->geom64[id][1] = t.ox;
+    s->geom64[id][2] = t.oy;
+    s->geom64[id][3] = t.outside;
 }
 
 EXPORT void ORC_EXPORT(get_terrain)(const osim *s, int id, int *nxy, double *geom, double *heights)
@@ -1494,10 +1522,8 @@ EXPORT void ORC_EXPORT(get_terrain)(const osim *s, int id, int *nxy, double *geo
     int i;
     nxy[0] = t->nx;
     nxy[1] = t->ny;
-    geom[0] = t->cell;
-    geom[1] = t->ox;
-    geom[2] = t->oy;
-    geom[3] = t->outside;
+    for (i = 0; i < 4; ++i)
+        geom[i] = s->geom64[id][i];
     if (heights)
         for (i = 0; i < t->nx * t->ny; ++i)
             heights[i] = t->h[i];
