@@ -169,6 +169,27 @@ int arc_sim_synchronize(const arc_sim *s);
  * counted as 2): the roofline denominator of the step kernels. */
 int arc_probe_fp32_peak(double *flops_per_s, double *seconds);
 
+/* ---- one control step without any device allocation. No counterpart in
+ * the reference: for callers that cannot call cudaMalloc (a host runtime
+ * that owns all device memory through its own arena; a control loop that
+ * must not trigger cudaMalloc's device-wide synchronisation), which
+ * therefore cannot create an arc_sim. The caller owns every buffer:
+ *   d_state    n_worlds x arc_sim_state_size (387) FP64, the snapshot layout
+ *              of arc_sim_get_state, read and updated in place
+ *   d_heights  n_worlds x grid x grid FP32 column heights, h[ix + iy * grid],
+ *              grid centred on the origin, `outside` beyond it
+ *   d_targets  n_worlds x 12 FP64 drive targets (as arc_sim_step)
+ * and the quadruped steps in FP32 with the leg-parallel kernel, asynchronously
+ * on `stream`. The kernel's work memory is one static device array of the
+ * library (about 4.9 MB, held by every GPU that loads the library until exit),
+ * which limits a call to n_worlds <= 1024, grid <= 64 and cell >= 0.4 m;
+ * larger requests return ARC_ERR_ARG. The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * Every call shares the array, so calls whose work overlaps on the GPU race:
+ * serialise them (one stream, or events). */
+int arc_step_noalloc(double *d_state, const float *d_heights, int grid, double cell, double outside,
+                     const double *d_targets, int n_worlds, double dt, int substeps, void *stream);
+
 /* ---- the task layer on the device (arc/task.py ArcTask and the auto-reset
  * of arc/env.py ArcVecEnv.step_wait), so a training loop keeps observations,
  * rewards and done flags in device memory. */
