@@ -31,7 +31,8 @@ cudaError_t launch_step_fast(const DevModel<R>& M, const Worlds<R>& W, const Act
                              int spill_per_lane, int lane_cap, int worlds_per_cta, cudaStream_t stream);
 
 template <class R> size_t fast_smem_bytes(int stride, int worlds_per_cta);
-constexpr int kFastOnChipContacts = 4;
+constexpr int kFastOnChipContacts = 2;
+constexpr int kFastMaxSubsteps = 1023;  // touch counters of the leg-parallel kernel
 
 // ----- outputs of the reference ABI (double precision, any pointer may be null)
 template <class R>

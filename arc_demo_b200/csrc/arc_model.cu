@@ -268,6 +268,12 @@ template <class R> DevModel<R> make_dev_model(const ModelHost& m, double dt, int
     s.hh = s.h * s.h;
     s.inv_h = R(1) / s.h;
     s.two_h = R(2) / s.h;
+    for (int i = 0; i < m.nj; ++i) {
+        JointK<R>& j = d.joint[i];
+        j.alpha_hh = j.alpha / s.hh;
+        j.max_dl = j.max_torque * s.h * s.h;
+        j.max_th = j.max_torque * s.h;
+    }
     s.mu_s = (R)m.mu_s;
     s.mu_d = (R)m.mu_d;
     s.gravity = rv<R>(m.gravity);

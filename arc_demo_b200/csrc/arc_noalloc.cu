@@ -152,10 +152,10 @@ extern "C" int arc_step_noalloc(double* d_state, const float* d_heights, int gri
         std::fprintf(stderr, "arc_step_noalloc: %d worlds; at most %d per call\n", n_worlds, kNoAllocMaxWorlds);
         return ARC_ERR_ARG;
     }
-    if (grid < 1 || grid > kNoAllocGridMax || !(cell >= kMinCell) || substeps < 1 || substeps > 0xffff ||
+    if (grid < 1 || grid > kNoAllocGridMax || !(cell >= kMinCell) || substeps < 1 || substeps > kFastMaxSubsteps ||
         !(dt > 0.0)) {
-        std::fprintf(stderr, "arc_step_noalloc: need 1 <= grid <= %d, cell >= %.1f m, 1 <= substeps <= 65535, dt > 0\n",
-                     kNoAllocGridMax, kMinCell);
+        std::fprintf(stderr, "arc_step_noalloc: need 1 <= grid <= %d, cell >= %.1f m, 1 <= substeps <= %d, dt > 0\n",
+                     kNoAllocGridMax, kMinCell, kFastMaxSubsteps);
         return ARC_ERR_ARG;
     }
     if (n_worlds == 0)

@@ -274,6 +274,11 @@ arc_sim* create_with_model(const ModelHost& model, int n, double dt, int substep
     s->off_joint = s->off_sphere + s->model.ns * kSphereRec;
     const int per16 = 16 / rs;
     s->stride = (s->off_joint + s->model.nj * kJointRec + per16 - 1) / per16 * per16;
+    // FP32: the eight worlds of a warp stage their records at distinct
+    // shared-memory banks when the stride is 4, 12, 20 or 28 mod 32 words
+    if (rs == 4)
+        while (s->stride % 8 != 4)
+            s->stride += 4;
     const size_t nn = (size_t)std::max(n, 1);
     bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess;
     ok = ok && cudaMalloc(&s->rec, nn * s->stride * rs) == cudaSuccess;
@@ -318,7 +323,7 @@ template <class R> int step_impl(arc_sim* s, const Actuation& A, cudaStream_t st
     const Worlds<R> W = view<R>(s);
     const DevModel<R>& M = dev_model<R>(s);
     cudaError_t e;
-    if (s->kernel == ARC_KERNEL_LEGS && M.leaper)
+    if (s->kernel == ARC_KERNEL_LEGS && M.leaper && s->substeps <= kFastMaxSubsteps)
         e = launch_step_fast<R>(M, W, A, static_cast<R*>(s->spill), s->spill_per_lane, s->lane_cap, s->wpc, st);
     else
         e = launch_step_plain<R>(M, W, A, nullptr, s->n, st);

@@ -156,6 +156,9 @@ template <class R> struct JointK {
     R lo, hi, kp, kd, max_torque;
     R lim[4];   // cos lo, sin lo, cos hi, sin hi (FP64, rounded once)
     R alpha;    // 1 / kp, the drive compliance (csrc/arc_phys.c:427)
+    // per-step constants, the same operations as the reference's inline
+    // expressions: alpha / (h*h), max_torque*h*h, max_torque*h
+    R alpha_hh, max_dl, max_th;
 };
 
 template <class R> struct SphereK {
@@ -388,10 +391,11 @@ template <class R> struct JointStepK {
 
 template <class R> ARC_HD JointStepK<R> joint_step_k(const JointK<R>& j, const StepK<R>& s)
 {
+    (void)s;
     JointStepK<R> o;
-    o.alpha_hh = j.alpha / s.hh;
-    o.max_dl = j.max_torque * s.h * s.h;
-    o.max_th = j.max_torque * s.h;
+    o.alpha_hh = j.alpha_hh;
+    o.max_dl = j.max_dl;
+    o.max_th = j.max_th;
     return o;
 }
 

@@ -36,7 +36,7 @@ namespace fast {
 
 constexpr int kLanes = 4;     // lanes per world (legs)
 constexpr int kDer = 22;      // per-body derived data: rot 9, iiw 6, x_prev 3, q_prev 4
-constexpr int kOnChip = 4;    // contact records per lane in shared memory
+constexpr int kOnChip = kFastOnChipContacts;  // contact records per lane in shared memory
 constexpr int kCRec = 8;      // local 3, n 3, body, pad
 constexpr int kSlots = 6;     // joint wavefront length
 constexpr int kLaneSpheres = 6;
@@ -180,12 +180,13 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
     }
     const bool active = valid && W.unstable[world] == 0;
 
+    // per-sphere state of this lane: anchored bits, touch counts packed
+    // 10 bits each (the host runs this kernel only for <= 1023 substeps)
     uint32_t anch = 0;
-    int touch[kLaneSpheres];
+    unsigned long long touches = 0;
     const uint32_t* sph = W.sph + (size_t)(valid ? world : 0) * 21;
 #pragma unroll
     for (int it = 0; it < kLaneSpheres; ++it) {
-        touch[it] = 0;
         const int s = sphere_of(leg, it);
         if (valid && s >= 0)
             anch |= ((sph[s] >> 16) & 1u) << it;
@@ -194,7 +195,7 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
     const StepK<R>& st = M.step;
 
     // csrc/arc_phys.c:713-714
-#pragma unroll
+#pragma unroll 1
     for (int it = 0; it < 4; ++it) {
         const int b = body_of(leg, it);
         if (active && b >= 0) {
@@ -210,7 +211,7 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
 
     for (int sub = 0; sub < M.substeps; ++sub) {
         // integrate (csrc/arc_phys.c:658-672)
-#pragma unroll
+#pragma unroll 1
         for (int it = 0; it < 4; ++it) {
             const int b = body_of(leg, it);
             if (active && b >= 0) {
@@ -254,7 +255,7 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
             Pose<R> P;
             V3<R> xp{};
             Q4<R> qp{};
-#pragma unroll
+#pragma unroll 1
             for (int it = 0; it < kLaneSpheres; ++it) {
                 const int s = sphere_of(leg, it);
                 if (active && s >= 0) {
@@ -280,7 +281,7 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
                         }
                         ++nc;
                     });
-                    touch[it] += t;
+                    touches += (unsigned long long)t << (10 * it);
                     anch = (anch & ~(1u << it)) | ((uint32_t)(ss.anchored != 0) << it);
                     a[0] = ss.anchor.x; a[1] = ss.anchor.y; a[2] = ss.anchor.z;
                     a[3] = ss.anchor_n.x; a[4] = ss.anchor_n.y; a[5] = ss.anchor_n.z;
@@ -292,7 +293,7 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
         __syncwarp();
 
         // velocities from positions (csrc/arc_phys.c:674-687)
-#pragma unroll
+#pragma unroll 1
         for (int it = 0; it < 4; ++it) {
             const int b = body_of(leg, it);
             if (active && b >= 0) {
@@ -384,7 +385,7 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
         for (int it = 0; it < kLaneSpheres; ++it) {
             const int s = sphere_of(leg, it);
             if (s >= 0)
-                sphw[s] = (uint32_t)touch[it] | (((anch >> it) & 1u) << 16);
+                sphw[s] = (uint32_t)((touches >> (10 * it)) & 1023u) | (((anch >> it) & 1u) << 16);
         }
         if (leg == 0) {
             W.time[world] += M.step_dt;

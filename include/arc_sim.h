@@ -182,7 +182,8 @@ int arc_probe_fp32_peak(double *flops_per_s, double *seconds);
  * and the quadruped steps in FP32 with the leg-parallel kernel, asynchronously
  * on `stream`. The kernel's work memory is one static device array of the
  * library (about 4.9 MB, held by every GPU that loads the library until exit),
- * which limits a call to n_worlds <= 1024, grid <= 64 and cell >= 0.4 m;
+ * which limits a call to n_worlds <= 1024, grid <= 64, cell >= 0.4 m and
+ * substeps <= 1023;
  * larger requests return ARC_ERR_ARG. The first call on a device looks up the
  * array's device address; make that first call before any stream capture.
  * Every call shares the array, so calls whose work overlaps on the GPU race:
