@@ -31,6 +31,12 @@ cudaError_t launch_step_fast(const DevModel<R>& M, const Worlds<R>& W, const Act
                              int spill_per_lane, int lane_cap, int worlds_per_cta, cudaStream_t stream);
 
 template <class R> size_t fast_smem_bytes(int stride, int worlds_per_cta);
+
+// Warp-per-leg step (FP32): a CTA of four warps steps 32 worlds, warp k runs
+// leg k of every world; same spill layout as launch_step_fast.
+cudaError_t launch_step_warps(const DevModel<float>& M, const Worlds<float>& W, const Actuation& A, float* spill,
+                              int spill_per_lane, int lane_cap, cudaStream_t stream);
+size_t warps_smem_bytes();
 constexpr int kFastOnChipContacts = 2;
 constexpr int kFastMaxSubsteps = 1023;  // touch counters of the leg-parallel kernel
 

@@ -318,12 +318,25 @@ template <class R> const DevModel<R>& dev_model(const arc_sim* s);
 template <> const DevModel<float>& dev_model<float>(const arc_sim* s) { return s->mf; }
 template <> const DevModel<double>& dev_model<double>(const arc_sim* s) { return s->md; }
 
+template <class R> cudaError_t launch_warps_if_fp32(arc_sim*, const DevModel<R>&, const Worlds<R>&, const Actuation&,
+                                                   cudaStream_t)
+{
+    return cudaErrorNotSupported;
+}
+template <> cudaError_t launch_warps_if_fp32<float>(arc_sim* s, const DevModel<float>& M, const Worlds<float>& W,
+                                                    const Actuation& A, cudaStream_t st)
+{
+    return launch_step_warps(M, W, A, static_cast<float*>(s->spill), s->spill_per_lane, s->lane_cap, st);
+}
+
 template <class R> int step_impl(arc_sim* s, const Actuation& A, cudaStream_t st)
 {
     const Worlds<R> W = view<R>(s);
     const DevModel<R>& M = dev_model<R>(s);
     cudaError_t e;
-    if (s->kernel == ARC_KERNEL_LEGS && M.leaper && s->substeps <= kFastMaxSubsteps)
+    if (s->kernel == ARC_KERNEL_WARPS && !s->fp64 && M.leaper && s->substeps <= kFastMaxSubsteps)
+        e = launch_warps_if_fp32<R>(s, M, W, A, st);
+    else if (s->kernel == ARC_KERNEL_LEGS && M.leaper && s->substeps <= kFastMaxSubsteps)
         e = launch_step_fast<R>(M, W, A, static_cast<R*>(s->spill), s->spill_per_lane, s->lane_cap, s->wpc, st);
     else
         e = launch_step_plain<R>(M, W, A, nullptr, s->n, st);
@@ -636,6 +649,9 @@ int arc_sim_set_kernel(arc_sim* s, int kernel, int worlds_per_cta)
         if (smem > 227 * 1024)
             return fail(s, ARC_ERR_UNSUPPORTED, "worlds_per_cta needs more than 227 KB of shared memory");
         s->wpc = worlds_per_cta;
+    } else if (kernel == ARC_KERNEL_WARPS) {
+        if (!s->model.leaper || s->fp64)
+            return fail(s, ARC_ERR_UNSUPPORTED, "warp-per-leg kernel needs the quadruped in FP32");
     } else if (kernel != ARC_KERNEL_PLAIN) {
         return fail(s, ARC_ERR_ARG, "unknown kernel");
     }

@@ -34,6 +34,7 @@ FP64 = 1
 PLAIN = 2
 KERNEL_PLAIN = 0
 KERNEL_LEGS = 1
+KERNEL_WARPS = 2
 
 
 class ArcSimError(RuntimeError):

@@ -56,6 +56,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--wpc", type=int, default=0, help="worlds per CTA (0: autotune)")
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--kernel", choices=["auto", "warps"], default="auto")
     return p.parse_args()
 
 
@@ -140,13 +141,18 @@ def policy_forward(torch, params, obs, out):
     torch.addmm(b3, h, w3.t(), out=out)
 
 
-def autotune(env, torch, stream, candidates=(8, 16, 32), steps=4):
-    """Worlds-per-CTA of the leg-parallel kernel, by timing the step kernel."""
-    from arc_demo_b200.native import KERNEL_LEGS
+def autotune(env, torch, stream, candidates=("warps", 8, 16), steps=4):
+    """Step kernel and worlds-per-CTA, by timing the step kernel: the
+    warp-per-leg kernel (32 worlds per CTA) and the leg-parallel kernel at
+    several worlds per CTA."""
+    from arc_demo_b200.native import KERNEL_LEGS, KERNEL_WARPS
     lib, ptr = env.sim._lib, env.sim.ptr
     best, table = None, {}
     for wpc in candidates:
-        env.set_kernel(KERNEL_LEGS, wpc)
+        if wpc == "warps":
+            env.set_kernel(KERNEL_WARPS)
+        else:
+            env.set_kernel(KERNEL_LEGS, wpc)
         a = ctypes.c_void_p(env.actions.data_ptr())
         st = ctypes.c_void_p(stream.cuda_stream)
         for _ in range(2):
@@ -158,10 +164,13 @@ def autotune(env, torch, stream, candidates=(8, 16, 32), steps=4):
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / steps
-        table[wpc] = round(ms, 4)
-        if best is None or ms < table[best]:
+        table[str(wpc)] = round(ms, 4)
+        if best is None or ms < table[str(best)]:
             best = wpc
-    env.set_kernel(KERNEL_LEGS, best)
+    if best == "warps":
+        env.set_kernel(KERNEL_WARPS)
+    else:
+        env.set_kernel(KERNEL_LEGS, best)
     return best, table
 
 
@@ -178,7 +187,7 @@ def run_ours(args) -> dict | None:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    from arc_demo_b200.native import KERNEL_LEGS, KERNEL_PLAIN, sim_lib
+    from arc_demo_b200.native import KERNEL_LEGS, KERNEL_PLAIN, KERNEL_WARPS, sim_lib
     from arc_demo_b200.task import TaskConfig
     from arc_demo_b200.torch_env import DeviceVecEnv
 
@@ -194,6 +203,9 @@ def run_ours(args) -> dict | None:
         if args.wpc:
             env.set_kernel(KERNEL_LEGS, args.wpc)
             best_wpc, tune = args.wpc, None
+        elif args.kernel == "warps":
+            env.set_kernel(KERNEL_WARPS)
+            best_wpc, tune = "warps", None
         else:
             best_wpc, tune = autotune(env, torch, stream)
         env.reset()
@@ -269,7 +281,10 @@ def run_ours(args) -> dict | None:
             plain_kernel_ms = q0.elapsed_time(q1) / 3
             plain = {"ms_per_step": round(plain_ms, 3), "env_steps_per_s": round(n / plain_ms * 1e3),
                      "step_kernel_ms": round(plain_kernel_ms, 3)}
-            env.set_kernel(KERNEL_LEGS, best_wpc)
+            if best_wpc == "warps":
+                env.set_kernel(KERNEL_WARPS)
+            else:
+                env.set_kernel(KERNEL_LEGS, best_wpc)
 
         e2e = None if args.no_e2e else run_e2e(torch, env, params, stream, max(3, min(K, 50)))
 
@@ -289,8 +304,9 @@ def run_ours(args) -> dict | None:
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{n} worlds of the quadruped per GPU, difficulty uniform in {{0,...,1.0}}, "
                                "checkpoints, auto-reset, random-init MLP policy 195-256-256-12 tanh FP32 in the loop",
-                   "worlds_per_gpu": n, "substeps": 20, "dt": 1 / 30, "kernel": "leg-parallel",
-                   "worlds_per_cta": best_wpc, "autotune_step_kernel_ms": tune,
+                   "worlds_per_gpu": n, "substeps": 20, "dt": 1 / 30,
+                   "kernel": "warp-per-leg" if best_wpc == "warps" else "leg-parallel",
+                   "worlds_per_cta": 32 if best_wpc == "warps" else best_wpc, "autotune_step_kernel_ms": tune,
                    "l2": "inputs larger than L2 (world records + 64x64 terrains: ~1.2 GB per GPU)"},
         "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 4),
                        "p99": round(float(np.percentile(lat, 99)), 4), "max": round(float(lat.max()), 4)},
@@ -300,7 +316,8 @@ def run_ours(args) -> dict | None:
                      "peak": round(peak.value / 1e12, 3), "unit": "TFLOP/s",
                      "frac": round(achieved / peak.value, 4) if peak.value else None,
                      "traffic": None,
-                     "kernel": "leg-parallel step", "kernel_ms": round(step_kernel_ms, 4),
+                     "kernel": ("warp-per-leg" if best_wpc == "warps" else "leg-parallel") + " step",
+                     "kernel_ms": round(step_kernel_ms, 4),
                      "flop_per_env_step": FLOP_PER_ENV_STEP,
                      "peak_source": "measured FP32 FMA probe (arc_probe_fp32_peak) on this GPU",
                      "hbm_gbs_algorithmic": round(n * HBM_BYTES_PER_ENV_STEP / (step_kernel_ms * 1e-3) / 1e9, 1)},

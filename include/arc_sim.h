@@ -100,6 +100,7 @@ const arc_world *arc_sim_world(const arc_sim *s, int i);
 /* kernels */
 #define ARC_KERNEL_PLAIN 0      /* one thread per world */
 #define ARC_KERNEL_LEGS 1       /* four lanes per world (one per leg), shared-memory staging */
+#define ARC_KERNEL_WARPS 2      /* FP32: four warps per 32 worlds (one warp per leg), leg state in registers */
 
 arc_sim *arc_sim_create_ex(int n_worlds, double dt, int substeps, int grid, double cell, unsigned flags);
 
@@ -107,7 +108,8 @@ arc_sim *arc_sim_create_ex(int n_worlds, double dt, int substeps, int grid, doub
 int arc_sim_last_error(const arc_sim *s);
 const char *arc_sim_error_message(const arc_sim *s);
 
-/* Kernel choice; worlds_per_cta in {8, 16, 32, 64} for ARC_KERNEL_LEGS. */
+/* Kernel choice; worlds_per_cta in {8, 16, 32, 64} for ARC_KERNEL_LEGS
+ * (ARC_KERNEL_WARPS always steps 32 worlds per CTA). */
 int arc_sim_set_kernel(arc_sim *s, int kernel, int worlds_per_cta);
 int arc_sim_get_kernel(const arc_sim *s, int *kernel, int *worlds_per_cta);
 /* 4 for FP32, 8 for FP64 */

@@ -26,7 +26,7 @@ Tolerances (the parity contract):
 import numpy as np
 import pytest
 
-from arc_demo_b200.native import KERNEL_LEGS, KERNEL_PLAIN, Sim
+from arc_demo_b200.native import KERNEL_LEGS, KERNEL_PLAIN, KERNEL_WARPS, Sim
 from oracle.oracle import NB, NS, OracleSim, RefSim, ref_available
 
 pytestmark = pytest.mark.gpu
@@ -117,7 +117,7 @@ def test_fp64_teacher_forced_vs_reference(kernel):
 
 
 @pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
-@pytest.mark.parametrize("kernel", [KERNEL_PLAIN, KERNEL_LEGS])
+@pytest.mark.parametrize("kernel", [KERNEL_PLAIN, KERNEL_LEGS, KERNEL_WARPS])
 def test_fp32_teacher_forced_vs_reference(kernel):
     ref, seeds, diffs, rng = diverse_states(N, seed=5)
     g = Sim(N)
@@ -194,6 +194,61 @@ def test_plain_and_leg_parallel_kernels_agree(fp64):
         assert dx.max() <= 1e-10
     else:
         assert np.percentile(dx, 95) <= 1e-5 and np.percentile(dx, 99) <= 5e-5
+
+
+@pytest.mark.parametrize("n", [1, 31, 33, 100])
+def test_warp_per_leg_kernel_agrees_with_leg_parallel(n):
+    """The warp-per-leg kernel (isotropy-specialised arithmetic) against the
+    leg-parallel one, ragged world counts included: FP32 rounding only."""
+    seeds, diffs = seeds_diffs(n, 31)
+    a, b = Sim(n), Sim(n)
+    a.set_kernel(KERNEL_WARPS)
+    b.set_kernel(KERNEL_LEGS, 8)
+    for s in (a, b):
+        s.reset(np.arange(n), seeds, diffs)
+    rng = np.random.default_rng(n)
+    dxs = []
+    for _ in range(4):
+        t = a.default_angles + 0.6 * rng.uniform(-1, 1, (n, 12))
+        b.set_state(a.get_state())
+        a.step(t)
+        b.step(t)
+        sa, sb = a.get_state(), b.get_state()
+        dxs.append(body_errors(sa, sb)[0])
+        assert np.array_equal(sa[:, -1], sb[:, -1])  # both stepped every world
+    dx = np.concatenate(dxs)
+    print(f"warps vs legs (n={n}): rel |dx| p50 {np.median(dx):.2e} max {dx.max():.2e}")
+    assert np.percentile(dx, 95) <= 1e-5 and np.percentile(dx, 99) <= 5e-5
+
+
+@pytest.mark.gpu
+def test_warp_per_leg_kernel_on_a_fine_grid():
+    """5 cm columns: one sphere can touch many columns, four lane lists can
+    exceed the 128-contact cap, and both kernels take the path that counts
+    every lane's contacts before the contact velocities."""
+    n = 64
+    seeds, diffs = seeds_diffs(n, 32)
+    diffs[:] = 1.0
+    a, b = Sim(n, cell=0.05), Sim(n, cell=0.05)
+    a.set_kernel(KERNEL_WARPS)
+    b.set_kernel(KERNEL_LEGS, 8)
+    for s in (a, b):
+        s.reset(np.arange(n), seeds, diffs)
+    rng = np.random.default_rng(5)
+    dxs, touched = [], 0
+    for _ in range(4):
+        t = a.default_angles + 0.6 * rng.uniform(-1, 1, (n, 12))
+        b.set_state(a.get_state())
+        a.step(t)
+        b.step(t)
+        sa, sb = a.get_state(), b.get_state()
+        dxs.append(body_errors(sa, sb)[0])
+        touched += int((touches(sa) > 0).sum())
+        assert np.array_equal(sa[:, -1], sb[:, -1])
+    dx = np.concatenate(dxs)
+    print(f"warps vs legs, 5 cm grid: rel |dx| p50 {np.median(dx):.2e} max {dx.max():.2e}, touching {touched}")
+    assert touched > 0
+    assert np.percentile(dx, 95) <= 1e-5 and np.percentile(dx, 99) <= 5e-5
 
 
 @pytest.mark.parametrize("wpc", [16, 32, 64])
