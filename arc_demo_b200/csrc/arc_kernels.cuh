@@ -38,6 +38,10 @@ cudaError_t launch_step_warps(const DevModel<float>& M, const Worlds<float>& W, 
                               int spill_per_lane, int lane_cap, cudaStream_t stream);
 size_t warps_smem_bytes();
 constexpr int kFastOnChipContacts = 2;
+constexpr int kWarpsOnChipContacts = 1;  // keeps four CTAs of the warp-per-leg kernel per SM
+// the fewest on-chip records of any kernel: a spill area of lane_cap minus
+// this many records per lane serves every kernel
+constexpr int kMinOnChipContacts = kWarpsOnChipContacts;
 constexpr int kFastMaxSubsteps = 1023;  // touch counters of the leg-parallel kernel
 
 // ----- outputs of the reference ABI (double precision, any pointer may be null)

@@ -168,7 +168,7 @@ int ensure_spill(arc_sim* s, double cell)
     if (s->spill && cell >= s->spill_cell)
         return ARC_OK;
     const int cap = lane_contact_bound(s->model, cell);
-    const int per = std::max(cap - kFastOnChipContacts, 1);
+    const int per = std::max(cap - kMinOnChipContacts, 1);
     const size_t bytes = (size_t)std::max(s->n, 1) * 4 * per * 8 * real_size(s);
     void* p = nullptr;
     if (check(s, cudaMalloc(&p, bytes), "cudaMalloc(contact spill)") != ARC_OK)

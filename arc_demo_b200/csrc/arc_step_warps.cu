@@ -1,423 +1,96 @@
 // arc_step_warps.cu - the warp-per-leg step kernel (FP32).
 //
 // A CTA of four warps steps 32 worlds: lane j of warp k is leg k of world j.
-// The joint solves follow the same six-slot wavefront as the leg-parallel
-// kernel (warp k runs joint 3k+(s-k) at slot s; see arc_step_fast.cu for why
-// that is the reference's Gauss-Seidel order, csrc/arc_phys.c:729-735), but
-// now a whole warp is either working or waiting at the slot barrier: waiting
-// warps issue nothing and the scheduler fills their slots with other CTAs.
-// Every lane of an active warp runs the same joint, so each joint is solved
-// by code specialised for its bodies: joint 3k couples the torso and the
-// coxa, both with equal principal moments, whose world inverse inertia is
-// d*I (csrc/arc_phys.c:70-75); joint 3k+1 the coxa and the femur; joint 3k+2
-// the femur and the tibia. The specialised arithmetic equals the general
-// 3x3 arithmetic on a diagonal matrix term by term (the skipped products
-// are exact zeros).
+// The reference's Gauss-Seidel order (csrc/arc_phys.c:729-735) couples the
+// legs only through the torso: joint 3k (torso -> coxa of leg k) must see
+// the torso as joint 3(k-1) left it. So warp k solves its torso joint after
+// warp k-1 solved its own (a named barrier between the two warps, one
+// arrive and one sync), and everything else of leg k - its two other
+// joints, its five spheres, its three bodies' velocities - runs without
+// waiting. Warp 0 also owns the torso's integration, sphere and contact
+// velocities; it waits for warp 3 before the torso's sphere.
 //
-// State placement: each lane keeps its leg's three body poses (x, q, the
-// rotation and world inverse inertia) in registers; velocities, previous
-// poses and sphere anchors of its leg in shared memory ([field][lane],
-// conflict-free); the torso of each world in shared memory, written only by
-// the warp whose slot owns it.
+// Code size decides this kernel's speed. With 12 warps of 3 CTAs per SM in
+// different phases of the step, a kernel whose code does not fit the SM's
+// instruction cache spends most cycles waiting for instructions. Every
+// phase is therefore one generic routine, run by a small interpreter over a
+// per-warp list of operations (integrate bodies a..b, solve joints a..b,
+// collide spheres a..b, ...): one copy of each routine, whatever the body.
+// The bodies live in shared memory ([field][lane], conflict-free); a
+// routine loads the few it works on, recomputes their rotation and world
+// inverse inertia from q (the same function of q as the reference's
+// body_sync, so the same values), and stores them back.
+//
+// Rotations the reference leaves stale: update_velocities (csrc/arc_phys.c:
+// 674-687) normalises q without re-syncing, so the velocity pass and the
+// next substep's gyroscopic term use the rotation of the un-normalised q of
+// the position pass. Each body therefore keeps two quaternions: field Q, the
+// position-pass q the rotation comes from, and field QP, the substep-start
+// q (and, after the velocity update, the normalised q the next substep
+// starts from).
 #include "arc_kernels.cuh"
 
 namespace arc {
 namespace wl {
 
-constexpr int kWarps = 4;            // one per leg
-constexpr int kWorlds = 32;          // one per lane
+constexpr int kWarps = 4;   // one per leg
+constexpr int kWorlds = 32; // one per lane
 constexpr int kThreads = kWarps * kWorlds;
-constexpr int kOnChip = kFastOnChipContacts;
+constexpr int kOnChip = kWarpsOnChipContacts;
 
 using F = float;
 using V = V3<F>;
 using Q = Q4<F>;
+using P = Pose<F>;
 
-// world inverse inertia: d*I for a body with equal moments, else symmetric
-template <bool ISO> struct Iw;
-template <> struct Iw<true> {
-    F d;
-    __device__ __forceinline__ V mul(V v) const { return V{v.x * d, v.y * d, v.z * d}; }
-    __device__ __forceinline__ void sync(const M3<F>&, const BodyK<F>& k) { d = k.inv_inertia.x; }
-    __device__ __forceinline__ void add_to(S3<F>& K) const
-    {
-        K.xx += d;
-        K.yy += d;
-        K.zz += d;
-    }
-    // csrc/arc_phys.c:284-300 with a = d*I
-    __device__ __forceinline__ void add_point_mass(S3<F>& K, F inv_mass, V r) const
-    {
-        const F x = r.x, y = r.y, z = r.z;
-        K.xx += inv_mass + d * z * z + d * y * y;
-        K.yy += inv_mass + d * x * x + d * z * z;
-        K.zz += inv_mass + d * y * y + d * x * x;
-        K.xy += -(d * x * y);
-        K.xz += -(d * x * z);
-        K.yz += -(d * y * z);
-    }
-    __device__ __forceinline__ S3<F> s3() const { return S3<F>{d, F(0), F(0), d, F(0), d}; }
-};
-template <> struct Iw<false> {
-    S3<F> m;
-    __device__ __forceinline__ V mul(V v) const { return arc::mul(m, v); }
-    __device__ __forceinline__ void sync(const M3<F>& r, const BodyK<F>& k)
-    {
-        // the anisotropic branch of body_sync (csrc/arc_phys.c:76-81)
-        const V d = k.inv_inertia;
-        V r0{r.m[0][0] * d.x, r.m[0][1] * d.y, r.m[0][2] * d.z};
-        V r1{r.m[1][0] * d.x, r.m[1][1] * d.y, r.m[1][2] * d.z};
-        V r2{r.m[2][0] * d.x, r.m[2][1] * d.y, r.m[2][2] * d.z};
-        m.xx = r0.x * r.m[0][0] + r0.y * r.m[0][1] + r0.z * r.m[0][2];
-        m.xy = r0.x * r.m[1][0] + r0.y * r.m[1][1] + r0.z * r.m[1][2];
-        m.xz = r0.x * r.m[2][0] + r0.y * r.m[2][1] + r0.z * r.m[2][2];
-        m.yy = r1.x * r.m[1][0] + r1.y * r.m[1][1] + r1.z * r.m[1][2];
-        m.yz = r1.x * r.m[2][0] + r1.y * r.m[2][1] + r1.z * r.m[2][2];
-        m.zz = r2.x * r.m[2][0] + r2.y * r.m[2][1] + r2.z * r.m[2][2];
-    }
-    __device__ __forceinline__ void add_to(S3<F>& K) const
-    {
-        K.xx += m.xx; K.xy += m.xy; K.xz += m.xz;
-        K.yy += m.yy; K.yz += m.yz; K.zz += m.zz;
-    }
-    __device__ __forceinline__ void add_point_mass(S3<F>& K, F inv_mass, V r) const
-    {
-        arc::add_point_mass(K, m, inv_mass, r);
-    }
-    __device__ __forceinline__ S3<F> s3() const { return m; }
-};
+// body fields: x, q (position pass), v, w, x_prev, q_prev / normalised q
+constexpr int kX = 0, kQ = 3, kV = 7, kW = 10, kXP = 13, kQP = 16, kBodyF = 20;
+constexpr int kTorso = 3;  // body slot of the torso; 0..2: the lane's coxa, femur, tibia
 
-template <bool ISO> struct Body {
-    V x;
-    Q q;
-    M3<F> rot;
-    Iw<ISO> iw;
-    __device__ __forceinline__ void sync(const BodyK<F>& k)
-    {
-        rot = m3_from_quat(q);
-        iw.sync(rot, k);
-    }
-};
-
-// ---------------------------------------------------------------------------
-// solver primitives on specialised bodies (csrc/arc_phys.c:182-371)
-
-template <bool I> __device__ __forceinline__ F w_pos(const Body<I>& b, const BodyK<F>& k, V r, V n)
-{
-    V rn = cross(r, n);
-    return k.inv_mass + dot(rn, b.iw.mul(rn));
-}
-
-template <bool I> __device__ __forceinline__ void pos_impulse(Body<I>& b, const BodyK<F>& k, V r, V p)
-{
-    b.x = madd(b.x, p, k.inv_mass);
-    b.q = q_turn(b.q, b.iw.mul(cross(r, p)));
-    b.sync(k);
-}
-
-template <bool I> __device__ __forceinline__ void rot_impulse(Body<I>& b, const BodyK<F>& k, V p)
-{
-    b.q = q_turn(b.q, b.iw.mul(p));
-    b.sync(k);
-}
-
-template <bool I> __device__ __forceinline__ F solve_pos_static(Body<I>& b, const BodyK<F>& k, V r, V d)
-{
-    F c = len(d);
-    if (c < F(1e-12))
-        return F(0);
-    V n = scale(d, F(1) / c);
-    F denom = w_pos(b, k, r, n);
-    if (denom <= F(0))
-        return F(0);
-    F dl = c / denom;
-    pos_impulse(b, k, r, scale(n, dl));
-    return dl;
-}
-
-template <bool IP, bool IC>
-__device__ __forceinline__ void solve_point(Body<IP>& b1, const BodyK<F>& k1, V r1, Body<IC>& b2, const BodyK<F>& k2,
-                                            V r2, V d)
-{
-    if (len2(d) < F(1e-24))
-        return;
-    S3<F> K{F(0), F(0), F(0), F(0), F(0), F(0)};
-    b1.iw.add_point_mass(K, k1.inv_mass, r1);
-    b2.iw.add_point_mass(K, k2.inv_mass, r2);
-    V p;
-    if (!solve3_sym(K, d, p))
-        return;
-    pos_impulse(b1, k1, r1, p);
-    pos_impulse(b2, k2, r2, -p);
-}
-
-template <bool IP, bool IC>
-__device__ __forceinline__ void solve_rot_block(Body<IP>& b1, const BodyK<F>& k1, Body<IC>& b2, const BodyK<F>& k2,
-                                                V rot)
-{
-    if (len2(rot) < F(1e-24))
-        return;
-    S3<F> K{F(0), F(0), F(0), F(0), F(0), F(0)};
-    b1.iw.add_to(K);
-    b2.iw.add_to(K);
-    V p;
-    if (!solve3_sym(K, rot, p))
-        return;
-    rot_impulse(b1, k1, p);
-    rot_impulse(b2, k2, -p);
-}
-
-template <bool IP, bool IC>
-__device__ __forceinline__ V solve_rot(Body<IP>& b1, const BodyK<F>& k1, Body<IC>& b2, const BodyK<F>& k2, V rot,
-                                       F alpha_hh, F max_dl)
-{
-    F theta = len(rot);
-    if (theta < F(1e-12))
-        return V{F(0), F(0), F(0)};
-    V n = scale(rot, F(1) / theta);
-    F denom = dot(n, b1.iw.mul(n)) + dot(n, b2.iw.mul(n)) + alpha_hh;
-    if (denom <= F(0))
-        return V{F(0), F(0), F(0)};
-    F dl = theta / denom;
-    if (dl > max_dl)
-        dl = max_dl;
-    V p = scale(n, dl);
-    rot_impulse(b1, k1, p);
-    rot_impulse(b2, k2, -p);
-    return p;
-}
-
-// csrc/arc_phys.c:413-457 for a joint with a parent body
-template <bool IP, bool IC>
-__device__ __forceinline__ void joint_positions(Body<IP>& bp, const BodyK<F>& kp, Body<IC>& bc, const BodyK<F>& kc,
-                                                const JointK<F>& j, F target, F& torque_acc, F hh)
-{
-    V a1;
-    F s, c;
-    if (j.kp > F(0)) {
-        a1 = mul(bp.rot, j.a1);
-        V b1 = mul(bp.rot, j.b1), b2 = mul(bc.rot, j.b2);
-        s = dot(cross(b1, b2), a1);
-        c = dot(b1, b2);
-        F phi = r_atan2(s, c);
-        V p = solve_rot(bp, kp, bc, kc, scale(a1, phi - target), j.alpha_hh, j.max_dl);
-        torque_acc -= dot(p, a1) / hh;
-    }
-    if (j.lo <= j.hi) {
-        a1 = mul(bp.rot, j.a1);
-        V b1 = mul(bp.rot, j.b1), b2 = mul(bc.rot, j.b2);
-        s = dot(cross(b1, b2), a1);
-        c = dot(b1, b2);
-        if (j.hi - j.lo > F(kPi) || s * j.lim[0] - c * j.lim[1] < F(0) || j.lim[3] * c - j.lim[2] * s < F(0)) {
-            F phi = r_atan2(s, c);
-            if (phi < j.lo)
-                solve_rot_block(bp, kp, bc, kc, scale(a1, phi - j.lo));
-            else if (phi > j.hi)
-                solve_rot_block(bp, kp, bc, kc, scale(a1, phi - j.hi));
-        }
-    }
-    a1 = mul(bp.rot, j.a1);
-    solve_rot_block(bp, kp, bc, kc, cross(a1, mul(bc.rot, j.a2)));
-    V r1 = mul(bp.rot, j.r1);
-    V r2 = mul(bc.rot, j.r2);
-    solve_point(bp, kp, r1, bc, kc, r2, (bc.x + r2) - (bp.x + r1));
-}
-
-// csrc/arc_phys.c:459-481
-template <bool IP, bool IC>
-__device__ __forceinline__ void joint_velocities(const Body<IP>& bp, V& wp, const Body<IC>& bc, V& wc,
-                                                 const JointK<F>& j, F h, F& torque_acc)
-{
-    if (j.kd <= F(0))
-        return;
-    V a = mul(bp.rot, j.a1);
-    F rel = dot(wc - wp, a);
-    F wsum = dot(a, bp.iw.mul(a)) + dot(a, bc.iw.mul(a));
-    if (wsum <= F(0))
-        return;
-    F impulse = -j.kd * rel * h;
-    F cap = r_min(r_fabs(rel) / wsum, j.max_th);
-    impulse = r_clamp(impulse, -cap, cap);
-    wp = wp - bp.iw.mul(scale(a, impulse));
-    wc = wc + bc.iw.mul(scale(a, impulse));
-    torque_acc += impulse / h;
-}
-
-// csrc/arc_phys.c:658-672 for one body; xp/qp receive the substep-start pose
-template <bool I>
-__device__ __forceinline__ void integrate(Body<I>& b, V& v, V& w, V& xp, Q& qp, const BodyK<F>& k, const StepK<F>& s)
-{
-    xp = b.x;
-    qp = b.q;
-    v = madd(v, s.gravity, s.h);
-    b.x = madd(b.x, v, s.h);
-    if (!I)
-        w = mul(b.rot, gyroscopic(k, tmul(b.rot, w), s.h));
-    b.q = q_turn(b.q, scale(w, s.h));
-    b.sync(k);
-}
-
-// csrc/arc_phys.c:512-539
-template <bool I>
-__device__ __forceinline__ void friction(Body<I>& b, const BodyK<F>& k, V xprev, Q qprev, const SphereK<F>& sk,
-                                         SphereState<F>& ss, V n, F ln, const StepK<F>& st)
-{
-    V c = b.x + mul(b.rot, sk.pos);
-    V p = madd(c, n, -sk.radius);
-    F frac = F(1);
-    if (!ss.anchored || dot(n, ss.anchor_n) < F(0.9)) {
-        V c0 = xprev + qrotate(qprev, sk.pos);
-        ss.anchor = madd(c0, n, -sk.radius);
-        ss.anchor_n = n;
-        ss.anchored = 1;
-    }
-    V e = p - ss.anchor;
-    e = madd(e, n, -dot(e, n));
-    F l = len(e);
-    if (l < F(1e-12))
-        return;
-    V r = p - b.x;
-    F wt = w_pos(b, k, r, scale(e, F(1) / l));
-    F lt = l / wt;
-    if (lt > st.mu_s * ln) {
-        frac = r_min(st.mu_d * ln / lt, F(1));
-        ss.anchor = madd(ss.anchor, e, F(1) - frac);
-    }
-    solve_pos_static(b, k, r, scale(e, -frac));
-}
-
-// csrc/arc_phys.c:542-610; record(local, n) receives each contact
-template <bool I, class Rec>
-__device__ __forceinline__ int collide(Body<I>& b, const BodyK<F>& k, V xprev, Q qprev, const SphereK<F>& sk,
-                                       SphereState<F>& ss, const TerrainView<F>& t, const StepK<F>& st, Rec&& record)
-{
-    F rad = sk.radius, ln = F(0);
-    V c = b.x + mul(b.rot, sk.pos), n_max{F(0), F(0), F(1)};
-    F depth_max = F(0);
-    int touched = 0;
-    if (!(r_fabs(c.x) < F(1e6) && r_fabs(c.y) < F(1e6))) {
-        ss.anchored = 0;
-        return 0;
-    }
-    const int ix0 = (int)r_floor((c.x - rad - t.ox) / t.cell);
-    const int ix1 = (int)r_floor((c.x + rad - t.ox) / t.cell);
-    const int iy0 = (int)r_floor((c.y - rad - t.oy) / t.cell);
-    const int iy1 = (int)r_floor((c.y + rad - t.oy) / t.cell);
-    for (int iy = iy0; iy <= iy1; ++iy) {
-        for (int ix = ix0; ix <= ix1; ++ix) {
-            F top = terrain_cell(t, ix, iy);
-            if (c.z - rad >= top)
-                continue;
-            F x0 = t.ox + F(ix) * t.cell, x1 = x0 + t.cell;
-            F y0 = t.oy + F(iy) * t.cell, y1 = y0 + t.cell;
-            int sx = c.x > x1 ? 1 : (c.x < x0 ? -1 : 0);
-            int sy = c.y > y1 ? 1 : (c.y < y0 ? -1 : 0);
-            if (sx && terrain_cell(t, ix + sx, iy) >= top)
-                continue;
-            if (sy && terrain_cell(t, ix, iy + sy) >= top)
-                continue;
-            if (sx && sy && terrain_cell(t, ix + sx, iy + sy) >= top)
-                continue;
-            V q{r_clamp(c.x, x0, x1), r_clamp(c.y, y0, y1), r_min(c.z, top)};
-            V diff = c - q;
-            F dist = len(diff), depth;
-            V n;
-            if (dist > F(1e-9)) {
-                if (dist >= rad)
-                    continue;
-                n = scale(diff, F(1) / dist);
-                depth = rad - dist;
-            } else {
-                n = V{F(0), F(0), F(1)};
-                depth = top - c.z + rad;
-            }
-            V r = madd(c, n, -rad) - b.x;
-            ln += solve_pos_static(b, k, r, scale(n, depth));
-            record(tmul(b.rot, r), n);
-            c = b.x + mul(b.rot, sk.pos);
-            if (depth > depth_max) {
-                depth_max = depth;
-                n_max = n;
-            }
-            touched = 1;
-        }
-    }
-    if (touched)
-        friction(b, k, xprev, qprev, sk, ss, n_max, ln, st);
-    else
-        ss.anchored = 0;
-    return touched;
-}
-
-// ---------------------------------------------------------------------------
-// shared memory
-
-constexpr int kTorso = 29;  // x3 q4 v3 w3 xp3 qp4 rot9 of each world's torso
-// per lane (leg k of world j): v3 w3 xp3 qp4 of coxa, femur, tibia (39), anchors of
-// its 5 spheres (30), and for warp 0 the torso sphere's anchor (6)
-constexpr int kCold = 39 + 30 + 6;
-constexpr int kCon = kOnChip * 7;  // on-chip contacts: local3 n3 body
-
+// The model constants stay in the kernel's parameter space: all lanes of a
+// warp read the same body, joint or sphere, a broadcast from the constant
+// cache.
 struct Smem {
-    BodyK<F> body[13];
-    JointK<F> joint[12];
-    SphereK<F> sphere[21];
-    F torso[kTorso][kWorlds];
-    F cold[kCold][kThreads];
-    F con[kCon][kThreads];
-    int nc[2][kWarps][kWorlds];
+    F leg[3 * kBodyF][kThreads];      // the lane's three bodies
+    F anch[5 * 6][kThreads];          // anchor, anchor normal of the lane's five spheres
+    F con[kOnChip * 7][kThreads];     // on-chip contact records: local3 n3 body
+    F torso[kBodyF + 6][kWorlds];     // each world's torso, then its sphere's anchor
+    int nc[2][kWarps][kWorlds];       // contact counts (capped lists), by substep parity
     int bad[kWarps][kWorlds];
 };
 
-// torso pose in shared memory of world j
-__device__ __forceinline__ void load_torso(const Smem& sm, int j, Body<true>& b)
+// a field array in shared memory: element f at p[f * s]
+struct Ref {
+    F* p;
+    int s;
+    __device__ __forceinline__ F& operator[](int f) const { return p[f * s]; }
+};
+__device__ __forceinline__ V getv(Ref r, int f) { return V{r[f], r[f + 1], r[f + 2]}; }
+__device__ __forceinline__ void setv(Ref r, int f, V v)
 {
-    b.x = V{sm.torso[0][j], sm.torso[1][j], sm.torso[2][j]};
-    b.q = Q{sm.torso[3][j], sm.torso[4][j], sm.torso[5][j], sm.torso[6][j]};
-#pragma unroll
-    for (int a = 0; a < 9; ++a)
-        (&b.rot.m[0][0])[a] = sm.torso[20 + a][j];
-    b.iw.d = sm.body[0].inv_inertia.x;
+    r[f] = v.x;
+    r[f + 1] = v.y;
+    r[f + 2] = v.z;
 }
-__device__ __forceinline__ void store_torso(Smem& sm, int j, const Body<true>& b)
+__device__ __forceinline__ Q getq(Ref r, int f) { return Q{r[f], r[f + 1], r[f + 2], r[f + 3]}; }
+__device__ __forceinline__ void setq(Ref r, int f, Q q)
 {
-    sm.torso[0][j] = b.x.x; sm.torso[1][j] = b.x.y; sm.torso[2][j] = b.x.z;
-    sm.torso[3][j] = b.q.w; sm.torso[4][j] = b.q.x; sm.torso[5][j] = b.q.y; sm.torso[6][j] = b.q.z;
-#pragma unroll
-    for (int a = 0; a < 9; ++a)
-        sm.torso[20 + a][j] = (&b.rot.m[0][0])[a];
+    r[f] = q.w;
+    r[f + 1] = q.x;
+    r[f + 2] = q.y;
+    r[f + 3] = q.z;
 }
-__device__ __forceinline__ V tget(const Smem& sm, int f, int j) { return V{sm.torso[f][j], sm.torso[f + 1][j], sm.torso[f + 2][j]}; }
-__device__ __forceinline__ void tset(Smem& sm, int f, int j, V v)
+__device__ __forceinline__ void load_pose(Ref r, const BodyK<F>& k, P& b)
 {
-    sm.torso[f][j] = v.x;
-    sm.torso[f + 1][j] = v.y;
-    sm.torso[f + 2][j] = v.z;
+    b.x = getv(r, kX);
+    b.q = getq(r, kQ);
+    body_sync(b, k);
 }
-__device__ __forceinline__ V cget(const Smem& sm, int f, int t) { return V{sm.cold[f][t], sm.cold[f + 1][t], sm.cold[f + 2][t]}; }
-__device__ __forceinline__ void cset(Smem& sm, int f, int t, V v)
+__device__ __forceinline__ void store_pose(Ref r, const P& b)
 {
-    sm.cold[f][t] = v.x;
-    sm.cold[f + 1][t] = v.y;
-    sm.cold[f + 2][t] = v.z;
+    setv(r, kX, b.x);
+    setq(r, kQ, b.q);
 }
-__device__ __forceinline__ Q cgetq(const Smem& sm, int f, int t)
-{
-    return Q{sm.cold[f][t], sm.cold[f + 1][t], sm.cold[f + 2][t], sm.cold[f + 3][t]};
-}
-__device__ __forceinline__ void csetq(Smem& sm, int f, int t, Q q)
-{
-    sm.cold[f][t] = q.w;
-    sm.cold[f + 1][t] = q.x;
-    sm.cold[f + 2][t] = q.y;
-    sm.cold[f + 3][t] = q.z;
-}
-// cold-field offsets of leg body i (0 coxa, 1 femur, 2 tibia): v, w, xp, qp
-__host__ __device__ constexpr int cv(int i) { return 13 * i; }
-__host__ __device__ constexpr int cw(int i) { return 13 * i + 3; }
-__host__ __device__ constexpr int cxp(int i) { return 13 * i + 6; }
-__host__ __device__ constexpr int cqp(int i) { return 13 * i + 9; }
-__host__ __device__ constexpr int canch(int s) { return 39 + 6 * s; }  // leg sphere s = 0..4, torso sphere 5
 
 // named barriers between two warps (ids 1..8; 0 is __syncthreads). The
 // producer's arrive orders its earlier shared-memory writes before the
@@ -425,9 +98,251 @@ __host__ __device__ constexpr int canch(int s) { return 39 + 6 * s; }  // leg sp
 __device__ __forceinline__ void bar_arrive(int id) { asm volatile("bar.arrive %0, 64;" ::"r"(id) : "memory"); }
 __device__ __forceinline__ void bar_sync(int id) { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
 
+// csrc/arc_phys.c:413-457 for a joint with a parent: the drive (solve_rot,
+// :353-371), the limit and the axis alignment (solve_rot_block, :328-346)
+// and the attachment (solve_point, :308-320), in that order, with one site
+// that applies the impulse (+p on the parent, -p on the child, :196-211).
+__device__ __forceinline__ void joint_positions(P& bp, const BodyK<F>& kp, P& bc, const BodyK<F>& kc,
+                                                const JointK<F>& j, F target, F& torque_acc, F hh)
+{
+#pragma unroll 1
+    for (int stage = 0; stage < 4; ++stage) {
+        const V a1 = mul(bp.rot, j.a1);
+        S3<F> K{F(0), F(0), F(0), F(0), F(0), F(0)};
+        V rhs{F(0), F(0), F(0)}, p{F(0), F(0), F(0)}, r1{F(0), F(0), F(0)}, r2{F(0), F(0), F(0)};
+        bool positional = false;
+        if (stage < 2) {
+            if (stage == 0 ? !(j.kp > F(0)) : !(j.lo <= j.hi))
+                continue;
+            const V b1 = mul(bp.rot, j.b1), b2 = mul(bc.rot, j.b2);
+            const F s = dot(cross(b1, b2), a1), c = dot(b1, b2);
+            // the limit needs the angle only outside [lo, hi]
+            if (stage == 1 &&
+                !(j.hi - j.lo > F(kPi) || s * j.lim[0] - c * j.lim[1] < F(0) || j.lim[3] * c - j.lim[2] * s < F(0)))
+                continue;
+            const F phi = r_atan2(s, c);
+            if (stage == 0) {
+                const V rot = scale(a1, phi - target);
+                const F theta = len(rot);
+                if (theta < F(1e-12))
+                    continue;
+                const V n = scale(rot, F(1) / theta);
+                const F denom = dot(n, mul(bp.iiw, n)) + dot(n, mul(bc.iiw, n)) + j.alpha_hh;
+                if (denom <= F(0))
+                    continue;
+                F dl = theta / denom;
+                if (dl > j.max_dl)
+                    dl = j.max_dl;
+                p = scale(n, dl);
+                torque_acc -= dot(p, a1) / hh;
+            } else {
+                if (phi < j.lo)
+                    rhs = scale(a1, phi - j.lo);
+                else if (phi > j.hi)
+                    rhs = scale(a1, phi - j.hi);
+                else
+                    continue;
+            }
+        } else if (stage == 2) {
+            rhs = cross(a1, mul(bc.rot, j.a2));
+        } else {
+            r1 = mul(bp.rot, j.r1);
+            r2 = mul(bc.rot, j.r2);
+            rhs = (bc.x + r2) - (bp.x + r1);
+            positional = true;
+        }
+        if (stage > 0) {
+            if (len2(rhs) < F(1e-24))
+                continue;
+            if (positional) {
+                add_point_mass(K, bp.iiw, kp.inv_mass, r1);
+                add_point_mass(K, bc.iiw, kc.inv_mass, r2);
+            } else {
+                K.xx = bp.iiw.xx + bc.iiw.xx; K.xy = bp.iiw.xy + bc.iiw.xy; K.xz = bp.iiw.xz + bc.iiw.xz;
+                K.yy = bp.iiw.yy + bc.iiw.yy; K.yz = bp.iiw.yz + bc.iiw.yz; K.zz = bp.iiw.zz + bc.iiw.zz;
+            }
+            if (!solve3_sym(K, rhs, p))
+                continue;
+        }
+        const V pn = -p;
+        if (positional) {
+            bp.x = madd(bp.x, p, kp.inv_mass);
+            bc.x = madd(bc.x, pn, kc.inv_mass);
+        }
+        const V tp = mul(bp.iiw, positional ? cross(r1, p) : p);
+        const V tc = mul(bc.iiw, positional ? cross(r2, pn) : pn);
+        bp.q = q_turn(bp.q, tp);
+        bc.q = q_turn(bc.q, tc);
+        if (positional)  // the last stage: the caller keeps x and q only
+            break;
+        body_sync(bp, kp);
+        body_sync(bc, kc);
+    }
+}
+
+// One sphere against the column grid (csrc/arc_phys.c:542-610) with its
+// contacts (solve_contact, :488-500) and the closing friction correction
+// (solve_friction, :512-539). The scan and the friction share one site of
+// the positional correction against the static world (solve_pos with no
+// second body and alpha = 0, :226-242). Returns 1 when the sphere touched.
+template <class Rec>
+__device__ __forceinline__ int collide(P& b, const BodyK<F>& k, V xprev, Q qprev, const SphereK<F>& sk,
+                                       SphereState<F>& ss, const TerrainView<F>& t, const StepK<F>& st, Rec&& record)
+{
+    const F rad = sk.radius;
+    V c = b.x + mul(b.rot, sk.pos);
+    // a blown-up state must not reach the int conversions
+    if (!(r_fabs(c.x) < F(1e6) && r_fabs(c.y) < F(1e6))) {
+        ss.anchored = 0;
+        return 0;
+    }
+    int ix0 = 0, ix1 = 0, iy0 = 0, iy1 = 0;
+#pragma unroll 1
+    for (int e = 0; e < 4; ++e) {
+        const F cv = e < 2 ? c.x : c.y, o = e < 2 ? t.ox : t.oy;
+        const int v = (int)r_floor((((e & 1) ? cv + rad : cv - rad) - o) / t.cell);
+        if (e == 0) ix0 = v;
+        else if (e == 1) ix1 = v;
+        else if (e == 2) iy0 = v;
+        else iy1 = v;
+    }
+    F ln = F(0), depth_max = F(0);
+    V n_max{F(0), F(0), F(1)};
+    int touched = 0, ix = ix0, iy = iy0;
+#pragma unroll 1
+    for (;;) {
+        V r, d, n{F(0), F(0), F(1)};
+        F depth = F(0);
+        bool contact = false;
+#pragma unroll 1
+        while (!contact && iy <= iy1) {
+            const int cx = ix, cy = iy;
+            if (++ix > ix1) {
+                ix = ix0;
+                ++iy;
+            }
+            const F top = terrain_cell(t, cx, cy);
+            if (c.z - rad >= top)
+                continue;
+            const F x0 = t.ox + F(cx) * t.cell, x1 = x0 + t.cell;
+            const F y0 = t.oy + F(cy) * t.cell, y1 = y0 + t.cell;
+            // edges and corners buried by an equal or higher neighbour
+            const int sx = c.x > x1 ? 1 : (c.x < x0 ? -1 : 0);
+            const int sy = c.y > y1 ? 1 : (c.y < y0 ? -1 : 0);
+            bool buried = false;
+#pragma unroll 1
+            for (int m = 1; m < 4 && !buried; ++m) {
+                if (((m & 1) && !sx) || ((m & 2) && !sy))
+                    continue;
+                buried = terrain_cell(t, cx + ((m & 1) ? sx : 0), cy + ((m & 2) ? sy : 0)) >= top;
+            }
+            if (buried)
+                continue;
+            const V q{r_clamp(c.x, x0, x1), r_clamp(c.y, y0, y1), r_min(c.z, top)};
+            const V diff = c - q;
+            const F dist = len(diff);
+            if (dist > F(1e-9)) {
+                if (dist >= rad)
+                    continue;
+                n = scale(diff, F(1) / dist);
+                depth = rad - dist;
+            } else {
+                depth = top - c.z + rad;  // centre inside the column: out through the top
+            }
+            r = madd(c, n, -rad) - b.x;
+            d = scale(n, depth);
+            contact = true;
+        }
+        if (!contact) {
+            if (!touched)
+                break;
+            // friction, once, after the scan; c is the current centre
+            const V p = madd(c, n_max, -rad);
+            if (!ss.anchored || dot(n_max, ss.anchor_n) < F(0.9)) {
+                const V c0 = xprev + qrotate(qprev, sk.pos);
+                ss.anchor = madd(c0, n_max, -rad);
+                ss.anchor_n = n_max;
+                ss.anchored = 1;
+            }
+            V e = p - ss.anchor;
+            e = madd(e, n_max, -dot(e, n_max));
+            const F l = len(e);
+            if (l < F(1e-12))
+                break;
+            r = p - b.x;
+            const F lt = l / w_pos(b, k, r, scale(e, F(1) / l));
+            F frac = F(1);
+            if (lt > st.mu_s * ln) {
+                frac = r_min(st.mu_d * ln / lt, F(1));
+                ss.anchor = madd(ss.anchor, e, F(1) - frac);
+            }
+            d = scale(e, -frac);
+        }
+        F dl = F(0);
+        const F cl = len(d);
+        if (cl >= F(1e-12)) {
+            const V nn = scale(d, F(1) / cl);
+            const F denom = w_pos(b, k, r, nn);
+            if (denom > F(0)) {
+                dl = cl / denom;
+                pos_impulse(b, k, r, scale(nn, dl));
+            }
+        }
+        if (!contact)
+            break;  // the friction correction closes the sphere
+        ln += dl;
+        record(tmul(b.rot, r), n);
+        c = b.x + mul(b.rot, sk.pos);
+        if (depth > depth_max) {
+            depth_max = depth;
+            n_max = n;
+        }
+        touched = 1;
+    }
+    if (!touched)
+        ss.anchored = 0;
+    return touched;
+}
+
+// per-warp operation lists: kind | a << 4 | b << 8 | wait << 12 | arrive << 16
+enum : uint32_t { OP_END = 0, OP_INT, OP_JNT, OP_COL, OP_UPD, OP_DMP, OP_CVL, OP_CNT };
+// INT/UPD a..b: body ordinals (0 torso, 1..3 coxa, femur, tibia)
+// JNT/DMP a..b: the leg's joints (0 torso->coxa, 1 coxa->femur, 2 femur->tibia)
+// COL a..b: sphere ordinals on one body (0 torso sphere, 1 femur, 2..5 tibia)
+// CVL a: contact velocities of the leg's bodies (0) or of the torso (1)
+// CNT: publish the contact count, then __syncthreads (capped lists only)
+#define ARC_OP(kind, a, b, w, r) ((kind) | (a) << 4 | (b) << 8 | (w) << 12 | (r) << 16)
+#define ARC_LEG_OPS(k, cnt)                                                                                       \
+    {ARC_OP(OP_INT, 1, 4, 0, 0), ARC_OP(OP_JNT, 0, 1, k, k + 1), ARC_OP(OP_JNT, 1, 3, 0, 0),                      \
+     ARC_OP(OP_COL, 1, 2, 0, 0), ARC_OP(OP_COL, 2, 6, 0, 0), ARC_OP(OP_UPD, 1, 4, 0, 0), cnt,                     \
+     ARC_OP(OP_DMP, 0, 1, 4 + k, 5 + k), ARC_OP(OP_DMP, 1, 3, 0, 0), ARC_OP(OP_CVL, 0, 0, 0, 0), OP_END}
+#define ARC_NOP ARC_OP(OP_UPD, 0, 0, 0, 0)  // an empty range
+#define ARC_CNT ARC_OP(OP_CNT, 0, 0, 0, 0)
+
+constexpr int kMaxOps = 16;
+__constant__ uint32_t kOps[2][kWarps][kMaxOps] = {
+    // contact lists that cannot reach the cap: warp 0 takes the torso sphere
+    // after its own leg (the contacts of different bodies commute)
+    {{ARC_OP(OP_INT, 0, 2, 0, 0), ARC_OP(OP_JNT, 0, 1, 0, 1), ARC_OP(OP_INT, 2, 4, 0, 0), ARC_OP(OP_JNT, 1, 3, 0, 0),
+      ARC_OP(OP_COL, 1, 2, 0, 0), ARC_OP(OP_COL, 2, 6, 0, 0), ARC_OP(OP_UPD, 1, 4, 0, 0), ARC_OP(OP_COL, 0, 1, 4, 0),
+      ARC_OP(OP_UPD, 0, 1, 0, 0), ARC_OP(OP_DMP, 0, 1, 0, 5), ARC_OP(OP_DMP, 1, 3, 0, 0), ARC_OP(OP_CVL, 0, 0, 0, 0),
+      ARC_OP(OP_CVL, 1, 0, 8, 0), OP_END},
+     ARC_LEG_OPS(1, ARC_NOP), ARC_LEG_OPS(2, ARC_NOP), ARC_LEG_OPS(3, ARC_NOP)},
+    // capped lists: the torso sphere's contacts lead, as sphere 0 leads the
+    // reference's list, and every lane's count is published
+    {{ARC_OP(OP_INT, 0, 2, 0, 0), ARC_OP(OP_JNT, 0, 1, 0, 1), ARC_OP(OP_INT, 2, 4, 0, 0), ARC_OP(OP_JNT, 1, 3, 0, 0),
+      ARC_OP(OP_COL, 0, 1, 4, 0), ARC_OP(OP_UPD, 0, 1, 0, 0), ARC_OP(OP_COL, 1, 2, 0, 0), ARC_OP(OP_COL, 2, 6, 0, 0),
+      ARC_OP(OP_UPD, 1, 4, 0, 0), ARC_CNT, ARC_OP(OP_DMP, 0, 1, 0, 5), ARC_OP(OP_DMP, 1, 3, 0, 0),
+      ARC_OP(OP_CVL, 0, 0, 0, 0), ARC_OP(OP_CVL, 1, 0, 8, 0), OP_END},
+     ARC_LEG_OPS(1, ARC_CNT), ARC_LEG_OPS(2, ARC_CNT), ARC_LEG_OPS(3, ARC_CNT)}};
+#undef ARC_LEG_OPS
+#undef ARC_NOP
+#undef ARC_CNT
+#undef ARC_OP
+
 // ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kThreads, 4)
 k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F* __restrict__ spill, int spill_per_lane,
              int lane_cap)
 {
@@ -438,40 +353,37 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
     const bool valid = world < W.n;
     const int wi = valid ? world : 0;
 
-    for (int k = tid; k < 13; k += kThreads)
-        sm.body[k] = M.body[k];
-    for (int k = tid; k < 12; k += kThreads)
-        sm.joint[k] = M.joint[k];
-    for (int k = tid; k < 21; k += kThreads)
-        sm.sphere[k] = M.sphere[k];
-
     F* rec = W.rec + (size_t)wi * W.stride;
     F* sr = rec + W.off_sphere;
     F* jr = rec + W.off_joint;
     const int b_c = 1 + 3 * leg, b_f = 2 + 3 * leg, b_t = 3 + 3 * leg;  // coxa, femur, tibia
     const int j0 = 3 * leg;
-    // actuation (csrc/arc_sim.c:132-136) and the leg's state
-    F target[3], tacc[3] = {F(0), F(0), F(0)};
-    if (valid) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            target[c] = actuate(M, A, world, j0 + c);
-            jr[(j0 + c) * kJointRec] = target[c];
-        }
-    }
-    const bool active = valid && W.unstable[wi] == 0;
-    Body<true> co;
-    Body<false> fe, ti;
-    auto load_body = [&](int b, V& x, Q& q) {
-        const F* r = rec + b * kBodyRec;
-        x = V{r[0], r[1], r[2]};
-        q = Q{r[3], r[4], r[5], r[6]};
-        cset(sm, cv(b == b_c ? 0 : (b == b_f ? 1 : 2)), tid, V{r[7], r[8], r[9]});
-        cset(sm, cw(b == b_c ? 0 : (b == b_f ? 1 : 2)), tid, V{r[10], r[11], r[12]});
+    const Ref torso{&sm.torso[0][j], kWorlds};
+    auto body_ref = [&](int slot) {
+        return slot == kTorso ? torso : Ref{&sm.leg[slot * kBodyF][tid], kThreads};
     };
-    load_body(b_c, co.x, co.q);
-    load_body(b_f, fe.x, fe.q);
-    load_body(b_t, ti.x, ti.q);
+    // actuation (csrc/arc_sim.c:132-136)
+    F target0 = F(0), target1 = F(0), target2 = F(0);
+    if (valid) {
+        target0 = actuate(M, A, world, j0);
+        target1 = actuate(M, A, world, j0 + 1);
+        target2 = actuate(M, A, world, j0 + 2);
+        jr[j0 * kJointRec] = target0;
+        jr[(j0 + 1) * kJointRec] = target1;
+        jr[(j0 + 2) * kJointRec] = target2;
+    }
+    F tacc0 = F(0), tacc1 = F(0), tacc2 = F(0);
+    const bool active = valid && W.unstable[wi] == 0;
+    auto stage_body = [&](Ref r, const F* src) {
+        setv(r, kX, V{src[0], src[1], src[2]});
+        setq(r, kQ, Q{src[3], src[4], src[5], src[6]});
+        setq(r, kQP, Q{src[3], src[4], src[5], src[6]});
+        setv(r, kV, V{src[7], src[8], src[9]});
+        setv(r, kW, V{src[10], src[11], src[12]});
+    };
+#pragma unroll 1
+    for (int i = 0; i < 3; ++i)
+        stage_body(body_ref(i), rec + (b_c + i) * kBodyRec);
     uint32_t anch = 0;
     const uint32_t* sphr = W.sph + (size_t)wi * 21;
 #pragma unroll
@@ -479,315 +391,255 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
         const F* a = sr + (5 * leg + 1 + s) * kSphereRec;
 #pragma unroll
         for (int c = 0; c < 6; ++c)
-            sm.cold[canch(s) + c][tid] = a[c];
+            sm.anch[6 * s + c][tid] = a[c];
         anch |= ((sphr[5 * leg + 1 + s] >> 16) & 1u) << s;
     }
     if (leg == 0) {
-        const F* r = rec;  // torso, body 0
-        for (int f = 0; f < 13; ++f)
-            sm.torso[f][j] = r[f];
+        stage_body(torso, rec);
 #pragma unroll
         for (int c = 0; c < 6; ++c)
-            sm.cold[canch(5) + c][tid] = sr[c];
+            torso[kBodyF + c] = sr[c];
         anch |= ((sphr[0] >> 16) & 1u) << 5;
     }
     const TerrainView<F> T = terrain_of(W, wi);
     const StepK<F>& st = M.step;
-    const BodyK<F>& K0 = M.body[0];
-    __syncthreads();
-    const BodyK<F> Kc = sm.body[b_c], Kf = sm.body[b_f], Kt = sm.body[b_t];
-
-    // csrc/arc_phys.c:713-714
-    if (active) {
-        co.sync(Kc);
-        fe.sync(Kf);
-        ti.sync(Kt);
-        if (leg == 0) {
-            Body<true> to;
-            to.q = Q{sm.torso[3][j], sm.torso[4][j], sm.torso[5][j], sm.torso[6][j]};
-            to.sync(K0);
-#pragma unroll
-            for (int a = 0; a < 9; ++a)
-                sm.torso[20 + a][j] = (&to.rot.m[0][0])[a];
-        }
-    }
-    unsigned long long touches = 0;
-    __syncthreads();
-
-    // Only joint 3k of each leg touches a body another warp owns (the torso),
-    // so the wavefront needs no CTA-wide barrier: warp k waits for warp k-1
-    // to finish its torso joint (named barrier k, producer arrives, consumer
-    // syncs), and warp 0 waits for warp 3 before the torso's own sphere and
-    // contact velocities. Each barrier is re-armed only after its consumer
-    // passed it: the arrivals form one ring per substep.
-    // Contact lists can exceed the reference's cap of kMaxContacts only when
-    // four lane lists can; then the leg-major prefix needs every count.
+    unsigned long long touches = 0;  // 10 bits per sphere: leg spheres 0..4, torso sphere at 50
     const bool capped = kWarps * lane_cap > kMaxContacts;
-    const int pos_wait = leg == 0 ? kWarps : leg, pos_done = leg + 1;  // barrier ids 1..4
-    const int vel_wait = pos_wait + kWarps, vel_done = pos_done + kWarps;  // 5..8
-    for (int sub = 0; sub < M.substeps; ++sub) {
-        // integrate (csrc/arc_phys.c:658-672); warp 0 starts the wavefront,
-        // so it integrates its femur and tibia after handing the torso on
-        auto integrate_ft = [&]() {
-            V v = cget(sm, cv(1), tid), w = cget(sm, cw(1), tid), xp;
-            Q qp;
-            integrate(fe, v, w, xp, qp, Kf, st);
-            cset(sm, cv(1), tid, v); cset(sm, cw(1), tid, w); cset(sm, cxp(1), tid, xp); csetq(sm, cqp(1), tid, qp);
-            v = cget(sm, cv(2), tid); w = cget(sm, cw(2), tid);
-            integrate(ti, v, w, xp, qp, Kt, st);
-            cset(sm, cv(2), tid, v); cset(sm, cw(2), tid, w); cset(sm, cxp(2), tid, xp); csetq(sm, cqp(2), tid, qp);
-        };
-        if (active) {
-            V v, w, xp;
-            Q qp;
-            v = cget(sm, cv(0), tid); w = cget(sm, cw(0), tid);
-            integrate(co, v, w, xp, qp, Kc, st);
-            cset(sm, cv(0), tid, v); cset(sm, cw(0), tid, w); cset(sm, cxp(0), tid, xp); csetq(sm, cqp(0), tid, qp);
-            if (leg == 0) {
-                Body<true> to;
-                load_torso(sm, j, to);
-                V tv = tget(sm, 7, j), tw = tget(sm, 10, j), txp;
-                Q tqp;
-                integrate(to, tv, tw, txp, tqp, K0, st);
-                store_torso(sm, j, to);
-                tset(sm, 7, j, tv);
-                tset(sm, 10, j, tw);
-                tset(sm, 13, j, txp);
-                sm.torso[16][j] = tqp.w; sm.torso[17][j] = tqp.x; sm.torso[18][j] = tqp.y; sm.torso[19][j] = tqp.z;
-            }
-        }
-#pragma unroll 1
-        for (int part = 0; part < 2; ++part) {
-            if (part == (leg == 0 ? 1 : 0) && active)
-                integrate_ft();
-            if (part == 0) {
-                // joint 3*leg: torso -> coxa (csrc/arc_phys.c:729-730)
-                if (leg != 0)
-                    bar_sync(pos_wait);
-                if (active) {
-                    Body<true> to;
-                    load_torso(sm, j, to);
-                    joint_positions(to, K0, co, Kc, sm.joint[j0], target[0], tacc[0], st.hh);
-                    store_torso(sm, j, to);
-                }
-                bar_arrive(pos_done);
-            }
-        }
-        if (active) {
-            joint_positions(co, Kc, fe, Kf, sm.joint[j0 + 1], target[1], tacc[1], st.hh);
-            joint_positions(fe, Kf, ti, Kt, sm.joint[j0 + 2], target[2], tacc[2], st.hh);
-        }
+    const uint32_t* ops = &kOps[capped ? 1 : 0][leg][0];
+    __syncthreads();
 
-        // sphere contacts (csrc/arc_phys.c:731-732) and velocities from
-        // positions (csrc/arc_phys.c:674-687). The torso's sphere waits for
-        // the last torso joint; when the cap can bind it also leads warp 0's
-        // list, as sphere 0 leads the reference's.
+    for (int sub = 0; sub < M.substeps; ++sub) {
         int nc = 0;
         auto record = [&](int body, V local, V n) {
-            F* dst = nullptr;
             if (nc < kOnChip) {
-                sm.con[nc * 7 + 0][tid] = local.x; sm.con[nc * 7 + 1][tid] = local.y; sm.con[nc * 7 + 2][tid] = local.z;
-                sm.con[nc * 7 + 3][tid] = n.x; sm.con[nc * 7 + 4][tid] = n.y; sm.con[nc * 7 + 5][tid] = n.z;
-                sm.con[nc * 7 + 6][tid] = (F)body;
+                F* d = &sm.con[nc * 7][tid];
+                d[0] = local.x; d[kThreads] = local.y; d[2 * kThreads] = local.z;
+                d[3 * kThreads] = n.x; d[4 * kThreads] = n.y; d[5 * kThreads] = n.z;
+                d[6 * kThreads] = (F)body;
             } else if (nc < lane_cap) {
-                dst = spill + (((size_t)wi * kWarps + leg) * (size_t)spill_per_lane + (nc - kOnChip)) * 8;
-                dst[0] = local.x; dst[1] = local.y; dst[2] = local.z;
-                dst[3] = n.x; dst[4] = n.y; dst[5] = n.z;
-                dst[6] = (F)body;
+                F* d = spill + (((size_t)wi * kWarps + leg) * (size_t)spill_per_lane + (nc - kOnChip)) * 8;
+                d[0] = local.x; d[1] = local.y; d[2] = local.z;
+                d[3] = n.x; d[4] = n.y; d[5] = n.z;
+                d[6] = (F)body;
             }
             ++nc;
         };
 #pragma unroll 1
-        for (int part = 0; part < 2; ++part) {
-            if ((part == 0) == capped) {
-                if (leg != 0)
-                    continue;
-                bar_sync(pos_wait);
-                if (!active)
-                    continue;
-                Body<true> to;
-                load_torso(sm, j, to);
-                SphereState<F> ss{cget(sm, canch(5), tid), cget(sm, canch(5) + 3, tid), (int)((anch >> 5) & 1u)};
-                const V txp = tget(sm, 13, j);
-                const Q tqp{sm.torso[16][j], sm.torso[17][j], sm.torso[18][j], sm.torso[19][j]};
-                const int t = collide(to, K0, txp, tqp, sm.sphere[0], ss, T, st, [&](V l, V n) { record(0, l, n); });
-                touches += (unsigned long long)t << 50;
-                anch = (anch & ~(1u << 5)) | ((uint32_t)(ss.anchored != 0) << 5);
-                cset(sm, canch(5), tid, ss.anchor);
-                cset(sm, canch(5) + 3, tid, ss.anchor_n);
-                V v, w;
-                update_velocity(to.q, to.x, v, w, txp, tqp, st);
-                store_torso(sm, j, to);
-                tset(sm, 7, j, v);
-                tset(sm, 10, j, w);
-                continue;
-            }
-            if (!active)
-                continue;
-            {
-                const int s = 5 * leg + 1;
-                SphereState<F> ss{cget(sm, canch(0), tid), cget(sm, canch(0) + 3, tid), (int)(anch & 1u)};
-                const int t = collide(fe, Kf, cget(sm, cxp(1), tid), cgetq(sm, cqp(1), tid), sm.sphere[s], ss, T, st,
-                                      [&](V l, V n) { record(b_f, l, n); });
-                touches += (unsigned long long)t;
-                anch = (anch & ~1u) | (uint32_t)(ss.anchored != 0);
-                cset(sm, canch(0), tid, ss.anchor);
-                cset(sm, canch(0) + 3, tid, ss.anchor_n);
-            }
-            const V txp = cget(sm, cxp(2), tid);
-            const Q tqp = cgetq(sm, cqp(2), tid);
+        for (int i = 0;; ++i) {
+            const uint32_t op = ops[i];
+            const uint32_t kind = op & 15u;
+            if (kind == OP_END)
+                break;
+            const int a = (op >> 4) & 15, b = (op >> 8) & 15, wait = (op >> 12) & 15, arrive = (op >> 16) & 15;
+            if (wait)
+                bar_sync(wait);
+            if (kind == OP_CNT) {
+                // double-buffered: a warp may record substep s+1 while
+                // another still reads the counts of substep s
+                sm.nc[sub & 1][leg][j] = nc;
+                __syncthreads();
+            } else if (active) {
+                switch (kind) {
+                case OP_INT:
+                    // csrc/arc_phys.c:658-672
 #pragma unroll 1
-            for (int it = 1; it < 5; ++it) {
-                const int s = 5 * leg + 1 + it;
-                SphereState<F> ss{cget(sm, canch(it), tid), cget(sm, canch(it) + 3, tid), (int)((anch >> it) & 1u)};
-                const int t = collide(ti, Kt, txp, tqp, sm.sphere[s], ss, T, st, [&](V l, V n) { record(b_t, l, n); });
-                touches += (unsigned long long)t << (10 * it);
-                anch = (anch & ~(1u << it)) | ((uint32_t)(ss.anchored != 0) << it);
-                cset(sm, canch(it), tid, ss.anchor);
-                cset(sm, canch(it) + 3, tid, ss.anchor_n);
-            }
-            V v, w;
-            update_velocity(co.q, co.x, v, w, cget(sm, cxp(0), tid), cgetq(sm, cqp(0), tid), st);
-            cset(sm, cv(0), tid, v); cset(sm, cw(0), tid, w);
-            update_velocity(fe.q, fe.x, v, w, cget(sm, cxp(1), tid), cgetq(sm, cqp(1), tid), st);
-            cset(sm, cv(1), tid, v); cset(sm, cw(1), tid, w);
-            update_velocity(ti.q, ti.x, v, w, cget(sm, cxp(2), tid), cgetq(sm, cqp(2), tid), st);
-            cset(sm, cv(2), tid, v); cset(sm, cw(2), tid, w);
-        }
-        if (capped) {
-            // double-buffered: a warp may record substep s+1 while another
-            // still reads the counts of substep s
-            sm.nc[sub & 1][leg][j] = nc;
-            __syncthreads();
-        }
-
-        // drive damping, the same wavefront (csrc/arc_phys.c:700-705)
-        if (leg != 0)
-            bar_sync(vel_wait);
-        if (active) {
-            Body<true> to;
-            load_torso(sm, j, to);
-            V wp = tget(sm, 10, j), wc = cget(sm, cw(0), tid);
-            joint_velocities(to, wp, co, wc, sm.joint[j0], st.h, tacc[0]);
-            tset(sm, 10, j, wp);
-            cset(sm, cw(0), tid, wc);
-        }
-        bar_arrive(vel_done);
-        if (active) {
-            V wp = cget(sm, cw(0), tid), wc = cget(sm, cw(1), tid);
-            joint_velocities(co, wp, fe, wc, sm.joint[j0 + 1], st.h, tacc[1]);
-            cset(sm, cw(0), tid, wp);
-            wp = wc;
-            wc = cget(sm, cw(2), tid);
-            joint_velocities(fe, wp, ti, wc, sm.joint[j0 + 2], st.h, tacc[2]);
-            cset(sm, cw(1), tid, wp);
-            cset(sm, cw(2), tid, wc);
-        }
-
-        // contact velocities, in the reference's (leg-major) order under its
-        // cap; the torso's after the last torso joint
-        int base = 0;
-        if (capped && active)
-            for (int l = 0; l < leg; ++l)
-                base += sm.nc[sub & 1][l][j];
-        const int ncl = nc < lane_cap ? nc : lane_cap;
-#pragma unroll 1
-        for (int part = 0; part < 2; ++part) {
-            if (part == 1) {
-                if (leg != 0)
+                    for (int o = a; o < b; ++o) {
+                        const Ref r = body_ref(o == 0 ? kTorso : o - 1);
+                        const BodyK<F>& k = M.body[o == 0 ? 0 : b_c + o - 1];
+                        V x = getv(r, kX), v = getv(r, kV), w = getv(r, kW);
+                        const Q q0 = getq(r, kQP);
+                        setv(r, kXP, x);
+                        v = madd(v, st.gravity, st.h);
+                        x = madd(x, v, st.h);
+                        if (!k.iso) {
+                            const M3<F> rot = m3_from_quat(getq(r, kQ));
+                            w = mul(rot, gyroscopic(k, tmul(rot, w), st.h));
+                        }
+                        setv(r, kX, x);
+                        setq(r, kQ, q_turn(q0, scale(w, st.h)));
+                        setv(r, kV, v);
+                        setv(r, kW, w);
+                    }
                     break;
-                bar_sync(vel_wait);
-            }
-            if (!active)
-                continue;
-            for (int c = 0; c < ncl && base + c < kMaxContacts; ++c) {
-                F rc[7];
-                if (c < kOnChip) {
-#pragma unroll
-                    for (int f = 0; f < 7; ++f)
-                        rc[f] = sm.con[c * 7 + f][tid];
-                } else {
-                    const F* src = spill + (((size_t)wi * kWarps + leg) * (size_t)spill_per_lane + (c - kOnChip)) * 8;
-#pragma unroll
-                    for (int f = 0; f < 7; ++f)
-                        rc[f] = src[f];
+                case OP_JNT:
+#pragma unroll 1
+                    for (int c = a; c < b; ++c) {
+                        const Ref rp = body_ref(c == 0 ? kTorso : c - 1), rc = body_ref(c);
+                        const BodyK<F>& kp = M.body[c == 0 ? 0 : b_c + c - 1];
+                        const BodyK<F>& kc = M.body[b_c + c];
+                        P bp, bc;
+                        load_pose(rp, kp, bp);
+                        load_pose(rc, kc, bc);
+                        F acc = c == 0 ? tacc0 : (c == 1 ? tacc1 : tacc2);
+                        joint_positions(bp, kp, bc, kc, M.joint[j0 + c], c == 0 ? target0 : (c == 1 ? target1 : target2),
+                                        acc, st.hh);
+                        if (c == 0)
+                            tacc0 = acc;
+                        else if (c == 1)
+                            tacc1 = acc;
+                        else
+                            tacc2 = acc;
+                        store_pose(rp, bp);
+                        store_pose(rc, bc);
+                    }
+                    break;
+                case OP_COL: {
+                    // csrc/arc_phys.c:542-610, spheres a..b-1 of one body
+                    const int slot = a == 0 ? kTorso : (a == 1 ? 1 : 2);
+                    const int bid = a == 0 ? 0 : (a == 1 ? b_f : b_t);
+                    const Ref r = body_ref(slot);
+                    const BodyK<F>& k = M.body[bid];
+                    P pose;
+                    load_pose(r, k, pose);
+                    const V xp = getv(r, kXP);
+                    const Q qp = getq(r, kQP);
+#pragma unroll 1
+                    for (int s = a; s < b; ++s) {
+                        const int bit = s == 0 ? 5 : s - 1;
+                        const Ref ra = s == 0 ? Ref{&sm.torso[kBodyF][j], kWorlds} : Ref{&sm.anch[6 * (s - 1)][tid], kThreads};
+                        SphereState<F> ss{getv(ra, 0), getv(ra, 3), (int)((anch >> bit) & 1u)};
+                        const int t = collide(pose, k, xp, qp, M.sphere[s == 0 ? 0 : 5 * leg + s], ss, T, st,
+                                                     [&](V l, V n) { record(bid, l, n); });
+                        touches += (unsigned long long)t << (10 * bit);
+                        anch = (anch & ~(1u << bit)) | ((uint32_t)(ss.anchored != 0) << bit);
+                        setv(ra, 0, ss.anchor);
+                        setv(ra, 3, ss.anchor_n);
+                    }
+                    store_pose(r, pose);
+                    break;
                 }
-                const int b = (int)rc[6];
-                if ((b == 0) != (part == 1))
-                    continue;
-                const ContactRec<F> cr{V{rc[0], rc[1], rc[2]}, V{rc[3], rc[4], rc[5]}};
-                if (b == 0) {
-                    V v = tget(sm, 7, j), w = tget(sm, 10, j);
-                    Body<true> to;
-                    load_torso(sm, j, to);
-                    contact_velocity(to.rot, to.iw.s3(), K0.inv_mass, v, w, cr);
-                    tset(sm, 7, j, v);
-                    tset(sm, 10, j, w);
-                } else if (b == b_f) {
-                    V v = cget(sm, cv(1), tid), w = cget(sm, cw(1), tid);
-                    contact_velocity(fe.rot, fe.iw.m, Kf.inv_mass, v, w, cr);
-                    cset(sm, cv(1), tid, v);
-                    cset(sm, cw(1), tid, w);
-                } else {
-                    V v = cget(sm, cv(2), tid), w = cget(sm, cw(2), tid);
-                    contact_velocity(ti.rot, ti.iw.m, Kt.inv_mass, v, w, cr);
-                    cset(sm, cv(2), tid, v);
-                    cset(sm, cw(2), tid, w);
+                case OP_UPD:
+                    // csrc/arc_phys.c:674-687; the rotation stays that of the
+                    // un-normalised q (field Q)
+#pragma unroll 1
+                    for (int o = a; o < b; ++o) {
+                        const Ref r = body_ref(o == 0 ? kTorso : o - 1);
+                        Q q = getq(r, kQ);
+                        V v, w;
+                        update_velocity(q, getv(r, kX), v, w, getv(r, kXP), getq(r, kQP), st);
+                        setq(r, kQP, q);
+                        setv(r, kV, v);
+                        setv(r, kW, w);
+                    }
+                    break;
+                case OP_DMP:
+                    // csrc/arc_phys.c:459-481
+#pragma unroll 1
+                    for (int c = a; c < b; ++c) {
+                        const Ref rp = body_ref(c == 0 ? kTorso : c - 1), rc = body_ref(c);
+                        const BodyK<F>& kp = M.body[c == 0 ? 0 : b_c + c - 1];
+                        const BodyK<F>& kc = M.body[b_c + c];
+                        P bp, bc;
+                        bp.q = getq(rp, kQ);
+                        bc.q = getq(rc, kQ);
+                        body_sync(bp, kp);
+                        body_sync(bc, kc);
+                        V wp = getv(rp, kW), wc = getv(rc, kW);
+                        const JointK<F>& J = M.joint[j0 + c];
+                        F acc = c == 0 ? tacc0 : (c == 1 ? tacc1 : tacc2);
+                        joint_velocities<F, true>(bp.rot, bp.iiw, wp, bc.iiw, wc, J, joint_step_k(J, st), st.h, acc);
+                        if (c == 0)
+                            tacc0 = acc;
+                        else if (c == 1)
+                            tacc1 = acc;
+                        else
+                            tacc2 = acc;
+                        setv(rp, kW, wp);
+                        setv(rc, kW, wc);
+                    }
+                    break;
+                case OP_CVL: {
+                    // csrc/arc_phys.c:612-626, the reference's (sphere-major)
+                    // list order under its cap
+                    int base = 0;
+                    if (capped)
+                        for (int l = 0; l < leg; ++l)
+                            base += sm.nc[sub & 1][l][j];
+                    const int ncl = nc < lane_cap ? nc : lane_cap;
+#pragma unroll 1
+                    for (int c = 0; c < ncl && base + c < kMaxContacts; ++c) {
+                        F rc[7];
+                        if (c < kOnChip) {
+#pragma unroll
+                            for (int f = 0; f < 7; ++f)
+                                rc[f] = sm.con[c * 7 + f][tid];
+                        } else {
+                            const F* src =
+                                spill + (((size_t)wi * kWarps + leg) * (size_t)spill_per_lane + (c - kOnChip)) * 8;
+#pragma unroll
+                            for (int f = 0; f < 7; ++f)
+                                rc[f] = src[f];
+                        }
+                        const int bid = (int)rc[6];
+                        if ((bid == 0) != (a == 1))
+                            continue;
+                        const Ref r = body_ref(bid == 0 ? kTorso : (bid == b_f ? 1 : 2));
+                        const BodyK<F>& k = M.body[bid];
+                        P pose;
+                        pose.q = getq(r, kQ);
+                        body_sync(pose, k);
+                        V v = getv(r, kV), w = getv(r, kW);
+                        contact_velocity(pose.rot, pose.iiw, k.inv_mass, v, w,
+                                         ContactRec<F>{V{rc[0], rc[1], rc[2]}, V{rc[3], rc[4], rc[5]}});
+                        setv(r, kV, v);
+                        setv(r, kW, w);
+                    }
+                    break;
+                }
+                default:
+                    break;
                 }
             }
+            if (arrive)
+                bar_arrive(arrive);
         }
     }
     __syncthreads();
 
-    // epilogue (csrc/arc_phys.c:739-746)
+    // epilogue (csrc/arc_phys.c:739-746), from the normalised quaternions
     int bad = 0;
     if (active) {
-        const Q tq{sm.torso[3][j], sm.torso[4][j], sm.torso[5][j], sm.torso[6][j]};
-        const V tw = tget(sm, 10, j);
-        const V wc0 = cget(sm, cw(0), tid), wc1 = cget(sm, cw(1), tid), wc2 = cget(sm, cw(2), tid);
-        const JointK<F>& J0 = sm.joint[j0];
-        const JointK<F>& J1 = sm.joint[j0 + 1];
-        const JointK<F>& J2 = sm.joint[j0 + 2];
-        jr[(j0 + 0) * kJointRec + 1] = joint_angle(tq, co.q, J0);
-        jr[(j0 + 0) * kJointRec + 2] = joint_rate(tq, tw, wc0, J0);
-        jr[(j0 + 1) * kJointRec + 1] = joint_angle(co.q, fe.q, J1);
-        jr[(j0 + 1) * kJointRec + 2] = joint_rate(co.q, wc0, wc1, J1);
-        jr[(j0 + 2) * kJointRec + 1] = joint_angle(fe.q, ti.q, J2);
-        jr[(j0 + 2) * kJointRec + 2] = joint_rate(fe.q, wc1, wc2, J2);
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-            jr[(j0 + c) * kJointRec + 3] = tacc[c] / F(M.substeps);
-        bad |= body_unstable(co.x, cget(sm, cv(0), tid), wc0);
-        bad |= body_unstable(fe.x, cget(sm, cv(1), tid), wc1);
-        bad |= body_unstable(ti.x, cget(sm, cv(2), tid), wc2);
-        if (leg == 0)
-            bad |= body_unstable(tget(sm, 0, j), tget(sm, 7, j), tw);
-        // write back the leg's bodies and spheres
-        auto put = [&](int b, V x, Q q, V v, V w) {
-            F* r = rec + b * kBodyRec;
-            r[0] = x.x; r[1] = x.y; r[2] = x.z;
-            r[3] = q.w; r[4] = q.x; r[5] = q.y; r[6] = q.z;
-            r[7] = v.x; r[8] = v.y; r[9] = v.z;
-            r[10] = w.x; r[11] = w.y; r[12] = w.z;
+        const Ref r0 = body_ref(0), r1 = body_ref(1), r2 = body_ref(2);
+        const Q tq = getq(torso, kQP), q0 = getq(r0, kQP), q1 = getq(r1, kQP), q2 = getq(r2, kQP);
+        const V tw = getv(torso, kW), w0 = getv(r0, kW), w1 = getv(r1, kW), w2 = getv(r2, kW);
+        const JointK<F>& J0 = M.joint[j0];
+        const JointK<F>& J1 = M.joint[j0 + 1];
+        const JointK<F>& J2 = M.joint[j0 + 2];
+        jr[(j0 + 0) * kJointRec + 1] = joint_angle(tq, q0, J0);
+        jr[(j0 + 0) * kJointRec + 2] = joint_rate(tq, tw, w0, J0);
+        jr[(j0 + 1) * kJointRec + 1] = joint_angle(q0, q1, J1);
+        jr[(j0 + 1) * kJointRec + 2] = joint_rate(q0, w0, w1, J1);
+        jr[(j0 + 2) * kJointRec + 1] = joint_angle(q1, q2, J2);
+        jr[(j0 + 2) * kJointRec + 2] = joint_rate(q1, w1, w2, J2);
+        jr[(j0 + 0) * kJointRec + 3] = tacc0 / F(M.substeps);
+        jr[(j0 + 1) * kJointRec + 3] = tacc1 / F(M.substeps);
+        jr[(j0 + 2) * kJointRec + 3] = tacc2 / F(M.substeps);
+        auto put = [&](Ref r, F* d) {
+            const V x = getv(r, kX), v = getv(r, kV), w = getv(r, kW);
+            const Q q = getq(r, kQP);
+            bad |= body_unstable(x, v, w);
+            d[0] = x.x; d[1] = x.y; d[2] = x.z;
+            d[3] = q.w; d[4] = q.x; d[5] = q.y; d[6] = q.z;
+            d[7] = v.x; d[8] = v.y; d[9] = v.z;
+            d[10] = w.x; d[11] = w.y; d[12] = w.z;
         };
-        put(b_c, co.x, co.q, cget(sm, cv(0), tid), wc0);
-        put(b_f, fe.x, fe.q, cget(sm, cv(1), tid), wc1);
-        put(b_t, ti.x, ti.q, cget(sm, cv(2), tid), wc2);
+#pragma unroll 1
+        for (int i = 0; i < 3; ++i)
+            put(body_ref(i), rec + (b_c + i) * kBodyRec);
         uint32_t* sphw = W.sph + (size_t)world * 21;
 #pragma unroll
         for (int s = 0; s < 5; ++s) {
             F* a = sr + (5 * leg + 1 + s) * kSphereRec;
 #pragma unroll
             for (int c = 0; c < 6; ++c)
-                a[c] = sm.cold[canch(s) + c][tid];
+                a[c] = sm.anch[6 * s + c][tid];
             sphw[5 * leg + 1 + s] = (uint32_t)((touches >> (10 * s)) & 1023u) | (((anch >> s) & 1u) << 16);
         }
         if (leg == 0) {
-            for (int f = 0; f < 13; ++f)
-                rec[f] = sm.torso[f][j];
+            put(torso, rec);
 #pragma unroll
             for (int c = 0; c < 6; ++c)
-                sr[c] = sm.cold[canch(5) + c][tid];
+                sr[c] = torso[kBodyF + c];
             sphw[0] = (uint32_t)((touches >> 50) & 1023u) | (((anch >> 5) & 1u) << 16);
         }
     }
