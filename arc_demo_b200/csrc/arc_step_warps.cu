@@ -7,8 +7,10 @@
 // warp k-1 solved its own (a named barrier between the two warps, one
 // arrive and one sync), and everything else of leg k - its two other
 // joints, its five spheres, its three bodies' velocities - runs without
-// waiting. Warp 0 also owns the torso's integration, sphere and contact
-// velocities; it waits for warp 3 before the torso's sphere.
+// waiting. One warp also owns the torso's own work (its integration, its
+// sphere, its contact velocities): warp 3, right after it moved the torso
+// last, or warp 0 when contact lists can reach the reference's cap (the
+// torso sphere's contacts then have to lead warp 0's list).
 //
 // Code size decides this kernel's speed. With 12 warps of 3 CTAs per SM in
 // different phases of the step, a kernel whose code does not fit the SM's
@@ -16,7 +18,7 @@
 // phase is therefore one generic routine, run by a small interpreter over a
 // per-warp list of operations (integrate bodies a..b, solve joints a..b,
 // collide spheres a..b, ...): one copy of each routine, whatever the body.
-// The bodies live in shared memory ([field][lane], conflict-free); a
+// The bodies live in shared memory ([field][world], conflict-free); a
 // routine loads the few it works on, recomputes their rotation and world
 // inverse inertia from q (the same function of q as the reference's
 // body_sync, so the same values), and stores them back.
@@ -51,19 +53,20 @@ constexpr int kTorso = 3;  // body slot of the torso; 0..2: the lane's coxa, fem
 // warp read the same body, joint or sphere, a broadcast from the constant
 // cache.
 struct Smem {
-    F leg[3 * kBodyF][kThreads];      // the lane's three bodies
-    F anch[5 * 6][kThreads];          // anchor, anchor normal of the lane's five spheres
-    F con[kOnChip * 7][kThreads];     // on-chip contact records: local3 n3 body
+    F leg[kWarps][3 * kBodyF][kWorlds];   // the lane's three bodies
+    F anch[kWarps][5 * 6][kWorlds];       // anchor, anchor normal of the lane's five spheres
+    F con[kWarps][kOnChip * 7][kWorlds];  // on-chip contact records: local3 n3 body
     F torso[kBodyF + 6][kWorlds];     // each world's torso, then its sphere's anchor
     int nc[2][kWarps][kWorlds];       // contact counts (capped lists), by substep parity
     int bad[kWarps][kWorlds];
 };
 
-// a field array in shared memory: element f at p[f * s]
+// A field array in shared memory: element f at p[f * kWorlds]. Every
+// per-world array has the same row length, so fields are constant offsets
+// from the pointer whichever body it points at.
 struct Ref {
     F* p;
-    int s;
-    __device__ __forceinline__ F& operator[](int f) const { return p[f * s]; }
+    __device__ __forceinline__ F& operator[](int f) const { return p[f * kWorlds]; }
 };
 __device__ __forceinline__ V getv(Ref r, int f) { return V{r[f], r[f + 1], r[f + 2]}; }
 __device__ __forceinline__ void setv(Ref r, int f, V v)
@@ -305,39 +308,54 @@ __device__ __forceinline__ int collide(P& b, const BodyK<F>& k, V xprev, Q qprev
 }
 
 // per-warp operation lists: kind | a << 4 | b << 8 | wait << 12 | arrive << 16
+// | flags. An op with a wait first syncs on that named barrier; one with an
+// arrive arrives on it when done.
 enum : uint32_t { OP_END = 0, OP_INT, OP_JNT, OP_COL, OP_UPD, OP_DMP, OP_CVL, OP_CNT };
 // INT/UPD a..b: body ordinals (0 torso, 1..3 coxa, femur, tibia)
 // JNT/DMP a..b: the leg's joints (0 torso->coxa, 1 coxa->femur, 2 femur->tibia)
 // COL a..b: sphere ordinals on one body (0 torso sphere, 1 femur, 2..5 tibia)
 // CVL a: contact velocities of the leg's bodies (0) or of the torso (1)
 // CNT: publish the contact count, then __syncthreads (capped lists only)
+constexpr uint32_t kFirstOnly = 1u << 20;  // only in the first substep
+constexpr uint32_t kNotLast = 1u << 21;    // not in the last substep
 #define ARC_OP(kind, a, b, w, r) ((kind) | (a) << 4 | (b) << 8 | (w) << 12 | (r) << 16)
-#define ARC_LEG_OPS(k, cnt)                                                                                       \
-    {ARC_OP(OP_INT, 1, 4, 0, 0), ARC_OP(OP_JNT, 0, 1, k, k + 1), ARC_OP(OP_JNT, 1, 3, 0, 0),                      \
-     ARC_OP(OP_COL, 1, 2, 0, 0), ARC_OP(OP_COL, 2, 6, 0, 0), ARC_OP(OP_UPD, 1, 4, 0, 0), cnt,                     \
+// Uncapped lists. Warp 3 owns the torso's own work: it is the warp that
+// has just moved the torso (joint 9 before the torso's sphere, joint 9's
+// drive damping before the torso's contact velocities), and it integrates
+// the torso for the next substep at once, so the chain of torso hand-offs
+// (joints 0, 3, 6, 9; damping 0, 3, 6, 9) never waits for a warp busy with
+// its own leg. Each warp solves what the next hand-off needs first (its
+// coxa's velocity right after joint 3k+1, the only other joint that moves
+// the coxa) and the rest of its leg while the chain runs elsewhere; work on
+// different bodies commutes, so this is the reference's order.
+#define ARC_LEG_OPS(k)                                                                                         \
+    {ARC_OP(OP_INT, 1, 4, 0, 0), ARC_OP(OP_JNT, 0, 1, (k) == 0 ? 8 : (k), (k) + 1), ARC_OP(OP_JNT, 1, 2, 0, 0), \
+     ARC_OP(OP_UPD, 1, 2, 0, 0), ARC_OP(OP_DMP, 0, 1, 4 + (k), 5 + (k)), ARC_OP(OP_JNT, 2, 3, 0, 0),            \
+     ARC_OP(OP_COL, 1, 2, 0, 0), ARC_OP(OP_COL, 2, 6, 0, 0), ARC_OP(OP_UPD, 2, 4, 0, 0), ARC_OP(OP_DMP, 1, 3, 0, 0), \
+     ARC_OP(OP_CVL, 0, 0, 0, 0), OP_END}
+// Capped lists: warp 0 owns the torso, whose sphere's contacts lead the
+// list as sphere 0 leads the reference's, and every lane's count is
+// published before any contact velocity.
+#define ARC_CAPPED_OPS(k)                                                                                           \
+    {ARC_OP(OP_INT, 1, 4, 0, 0), ARC_OP(OP_JNT, 0, 1, k, k + 1), ARC_OP(OP_JNT, 1, 3, 0, 0),                        \
+     ARC_OP(OP_COL, 1, 2, 0, 0), ARC_OP(OP_COL, 2, 6, 0, 0), ARC_OP(OP_UPD, 1, 4, 0, 0), ARC_OP(OP_CNT, 0, 0, 0, 0), \
      ARC_OP(OP_DMP, 0, 1, 4 + k, 5 + k), ARC_OP(OP_DMP, 1, 3, 0, 0), ARC_OP(OP_CVL, 0, 0, 0, 0), OP_END}
-#define ARC_NOP ARC_OP(OP_UPD, 0, 0, 0, 0)  // an empty range
-#define ARC_CNT ARC_OP(OP_CNT, 0, 0, 0, 0)
 
-constexpr int kMaxOps = 16;
+constexpr int kMaxOps = 20;
 __constant__ uint32_t kOps[2][kWarps][kMaxOps] = {
-    // contact lists that cannot reach the cap: warp 0 takes the torso sphere
-    // after its own leg (the contacts of different bodies commute)
-    {{ARC_OP(OP_INT, 0, 2, 0, 0), ARC_OP(OP_JNT, 0, 1, 0, 1), ARC_OP(OP_INT, 2, 4, 0, 0), ARC_OP(OP_JNT, 1, 3, 0, 0),
-      ARC_OP(OP_COL, 1, 2, 0, 0), ARC_OP(OP_COL, 2, 6, 0, 0), ARC_OP(OP_UPD, 1, 4, 0, 0), ARC_OP(OP_COL, 0, 1, 4, 0),
-      ARC_OP(OP_UPD, 0, 1, 0, 0), ARC_OP(OP_DMP, 0, 1, 0, 5), ARC_OP(OP_DMP, 1, 3, 0, 0), ARC_OP(OP_CVL, 0, 0, 0, 0),
-      ARC_OP(OP_CVL, 1, 0, 8, 0), OP_END},
-     ARC_LEG_OPS(1, ARC_NOP), ARC_LEG_OPS(2, ARC_NOP), ARC_LEG_OPS(3, ARC_NOP)},
-    // capped lists: the torso sphere's contacts lead, as sphere 0 leads the
-    // reference's list, and every lane's count is published
+    {ARC_LEG_OPS(0), ARC_LEG_OPS(1), ARC_LEG_OPS(2),
+     {ARC_OP(OP_INT, 0, 1, 0, 8) | kFirstOnly, ARC_OP(OP_INT, 1, 4, 0, 0), ARC_OP(OP_JNT, 0, 1, 3, 0),
+      ARC_OP(OP_COL, 0, 1, 0, 0), ARC_OP(OP_UPD, 0, 1, 0, 4), ARC_OP(OP_JNT, 1, 2, 0, 0), ARC_OP(OP_UPD, 1, 2, 0, 0),
+      ARC_OP(OP_DMP, 0, 1, 7, 0), ARC_OP(OP_CVL, 1, 0, 0, 0), ARC_OP(OP_INT, 0, 1, 0, 8) | kNotLast,
+      ARC_OP(OP_JNT, 2, 3, 0, 0), ARC_OP(OP_COL, 1, 2, 0, 0), ARC_OP(OP_COL, 2, 6, 0, 0), ARC_OP(OP_UPD, 2, 4, 0, 0),
+      ARC_OP(OP_DMP, 1, 3, 0, 0), ARC_OP(OP_CVL, 0, 0, 0, 0), OP_END}},
     {{ARC_OP(OP_INT, 0, 2, 0, 0), ARC_OP(OP_JNT, 0, 1, 0, 1), ARC_OP(OP_INT, 2, 4, 0, 0), ARC_OP(OP_JNT, 1, 3, 0, 0),
       ARC_OP(OP_COL, 0, 1, 4, 0), ARC_OP(OP_UPD, 0, 1, 0, 0), ARC_OP(OP_COL, 1, 2, 0, 0), ARC_OP(OP_COL, 2, 6, 0, 0),
-      ARC_OP(OP_UPD, 1, 4, 0, 0), ARC_CNT, ARC_OP(OP_DMP, 0, 1, 0, 5), ARC_OP(OP_DMP, 1, 3, 0, 0),
+      ARC_OP(OP_UPD, 1, 4, 0, 0), ARC_OP(OP_CNT, 0, 0, 0, 0), ARC_OP(OP_DMP, 0, 1, 0, 5), ARC_OP(OP_DMP, 1, 3, 0, 0),
       ARC_OP(OP_CVL, 0, 0, 0, 0), ARC_OP(OP_CVL, 1, 0, 8, 0), OP_END},
-     ARC_LEG_OPS(1, ARC_CNT), ARC_LEG_OPS(2, ARC_CNT), ARC_LEG_OPS(3, ARC_CNT)}};
+     ARC_CAPPED_OPS(1), ARC_CAPPED_OPS(2), ARC_CAPPED_OPS(3)}};
 #undef ARC_LEG_OPS
-#undef ARC_NOP
-#undef ARC_CNT
+#undef ARC_CAPPED_OPS
 #undef ARC_OP
 
 // ---------------------------------------------------------------------------
@@ -358,9 +376,9 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
     F* jr = rec + W.off_joint;
     const int b_c = 1 + 3 * leg, b_f = 2 + 3 * leg, b_t = 3 + 3 * leg;  // coxa, femur, tibia
     const int j0 = 3 * leg;
-    const Ref torso{&sm.torso[0][j], kWorlds};
+    const Ref torso{&sm.torso[0][j]};
     auto body_ref = [&](int slot) {
-        return slot == kTorso ? torso : Ref{&sm.leg[slot * kBodyF][tid], kThreads};
+        return slot == kTorso ? torso : Ref{&sm.leg[leg][slot * kBodyF][j]};
     };
     // actuation (csrc/arc_sim.c:132-136)
     F target0 = F(0), target1 = F(0), target2 = F(0);
@@ -391,20 +409,23 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
         const F* a = sr + (5 * leg + 1 + s) * kSphereRec;
 #pragma unroll
         for (int c = 0; c < 6; ++c)
-            sm.anch[6 * s + c][tid] = a[c];
+            sm.anch[leg][6 * s + c][j] = a[c];
         anch |= ((sphr[5 * leg + 1 + s] >> 16) & 1u) << s;
     }
+    // the warp that collides the torso's sphere keeps its flags
+    const bool capped = kWarps * lane_cap > kMaxContacts;
+    const int torso_warp = capped ? 0 : kWarps - 1;
     if (leg == 0) {
         stage_body(torso, rec);
 #pragma unroll
         for (int c = 0; c < 6; ++c)
             torso[kBodyF + c] = sr[c];
-        anch |= ((sphr[0] >> 16) & 1u) << 5;
     }
+    if (leg == torso_warp)
+        anch |= ((sphr[0] >> 16) & 1u) << 5;
     const TerrainView<F> T = terrain_of(W, wi);
     const StepK<F>& st = M.step;
     unsigned long long touches = 0;  // 10 bits per sphere: leg spheres 0..4, torso sphere at 50
-    const bool capped = kWarps * lane_cap > kMaxContacts;
     const uint32_t* ops = &kOps[capped ? 1 : 0][leg][0];
     __syncthreads();
 
@@ -412,10 +433,10 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
         int nc = 0;
         auto record = [&](int body, V local, V n) {
             if (nc < kOnChip) {
-                F* d = &sm.con[nc * 7][tid];
-                d[0] = local.x; d[kThreads] = local.y; d[2 * kThreads] = local.z;
-                d[3 * kThreads] = n.x; d[4 * kThreads] = n.y; d[5 * kThreads] = n.z;
-                d[6 * kThreads] = (F)body;
+                const Ref d{&sm.con[leg][nc * 7][j]};
+                setv(d, 0, local);
+                setv(d, 3, n);
+                d[6] = (F)body;
             } else if (nc < lane_cap) {
                 F* d = spill + (((size_t)wi * kWarps + leg) * (size_t)spill_per_lane + (nc - kOnChip)) * 8;
                 d[0] = local.x; d[1] = local.y; d[2] = local.z;
@@ -430,6 +451,8 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
             const uint32_t kind = op & 15u;
             if (kind == OP_END)
                 break;
+            if (((op & kFirstOnly) && sub != 0) || ((op & kNotLast) && sub == M.substeps - 1))
+                continue;
             const int a = (op >> 4) & 15, b = (op >> 8) & 15, wait = (op >> 12) & 15, arrive = (op >> 16) & 15;
             if (wait)
                 bar_sync(wait);
@@ -496,7 +519,7 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
 #pragma unroll 1
                     for (int s = a; s < b; ++s) {
                         const int bit = s == 0 ? 5 : s - 1;
-                        const Ref ra = s == 0 ? Ref{&sm.torso[kBodyF][j], kWorlds} : Ref{&sm.anch[6 * (s - 1)][tid], kThreads};
+                        const Ref ra{s == 0 ? &sm.torso[kBodyF][j] : &sm.anch[leg][6 * (s - 1)][j]};
                         SphereState<F> ss{getv(ra, 0), getv(ra, 3), (int)((anch >> bit) & 1u)};
                         const int t = collide(pose, k, xp, qp, M.sphere[s == 0 ? 0 : 5 * leg + s], ss, T, st,
                                                      [&](V l, V n) { record(bid, l, n); });
@@ -522,19 +545,20 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
                         setv(r, kW, w);
                     }
                     break;
-                case OP_DMP:
-                    // csrc/arc_phys.c:459-481
+                case OP_DMP: {
+                    // csrc/arc_phys.c:459-481; the child of joint c is the
+                    // parent of joint c+1 (rotation of the position pass)
+                    P bp, bc;
+                    Ref rp = body_ref(a == 0 ? kTorso : a - 1);
+                    bp.q = getq(rp, kQ);
+                    body_sync(bp, M.body[a == 0 ? 0 : b_c + a - 1]);
+                    V wp = getv(rp, kW);
 #pragma unroll 1
                     for (int c = a; c < b; ++c) {
-                        const Ref rp = body_ref(c == 0 ? kTorso : c - 1), rc = body_ref(c);
-                        const BodyK<F>& kp = M.body[c == 0 ? 0 : b_c + c - 1];
-                        const BodyK<F>& kc = M.body[b_c + c];
-                        P bp, bc;
-                        bp.q = getq(rp, kQ);
+                        const Ref rc = body_ref(c);
                         bc.q = getq(rc, kQ);
-                        body_sync(bp, kp);
-                        body_sync(bc, kc);
-                        V wp = getv(rp, kW), wc = getv(rc, kW);
+                        body_sync(bc, M.body[b_c + c]);
+                        V wc = getv(rc, kW);
                         const JointK<F>& J = M.joint[j0 + c];
                         F acc = c == 0 ? tacc0 : (c == 1 ? tacc1 : tacc2);
                         joint_velocities<F, true>(bp.rot, bp.iiw, wp, bc.iiw, wc, J, joint_step_k(J, st), st.h, acc);
@@ -545,9 +569,13 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
                         else
                             tacc2 = acc;
                         setv(rp, kW, wp);
-                        setv(rc, kW, wc);
+                        rp = rc;
+                        bp = bc;
+                        wp = wc;
                     }
+                    setv(rp, kW, wp);
                     break;
+                }
                 case OP_CVL: {
                     // csrc/arc_phys.c:612-626, the reference's (sphere-major)
                     // list order under its cap
@@ -562,7 +590,7 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
                         if (c < kOnChip) {
 #pragma unroll
                             for (int f = 0; f < 7; ++f)
-                                rc[f] = sm.con[c * 7 + f][tid];
+                                rc[f] = sm.con[leg][c * 7 + f][j];
                         } else {
                             const F* src =
                                 spill + (((size_t)wi * kWarps + leg) * (size_t)spill_per_lane + (c - kOnChip)) * 8;
@@ -632,11 +660,12 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
             F* a = sr + (5 * leg + 1 + s) * kSphereRec;
 #pragma unroll
             for (int c = 0; c < 6; ++c)
-                a[c] = sm.anch[6 * s + c][tid];
+                a[c] = sm.anch[leg][6 * s + c][j];
             sphw[5 * leg + 1 + s] = (uint32_t)((touches >> (10 * s)) & 1023u) | (((anch >> s) & 1u) << 16);
         }
-        if (leg == 0) {
+        if (leg == 0)
             put(torso, rec);
+        if (leg == torso_warp) {
 #pragma unroll
             for (int c = 0; c < 6; ++c)
                 sr[c] = torso[kBodyF + c];
