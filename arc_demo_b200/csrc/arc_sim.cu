@@ -54,6 +54,10 @@ struct arc_sim {
     void* tg = nullptr;
     TerrainGeomD* tgd = nullptr;
     int* grid_of = nullptr;
+    std::vector<int> grid_host;  // terrain capacity of each world: grid_host[i]^2 columns
+    size_t th_count = 0;         // columns in the terrain pool
+    int* queue = nullptr;        // work queue of the warp-per-leg kernel (two ints)
+    bool use_queue = false;
     void* spill = nullptr;
     int spill_per_lane = 0, lane_cap = 0;
     double spill_cell = 0.0;
@@ -209,22 +213,28 @@ template <class R> int init_worlds(arc_sim* s)
     if (check(s, cudaMemcpy(s->rec, all.data(), sizeof(R) * all.size(), cudaMemcpyHostToDevice), "init records"))
         return ARC_ERR_CUDA;
     // flat terrain, outside at the same height (csrc/arc_sim.c:37: template terrain)
+    // the pool packs each world's grid_host[i]^2 columns
     std::vector<long long> toff(n);
     std::vector<TerrainGeom<R>> tg(n);
     std::vector<TerrainGeomD> tgd(n);
-    std::vector<int> grid_of(n, g);
-    TerrainGeomD gd{g, g, s->cell, -0.5 * g * s->cell, -0.5 * g * s->cell, 0.0};
+    const std::vector<int>& grid_of = s->grid_host;
+    long long off = 0;
     for (int i = 0; i < n; ++i) {
-        toff[i] = (long long)i * kGridMax * kGridMax;
+        const int gi = grid_of[i];
+        toff[i] = off;
+        off += (long long)gi * gi;
+        const TerrainGeomD gd{gi, gi, s->cell, -0.5 * gi * s->cell, -0.5 * gi * s->cell, 0.0};
         tgd[i] = gd;
-        tg[i] = TerrainGeom<R>{g, g, (R)gd.cell, (R)gd.ox, (R)gd.oy, (R)gd.outside};
+        tg[i] = TerrainGeom<R>{gi, gi, (R)gd.cell, (R)gd.ox, (R)gd.oy, (R)gd.outside};
     }
+    (void)g;
     int rc = ARC_OK;
     rc |= check(s, cudaMemcpy(s->toff, toff.data(), sizeof(long long) * n, cudaMemcpyHostToDevice), "init toff");
     rc |= check(s, cudaMemcpy(s->tg, tg.data(), sizeof(TerrainGeom<R>) * n, cudaMemcpyHostToDevice), "init tg");
     rc |= check(s, cudaMemcpy(s->tgd, tgd.data(), sizeof(TerrainGeomD) * n, cudaMemcpyHostToDevice), "init tgd");
     rc |= check(s, cudaMemcpy(s->grid_of, grid_of.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "init grid");
-    rc |= check(s, cudaMemset(s->th, 0, sizeof(R) * (size_t)n * kGridMax * kGridMax), "init terrain");
+    rc |= check(s, cudaMemset(s->th, 0, sizeof(R) * s->th_count), "init terrain");
+    rc |= check(s, cudaMemset(s->queue, 0, 2 * sizeof(int)), "init queue");
     rc |= check(s, cudaMemset(s->sph, 0, sizeof(uint32_t) * (size_t)n * std::max(s->model.ns, 1)), "init spheres");
     rc |= check(s, cudaMemset(s->unstable, 0, sizeof(int) * n), "init flags");
     rc |= check(s, cudaMemset(s->time, 0, sizeof(double) * n), "init time");
@@ -239,7 +249,7 @@ void free_all(arc_sim* s)
         cudaGraphDestroy(s->graph);
     for (void* p : s->env_allocs)
         cudaFree(p);
-    void* ps[] = {s->rec, s->sph, s->unstable, s->time, s->th, s->toff, s->tg, s->tgd, s->grid_of, s->spill,
+    void* ps[] = {s->rec, s->sph, s->unstable, s->time, s->th, s->toff, s->tg, s->tgd, s->grid_of, s->spill, s->queue,
                   s->st_in.p, s->st_in2.p, s->st_in3.p, s->st_out.p};
     for (void* p : ps)
         if (p)
@@ -250,7 +260,7 @@ void free_all(arc_sim* s)
 }
 
 arc_sim* create_with_model(const ModelHost& model, int n, double dt, int substeps, int grid, double cell,
-                           unsigned flags)
+                           unsigned flags, const int* grids = nullptr)
 {
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
@@ -265,6 +275,12 @@ arc_sim* create_with_model(const ModelHost& model, int n, double dt, int substep
     s->substeps = substeps;
     s->grid = std::max(1, std::min(grid, kGridMax));
     s->cell = cell;
+    s->grid_host.assign((size_t)std::max(n, 0), s->grid);
+    if (grids)
+        for (int i = 0; i < n; ++i)
+            s->grid_host[i] = grids[i];
+    for (int g : s->grid_host)
+        s->th_count += (size_t)g * g;
     s->fp64 = (flags & ARC_SIM_FP64) != 0;
     s->model = model;
     rebuild_models(s);
@@ -285,7 +301,8 @@ arc_sim* create_with_model(const ModelHost& model, int n, double dt, int substep
     ok = ok && cudaMalloc((void**)&s->sph, nn * std::max(s->model.ns, 1) * sizeof(uint32_t)) == cudaSuccess;
     ok = ok && cudaMalloc((void**)&s->unstable, nn * sizeof(int)) == cudaSuccess;
     ok = ok && cudaMalloc((void**)&s->time, nn * sizeof(double)) == cudaSuccess;
-    ok = ok && cudaMalloc(&s->th, nn * kGridMax * kGridMax * rs) == cudaSuccess;
+    ok = ok && cudaMalloc(&s->th, std::max<size_t>(s->th_count, 1) * rs) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&s->queue, 2 * sizeof(int)) == cudaSuccess;
     ok = ok && cudaMalloc((void**)&s->toff, nn * sizeof(long long)) == cudaSuccess;
     ok = ok && cudaMalloc(&s->tg, nn * (s->fp64 ? sizeof(TerrainGeom<double>) : sizeof(TerrainGeom<float>))) ==
                    cudaSuccess;
@@ -319,33 +336,39 @@ template <> const DevModel<float>& dev_model<float>(const arc_sim* s) { return s
 template <> const DevModel<double>& dev_model<double>(const arc_sim* s) { return s->md; }
 
 template <class R> cudaError_t launch_warps_if_fp32(arc_sim*, const DevModel<R>&, const Worlds<R>&, const Actuation&,
-                                                   cudaStream_t)
+                                                   const int*, int, cudaStream_t)
 {
     return cudaErrorNotSupported;
 }
 template <> cudaError_t launch_warps_if_fp32<float>(arc_sim* s, const DevModel<float>& M, const Worlds<float>& W,
-                                                    const Actuation& A, cudaStream_t st)
+                                                    const Actuation& A, const int* ids, int n_items, cudaStream_t st)
 {
-    return launch_step_warps(M, W, A, static_cast<float*>(s->spill), s->spill_per_lane, s->lane_cap, st);
+    return launch_step_warps(M, W, A, static_cast<float*>(s->spill), s->spill_per_lane, s->lane_cap, ids, n_items,
+                             s->use_queue ? s->queue : nullptr, st);
 }
 
-template <class R> int step_impl(arc_sim* s, const Actuation& A, cudaStream_t st)
+// ids: device list of n_ids distinct worlds to step (NULL: all worlds).
+// A subset is stepped by the warp-per-leg kernel (FP32 quadruped) or the
+// plain kernel; the leg-parallel kernel steps whole batches only.
+template <class R> int step_impl(arc_sim* s, const Actuation& A, cudaStream_t st, const int* ids, int n_ids)
 {
     const Worlds<R> W = view<R>(s);
     const DevModel<R>& M = dev_model<R>(s);
+    const int n_items = ids ? n_ids : s->n;
+    const bool warps_ok = !s->fp64 && M.leaper && s->substeps <= kFastMaxSubsteps;
     cudaError_t e;
-    if (s->kernel == ARC_KERNEL_WARPS && !s->fp64 && M.leaper && s->substeps <= kFastMaxSubsteps)
-        e = launch_warps_if_fp32<R>(s, M, W, A, st);
-    else if (s->kernel == ARC_KERNEL_LEGS && M.leaper && s->substeps <= kFastMaxSubsteps)
+    if (warps_ok && (s->kernel == ARC_KERNEL_WARPS || (ids && s->kernel == ARC_KERNEL_LEGS)))
+        e = launch_warps_if_fp32<R>(s, M, W, A, ids, n_items, st);
+    else if (!ids && s->kernel == ARC_KERNEL_LEGS && M.leaper && s->substeps <= kFastMaxSubsteps)
         e = launch_step_fast<R>(M, W, A, static_cast<R*>(s->spill), s->spill_per_lane, s->lane_cap, s->wpc, st);
     else
-        e = launch_step_plain<R>(M, W, A, nullptr, s->n, st);
+        e = launch_step_plain<R>(M, W, A, ids, n_items, st);
     return check(s, e, "step kernel");
 }
 
-int step_any(arc_sim* s, const Actuation& A, cudaStream_t st)
+int step_any(arc_sim* s, const Actuation& A, cudaStream_t st, const int* ids = nullptr, int n_ids = 0)
 {
-    return s->fp64 ? step_impl<double>(s, A, st) : step_impl<float>(s, A, st);
+    return s->fp64 ? step_impl<double>(s, A, st, ids, n_ids) : step_impl<float>(s, A, st, ids, n_ids);
 }
 
 cudaStream_t stream_of(const arc_sim* s, void* stream) { return stream ? (cudaStream_t)stream : s->stream; }
@@ -735,6 +758,8 @@ int arc_sim_set_terrain(arc_sim* s, int id, int nx, int ny, double cell, double 
 {
     if (id < 0 || id >= s->n || nx <= 0 || ny <= 0 || nx > kGridMax || ny > kGridMax || !(cell > 0.0))
         return fail(s, ARC_ERR_ARG, "arc_sim_set_terrain: bad world index or grid size");
+    if ((long long)nx * ny > (long long)s->grid_host[id] * s->grid_host[id])
+        return fail(s, ARC_ERR_ARG, "arc_sim_set_terrain: more columns than the world's terrain holds");
     if (ensure_spill(s, cell) != ARC_OK)
         return ARC_ERR_CUDA;
     double* d = (double*)grow(s, s->st_in, sizeof(double) * nx * ny);
@@ -901,6 +926,40 @@ int arc_sim_step_actions(arc_sim* s, const float* d_actions, void* stream)
 {
     Actuation A{nullptr, d_actions};
     return step_any(s, A, stream_of(s, stream));
+}
+
+int arc_sim_step_ids(arc_sim* s, const int* d_ids, int n_ids, const double* d_targets, const float* d_actions,
+                     void* stream)
+{
+    if (n_ids < 0 || (n_ids > 0 && !d_ids) || (!d_targets) == (!d_actions))
+        return fail(s, ARC_ERR_ARG, "arc_sim_step_ids: need ids and exactly one of targets, actions");
+    if (n_ids == 0)
+        return ARC_OK;
+    Actuation A{d_targets, d_actions};
+    return step_any(s, A, stream_of(s, stream), d_ids, n_ids);
+}
+
+int arc_sim_set_work_queue(arc_sim* s, int on)
+{
+    s->use_queue = on != 0;
+    return ARC_OK;
+}
+
+arc_sim* arc_sim_create_sized(int n_worlds, const int* grids, double dt, int substeps, double cell, unsigned flags)
+{
+    if (n_worlds < 0 || (n_worlds > 0 && !grids))
+        return nullptr;
+    int gmax = 1;
+    for (int i = 0; i < n_worlds; ++i) {
+        if (grids[i] < 1 || grids[i] > kGridMax) {
+            std::fprintf(stderr, "arc_sim_create_sized: world %d: grid %d outside 1..%d\n", i, grids[i], kGridMax);
+            return nullptr;
+        }
+        gmax = std::max(gmax, grids[i]);
+    }
+    ModelHost m;
+    build_leaper(m);
+    return create_with_model(m, n_worlds, dt, substeps, gmax, cell, flags, grids);
 }
 
 int arc_sim_observe_device(const arc_sim* s, double* root, double* rot, double* joints, double* contacts, int* flags,

@@ -19,6 +19,8 @@ k_step_plain(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, co
     if (k >= n_ids)
         return;
     const int i = ids ? ids[k] : k;
+    if (i < 0 || i >= W.n)
+        return;
     R* rec = W.rec + (size_t)i * W.stride;
     R* jr = rec + W.off_joint;
     R* sr = rec + W.off_sphere;

@@ -360,324 +360,352 @@ __constant__ uint32_t kOps[2][kWarps][kMaxOps] = {
 
 // ---------------------------------------------------------------------------
 
+// Work items are worlds (ids[item], or item itself without ids), 32 to a
+// group; CTA b steps group b. With a queue (two ints, zero before the
+// launch), a CTA that finished its group takes the next unclaimed one, and
+// the last CTA to leave zeroes the queue again for the next launch.
 __global__ void __launch_bounds__(kThreads, 4)
 k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F* __restrict__ spill, int spill_per_lane,
-             int lane_cap)
+             int lane_cap, const int* __restrict__ ids, int n_items, int* queue)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+    __shared__ int s_next;
     const int tid = threadIdx.x, leg = tid / kWorlds, j = tid % kWorlds;
-    const int world = blockIdx.x * kWorlds + j;
-    const bool valid = world < W.n;
-    const int wi = valid ? world : 0;
-
-    F* rec = W.rec + (size_t)wi * W.stride;
-    F* sr = rec + W.off_sphere;
-    F* jr = rec + W.off_joint;
-    const int b_c = 1 + 3 * leg, b_f = 2 + 3 * leg, b_t = 3 + 3 * leg;  // coxa, femur, tibia
-    const int j0 = 3 * leg;
-    const Ref torso{&sm.torso[0][j]};
-    auto body_ref = [&](int slot) {
-        return slot == kTorso ? torso : Ref{&sm.leg[leg][slot * kBodyF][j]};
-    };
-    // actuation (csrc/arc_sim.c:132-136)
-    F target0 = F(0), target1 = F(0), target2 = F(0);
-    if (valid) {
-        target0 = actuate(M, A, world, j0);
-        target1 = actuate(M, A, world, j0 + 1);
-        target2 = actuate(M, A, world, j0 + 2);
-        jr[j0 * kJointRec] = target0;
-        jr[(j0 + 1) * kJointRec] = target1;
-        jr[(j0 + 2) * kJointRec] = target2;
-    }
-    F tacc0 = F(0), tacc1 = F(0), tacc2 = F(0);
-    const bool active = valid && W.unstable[wi] == 0;
-    auto stage_body = [&](Ref r, const F* src) {
-        setv(r, kX, V{src[0], src[1], src[2]});
-        setq(r, kQ, Q{src[3], src[4], src[5], src[6]});
-        setq(r, kQP, Q{src[3], src[4], src[5], src[6]});
-        setv(r, kV, V{src[7], src[8], src[9]});
-        setv(r, kW, V{src[10], src[11], src[12]});
-    };
+    const int n_groups = (n_items + kWorlds - 1) / kWorlds;
 #pragma unroll 1
-    for (int i = 0; i < 3; ++i)
-        stage_body(body_ref(i), rec + (b_c + i) * kBodyRec);
-    uint32_t anch = 0;
-    const uint32_t* sphr = W.sph + (size_t)wi * 21;
-#pragma unroll
-    for (int s = 0; s < 5; ++s) {
-        const F* a = sr + (5 * leg + 1 + s) * kSphereRec;
-#pragma unroll
-        for (int c = 0; c < 6; ++c)
-            sm.anch[leg][6 * s + c][j] = a[c];
-        anch |= ((sphr[5 * leg + 1 + s] >> 16) & 1u) << s;
-    }
-    // the warp that collides the torso's sphere keeps its flags
-    const bool capped = kWarps * lane_cap > kMaxContacts;
-    const int torso_warp = capped ? 0 : kWarps - 1;
-    if (leg == 0) {
-        stage_body(torso, rec);
-#pragma unroll
-        for (int c = 0; c < 6; ++c)
-            torso[kBodyF + c] = sr[c];
-    }
-    if (leg == torso_warp)
-        anch |= ((sphr[0] >> 16) & 1u) << 5;
-    const TerrainView<F> T = terrain_of(W, wi);
-    const StepK<F>& st = M.step;
-    unsigned long long touches = 0;  // 10 bits per sphere: leg spheres 0..4, torso sphere at 50
-    const uint32_t* ops = &kOps[capped ? 1 : 0][leg][0];
-    __syncthreads();
+    for (int group = blockIdx.x; group < n_groups;) {
+        const int item = group * kWorlds + j;
+        const int world = item < n_items ? (ids ? ids[item] : item) : -1;
+        const bool valid = world >= 0 && world < W.n;
+        const int wi = valid ? world : 0;
 
-    for (int sub = 0; sub < M.substeps; ++sub) {
-        int nc = 0;
-        auto record = [&](int body, V local, V n) {
-            if (nc < kOnChip) {
-                const Ref d{&sm.con[leg][nc * 7][j]};
-                setv(d, 0, local);
-                setv(d, 3, n);
-                d[6] = (F)body;
-            } else if (nc < lane_cap) {
-                F* d = spill + (((size_t)wi * kWarps + leg) * (size_t)spill_per_lane + (nc - kOnChip)) * 8;
-                d[0] = local.x; d[1] = local.y; d[2] = local.z;
-                d[3] = n.x; d[4] = n.y; d[5] = n.z;
-                d[6] = (F)body;
-            }
-            ++nc;
+        F* rec = W.rec + (size_t)wi * W.stride;
+        F* sr = rec + W.off_sphere;
+        F* jr = rec + W.off_joint;
+        const int b_c = 1 + 3 * leg, b_f = 2 + 3 * leg, b_t = 3 + 3 * leg;  // coxa, femur, tibia
+        const int j0 = 3 * leg;
+        const Ref torso{&sm.torso[0][j]};
+        auto body_ref = [&](int slot) {
+            return slot == kTorso ? torso : Ref{&sm.leg[leg][slot * kBodyF][j]};
         };
-#pragma unroll 1
-        for (int i = 0;; ++i) {
-            const uint32_t op = ops[i];
-            const uint32_t kind = op & 15u;
-            if (kind == OP_END)
-                break;
-            if (((op & kFirstOnly) && sub != 0) || ((op & kNotLast) && sub == M.substeps - 1))
-                continue;
-            const int a = (op >> 4) & 15, b = (op >> 8) & 15, wait = (op >> 12) & 15, arrive = (op >> 16) & 15;
-            if (wait)
-                bar_sync(wait);
-            if (kind == OP_CNT) {
-                // double-buffered: a warp may record substep s+1 while
-                // another still reads the counts of substep s
-                sm.nc[sub & 1][leg][j] = nc;
-                __syncthreads();
-            } else if (active) {
-                switch (kind) {
-                case OP_INT:
-                    // csrc/arc_phys.c:658-672
-#pragma unroll 1
-                    for (int o = a; o < b; ++o) {
-                        const Ref r = body_ref(o == 0 ? kTorso : o - 1);
-                        const BodyK<F>& k = M.body[o == 0 ? 0 : b_c + o - 1];
-                        V x = getv(r, kX), v = getv(r, kV), w = getv(r, kW);
-                        const Q q0 = getq(r, kQP);
-                        setv(r, kXP, x);
-                        v = madd(v, st.gravity, st.h);
-                        x = madd(x, v, st.h);
-                        if (!k.iso) {
-                            const M3<F> rot = m3_from_quat(getq(r, kQ));
-                            w = mul(rot, gyroscopic(k, tmul(rot, w), st.h));
-                        }
-                        setv(r, kX, x);
-                        setq(r, kQ, q_turn(q0, scale(w, st.h)));
-                        setv(r, kV, v);
-                        setv(r, kW, w);
-                    }
-                    break;
-                case OP_JNT:
-#pragma unroll 1
-                    for (int c = a; c < b; ++c) {
-                        const Ref rp = body_ref(c == 0 ? kTorso : c - 1), rc = body_ref(c);
-                        const BodyK<F>& kp = M.body[c == 0 ? 0 : b_c + c - 1];
-                        const BodyK<F>& kc = M.body[b_c + c];
-                        P bp, bc;
-                        load_pose(rp, kp, bp);
-                        load_pose(rc, kc, bc);
-                        F acc = c == 0 ? tacc0 : (c == 1 ? tacc1 : tacc2);
-                        joint_positions(bp, kp, bc, kc, M.joint[j0 + c], c == 0 ? target0 : (c == 1 ? target1 : target2),
-                                        acc, st.hh);
-                        if (c == 0)
-                            tacc0 = acc;
-                        else if (c == 1)
-                            tacc1 = acc;
-                        else
-                            tacc2 = acc;
-                        store_pose(rp, bp);
-                        store_pose(rc, bc);
-                    }
-                    break;
-                case OP_COL: {
-                    // csrc/arc_phys.c:542-610, spheres a..b-1 of one body
-                    const int slot = a == 0 ? kTorso : (a == 1 ? 1 : 2);
-                    const int bid = a == 0 ? 0 : (a == 1 ? b_f : b_t);
-                    const Ref r = body_ref(slot);
-                    const BodyK<F>& k = M.body[bid];
-                    P pose;
-                    load_pose(r, k, pose);
-                    const V xp = getv(r, kXP);
-                    const Q qp = getq(r, kQP);
-#pragma unroll 1
-                    for (int s = a; s < b; ++s) {
-                        const int bit = s == 0 ? 5 : s - 1;
-                        const Ref ra{s == 0 ? &sm.torso[kBodyF][j] : &sm.anch[leg][6 * (s - 1)][j]};
-                        SphereState<F> ss{getv(ra, 0), getv(ra, 3), (int)((anch >> bit) & 1u)};
-                        const int t = collide(pose, k, xp, qp, M.sphere[s == 0 ? 0 : 5 * leg + s], ss, T, st,
-                                                     [&](V l, V n) { record(bid, l, n); });
-                        touches += (unsigned long long)t << (10 * bit);
-                        anch = (anch & ~(1u << bit)) | ((uint32_t)(ss.anchored != 0) << bit);
-                        setv(ra, 0, ss.anchor);
-                        setv(ra, 3, ss.anchor_n);
-                    }
-                    store_pose(r, pose);
-                    break;
-                }
-                case OP_UPD:
-                    // csrc/arc_phys.c:674-687; the rotation stays that of the
-                    // un-normalised q (field Q)
-#pragma unroll 1
-                    for (int o = a; o < b; ++o) {
-                        const Ref r = body_ref(o == 0 ? kTorso : o - 1);
-                        Q q = getq(r, kQ);
-                        V v, w;
-                        update_velocity(q, getv(r, kX), v, w, getv(r, kXP), getq(r, kQP), st);
-                        setq(r, kQP, q);
-                        setv(r, kV, v);
-                        setv(r, kW, w);
-                    }
-                    break;
-                case OP_DMP: {
-                    // csrc/arc_phys.c:459-481; the child of joint c is the
-                    // parent of joint c+1 (rotation of the position pass)
-                    P bp, bc;
-                    Ref rp = body_ref(a == 0 ? kTorso : a - 1);
-                    bp.q = getq(rp, kQ);
-                    body_sync(bp, M.body[a == 0 ? 0 : b_c + a - 1]);
-                    V wp = getv(rp, kW);
-#pragma unroll 1
-                    for (int c = a; c < b; ++c) {
-                        const Ref rc = body_ref(c);
-                        bc.q = getq(rc, kQ);
-                        body_sync(bc, M.body[b_c + c]);
-                        V wc = getv(rc, kW);
-                        const JointK<F>& J = M.joint[j0 + c];
-                        F acc = c == 0 ? tacc0 : (c == 1 ? tacc1 : tacc2);
-                        joint_velocities<F, true>(bp.rot, bp.iiw, wp, bc.iiw, wc, J, joint_step_k(J, st), st.h, acc);
-                        if (c == 0)
-                            tacc0 = acc;
-                        else if (c == 1)
-                            tacc1 = acc;
-                        else
-                            tacc2 = acc;
-                        setv(rp, kW, wp);
-                        rp = rc;
-                        bp = bc;
-                        wp = wc;
-                    }
-                    setv(rp, kW, wp);
-                    break;
-                }
-                case OP_CVL: {
-                    // csrc/arc_phys.c:612-626, the reference's (sphere-major)
-                    // list order under its cap
-                    int base = 0;
-                    if (capped)
-                        for (int l = 0; l < leg; ++l)
-                            base += sm.nc[sub & 1][l][j];
-                    const int ncl = nc < lane_cap ? nc : lane_cap;
-#pragma unroll 1
-                    for (int c = 0; c < ncl && base + c < kMaxContacts; ++c) {
-                        F rc[7];
-                        if (c < kOnChip) {
-#pragma unroll
-                            for (int f = 0; f < 7; ++f)
-                                rc[f] = sm.con[leg][c * 7 + f][j];
-                        } else {
-                            const F* src =
-                                spill + (((size_t)wi * kWarps + leg) * (size_t)spill_per_lane + (c - kOnChip)) * 8;
-#pragma unroll
-                            for (int f = 0; f < 7; ++f)
-                                rc[f] = src[f];
-                        }
-                        const int bid = (int)rc[6];
-                        if ((bid == 0) != (a == 1))
-                            continue;
-                        const Ref r = body_ref(bid == 0 ? kTorso : (bid == b_f ? 1 : 2));
-                        const BodyK<F>& k = M.body[bid];
-                        P pose;
-                        pose.q = getq(r, kQ);
-                        body_sync(pose, k);
-                        V v = getv(r, kV), w = getv(r, kW);
-                        contact_velocity(pose.rot, pose.iiw, k.inv_mass, v, w,
-                                         ContactRec<F>{V{rc[0], rc[1], rc[2]}, V{rc[3], rc[4], rc[5]}});
-                        setv(r, kV, v);
-                        setv(r, kW, w);
-                    }
-                    break;
-                }
-                default:
-                    break;
-                }
-            }
-            if (arrive)
-                bar_arrive(arrive);
+        // actuation (csrc/arc_sim.c:132-136)
+        F target0 = F(0), target1 = F(0), target2 = F(0);
+        if (valid) {
+            target0 = actuate(M, A, world, j0);
+            target1 = actuate(M, A, world, j0 + 1);
+            target2 = actuate(M, A, world, j0 + 2);
+            jr[j0 * kJointRec] = target0;
+            jr[(j0 + 1) * kJointRec] = target1;
+            jr[(j0 + 2) * kJointRec] = target2;
         }
-    }
-    __syncthreads();
-
-    // epilogue (csrc/arc_phys.c:739-746), from the normalised quaternions
-    int bad = 0;
-    if (active) {
-        const Ref r0 = body_ref(0), r1 = body_ref(1), r2 = body_ref(2);
-        const Q tq = getq(torso, kQP), q0 = getq(r0, kQP), q1 = getq(r1, kQP), q2 = getq(r2, kQP);
-        const V tw = getv(torso, kW), w0 = getv(r0, kW), w1 = getv(r1, kW), w2 = getv(r2, kW);
-        const JointK<F>& J0 = M.joint[j0];
-        const JointK<F>& J1 = M.joint[j0 + 1];
-        const JointK<F>& J2 = M.joint[j0 + 2];
-        jr[(j0 + 0) * kJointRec + 1] = joint_angle(tq, q0, J0);
-        jr[(j0 + 0) * kJointRec + 2] = joint_rate(tq, tw, w0, J0);
-        jr[(j0 + 1) * kJointRec + 1] = joint_angle(q0, q1, J1);
-        jr[(j0 + 1) * kJointRec + 2] = joint_rate(q0, w0, w1, J1);
-        jr[(j0 + 2) * kJointRec + 1] = joint_angle(q1, q2, J2);
-        jr[(j0 + 2) * kJointRec + 2] = joint_rate(q1, w1, w2, J2);
-        jr[(j0 + 0) * kJointRec + 3] = tacc0 / F(M.substeps);
-        jr[(j0 + 1) * kJointRec + 3] = tacc1 / F(M.substeps);
-        jr[(j0 + 2) * kJointRec + 3] = tacc2 / F(M.substeps);
-        auto put = [&](Ref r, F* d) {
-            const V x = getv(r, kX), v = getv(r, kV), w = getv(r, kW);
-            const Q q = getq(r, kQP);
-            bad |= body_unstable(x, v, w);
-            d[0] = x.x; d[1] = x.y; d[2] = x.z;
-            d[3] = q.w; d[4] = q.x; d[5] = q.y; d[6] = q.z;
-            d[7] = v.x; d[8] = v.y; d[9] = v.z;
-            d[10] = w.x; d[11] = w.y; d[12] = w.z;
+        F tacc0 = F(0), tacc1 = F(0), tacc2 = F(0);
+        const bool active = valid && W.unstable[wi] == 0;
+        auto stage_body = [&](Ref r, const F* src) {
+            setv(r, kX, V{src[0], src[1], src[2]});
+            setq(r, kQ, Q{src[3], src[4], src[5], src[6]});
+            setq(r, kQP, Q{src[3], src[4], src[5], src[6]});
+            setv(r, kV, V{src[7], src[8], src[9]});
+            setv(r, kW, V{src[10], src[11], src[12]});
         };
 #pragma unroll 1
         for (int i = 0; i < 3; ++i)
-            put(body_ref(i), rec + (b_c + i) * kBodyRec);
-        uint32_t* sphw = W.sph + (size_t)world * 21;
+            stage_body(body_ref(i), rec + (b_c + i) * kBodyRec);
+        uint32_t anch = 0;
+        const uint32_t* sphr = W.sph + (size_t)wi * 21;
 #pragma unroll
         for (int s = 0; s < 5; ++s) {
-            F* a = sr + (5 * leg + 1 + s) * kSphereRec;
+            const F* a = sr + (5 * leg + 1 + s) * kSphereRec;
 #pragma unroll
             for (int c = 0; c < 6; ++c)
-                a[c] = sm.anch[leg][6 * s + c][j];
-            sphw[5 * leg + 1 + s] = (uint32_t)((touches >> (10 * s)) & 1023u) | (((anch >> s) & 1u) << 16);
+                sm.anch[leg][6 * s + c][j] = a[c];
+            anch |= ((sphr[5 * leg + 1 + s] >> 16) & 1u) << s;
         }
-        if (leg == 0)
-            put(torso, rec);
-        if (leg == torso_warp) {
+        // the warp that collides the torso's sphere keeps its flags
+        const bool capped = kWarps * lane_cap > kMaxContacts;
+        const int torso_warp = capped ? 0 : kWarps - 1;
+        if (leg == 0) {
+            stage_body(torso, rec);
 #pragma unroll
             for (int c = 0; c < 6; ++c)
-                sr[c] = torso[kBodyF + c];
-            sphw[0] = (uint32_t)((touches >> 50) & 1023u) | (((anch >> 5) & 1u) << 16);
+                torso[kBodyF + c] = sr[c];
         }
+        if (leg == torso_warp)
+            anch |= ((sphr[0] >> 16) & 1u) << 5;
+        const TerrainView<F> T = terrain_of(W, wi);
+        const StepK<F>& st = M.step;
+        unsigned long long touches = 0;  // 10 bits per sphere: leg spheres 0..4, torso sphere at 50
+        const uint32_t* ops = &kOps[capped ? 1 : 0][leg][0];
+        __syncthreads();
+
+        for (int sub = 0; sub < M.substeps; ++sub) {
+            int nc = 0;
+            auto record = [&](int body, V local, V n) {
+                if (nc < kOnChip) {
+                    const Ref d{&sm.con[leg][nc * 7][j]};
+                    setv(d, 0, local);
+                    setv(d, 3, n);
+                    d[6] = (F)body;
+                } else if (nc < lane_cap) {
+                    F* d = spill + (((size_t)wi * kWarps + leg) * (size_t)spill_per_lane + (nc - kOnChip)) * 8;
+                    d[0] = local.x; d[1] = local.y; d[2] = local.z;
+                    d[3] = n.x; d[4] = n.y; d[5] = n.z;
+                    d[6] = (F)body;
+                }
+                ++nc;
+            };
+#pragma unroll 1
+            for (int i = 0;; ++i) {
+                const uint32_t op = ops[i];
+                const uint32_t kind = op & 15u;
+                if (kind == OP_END)
+                    break;
+                if (((op & kFirstOnly) && sub != 0) || ((op & kNotLast) && sub == M.substeps - 1))
+                    continue;
+                const int a = (op >> 4) & 15, b = (op >> 8) & 15, wait = (op >> 12) & 15, arrive = (op >> 16) & 15;
+                if (wait)
+                    bar_sync(wait);
+                if (kind == OP_CNT) {
+                    // double-buffered: a warp may record substep s+1 while
+                    // another still reads the counts of substep s
+                    sm.nc[sub & 1][leg][j] = nc;
+                    __syncthreads();
+                } else if (active) {
+                    switch (kind) {
+                    case OP_INT:
+                        // csrc/arc_phys.c:658-672
+#pragma unroll 1
+                        for (int o = a; o < b; ++o) {
+                            const Ref r = body_ref(o == 0 ? kTorso : o - 1);
+                            const BodyK<F>& k = M.body[o == 0 ? 0 : b_c + o - 1];
+                            V x = getv(r, kX), v = getv(r, kV), w = getv(r, kW);
+                            const Q q0 = getq(r, kQP);
+                            setv(r, kXP, x);
+                            v = madd(v, st.gravity, st.h);
+                            x = madd(x, v, st.h);
+                            if (!k.iso) {
+                                const M3<F> rot = m3_from_quat(getq(r, kQ));
+                                w = mul(rot, gyroscopic(k, tmul(rot, w), st.h));
+                            }
+                            setv(r, kX, x);
+                            setq(r, kQ, q_turn(q0, scale(w, st.h)));
+                            setv(r, kV, v);
+                            setv(r, kW, w);
+                        }
+                        break;
+                    case OP_JNT:
+#pragma unroll 1
+                        for (int c = a; c < b; ++c) {
+                            const Ref rp = body_ref(c == 0 ? kTorso : c - 1), rc = body_ref(c);
+                            const BodyK<F>& kp = M.body[c == 0 ? 0 : b_c + c - 1];
+                            const BodyK<F>& kc = M.body[b_c + c];
+                            P bp, bc;
+                            load_pose(rp, kp, bp);
+                            load_pose(rc, kc, bc);
+                            F acc = c == 0 ? tacc0 : (c == 1 ? tacc1 : tacc2);
+                            const F tgt = c == 0 ? target0 : (c == 1 ? target1 : target2);
+                            joint_positions(bp, kp, bc, kc, M.joint[j0 + c], tgt, acc, st.hh);
+                            if (c == 0)
+                                tacc0 = acc;
+                            else if (c == 1)
+                                tacc1 = acc;
+                            else
+                                tacc2 = acc;
+                            store_pose(rp, bp);
+                            store_pose(rc, bc);
+                        }
+                        break;
+                    case OP_COL: {
+                        // csrc/arc_phys.c:542-610, spheres a..b-1 of one body
+                        const int slot = a == 0 ? kTorso : (a == 1 ? 1 : 2);
+                        const int bid = a == 0 ? 0 : (a == 1 ? b_f : b_t);
+                        const Ref r = body_ref(slot);
+                        const BodyK<F>& k = M.body[bid];
+                        P pose;
+                        load_pose(r, k, pose);
+                        const V xp = getv(r, kXP);
+                        const Q qp = getq(r, kQP);
+#pragma unroll 1
+                        for (int s = a; s < b; ++s) {
+                            const int bit = s == 0 ? 5 : s - 1;
+                            const Ref ra{s == 0 ? &sm.torso[kBodyF][j] : &sm.anch[leg][6 * (s - 1)][j]};
+                            SphereState<F> ss{getv(ra, 0), getv(ra, 3), (int)((anch >> bit) & 1u)};
+                            const int t = collide(pose, k, xp, qp, M.sphere[s == 0 ? 0 : 5 * leg + s], ss, T, st,
+                                                         [&](V l, V n) { record(bid, l, n); });
+                            touches += (unsigned long long)t << (10 * bit);
+                            anch = (anch & ~(1u << bit)) | ((uint32_t)(ss.anchored != 0) << bit);
+                            setv(ra, 0, ss.anchor);
+                            setv(ra, 3, ss.anchor_n);
+                        }
+                        store_pose(r, pose);
+                        break;
+                    }
+                    case OP_UPD:
+                        // csrc/arc_phys.c:674-687; the rotation stays that of the
+                        // un-normalised q (field Q)
+#pragma unroll 1
+                        for (int o = a; o < b; ++o) {
+                            const Ref r = body_ref(o == 0 ? kTorso : o - 1);
+                            Q q = getq(r, kQ);
+                            V v, w;
+                            update_velocity(q, getv(r, kX), v, w, getv(r, kXP), getq(r, kQP), st);
+                            setq(r, kQP, q);
+                            setv(r, kV, v);
+                            setv(r, kW, w);
+                        }
+                        break;
+                    case OP_DMP: {
+                        // csrc/arc_phys.c:459-481; the child of joint c is the
+                        // parent of joint c+1 (rotation of the position pass)
+                        P bp, bc;
+                        Ref rp = body_ref(a == 0 ? kTorso : a - 1);
+                        bp.q = getq(rp, kQ);
+                        body_sync(bp, M.body[a == 0 ? 0 : b_c + a - 1]);
+                        V wp = getv(rp, kW);
+#pragma unroll 1
+                        for (int c = a; c < b; ++c) {
+                            const Ref rc = body_ref(c);
+                            bc.q = getq(rc, kQ);
+                            body_sync(bc, M.body[b_c + c]);
+                            V wc = getv(rc, kW);
+                            const JointK<F>& J = M.joint[j0 + c];
+                            F acc = c == 0 ? tacc0 : (c == 1 ? tacc1 : tacc2);
+                            joint_velocities<F, true>(bp.rot, bp.iiw, wp, bc.iiw, wc, J, joint_step_k(J, st), st.h,
+                                                      acc);
+                            if (c == 0)
+                                tacc0 = acc;
+                            else if (c == 1)
+                                tacc1 = acc;
+                            else
+                                tacc2 = acc;
+                            setv(rp, kW, wp);
+                            rp = rc;
+                            bp = bc;
+                            wp = wc;
+                        }
+                        setv(rp, kW, wp);
+                        break;
+                    }
+                    case OP_CVL: {
+                        // csrc/arc_phys.c:612-626, the reference's (sphere-major)
+                        // list order under its cap
+                        int base = 0;
+                        if (capped)
+                            for (int l = 0; l < leg; ++l)
+                                base += sm.nc[sub & 1][l][j];
+                        const int ncl = nc < lane_cap ? nc : lane_cap;
+#pragma unroll 1
+                        for (int c = 0; c < ncl && base + c < kMaxContacts; ++c) {
+                            F rc[7];
+                            if (c < kOnChip) {
+#pragma unroll
+                                for (int f = 0; f < 7; ++f)
+                                    rc[f] = sm.con[leg][c * 7 + f][j];
+                            } else {
+                                const F* src =
+                                    spill + (((size_t)wi * kWarps + leg) * (size_t)spill_per_lane + (c - kOnChip)) * 8;
+#pragma unroll
+                                for (int f = 0; f < 7; ++f)
+                                    rc[f] = src[f];
+                            }
+                            const int bid = (int)rc[6];
+                            if ((bid == 0) != (a == 1))
+                                continue;
+                            const Ref r = body_ref(bid == 0 ? kTorso : (bid == b_f ? 1 : 2));
+                            const BodyK<F>& k = M.body[bid];
+                            P pose;
+                            pose.q = getq(r, kQ);
+                            body_sync(pose, k);
+                            V v = getv(r, kV), w = getv(r, kW);
+                            contact_velocity(pose.rot, pose.iiw, k.inv_mass, v, w,
+                                             ContactRec<F>{V{rc[0], rc[1], rc[2]}, V{rc[3], rc[4], rc[5]}});
+                            setv(r, kV, v);
+                            setv(r, kW, w);
+                        }
+                        break;
+                    }
+                    default:
+                        break;
+                    }
+                }
+                if (arrive)
+                    bar_arrive(arrive);
+            }
+        }
+        __syncthreads();
+
+        // epilogue (csrc/arc_phys.c:739-746), from the normalised quaternions
+        int bad = 0;
+        if (active) {
+            const Ref r0 = body_ref(0), r1 = body_ref(1), r2 = body_ref(2);
+            const Q tq = getq(torso, kQP), q0 = getq(r0, kQP), q1 = getq(r1, kQP), q2 = getq(r2, kQP);
+            const V tw = getv(torso, kW), w0 = getv(r0, kW), w1 = getv(r1, kW), w2 = getv(r2, kW);
+            const JointK<F>& J0 = M.joint[j0];
+            const JointK<F>& J1 = M.joint[j0 + 1];
+            const JointK<F>& J2 = M.joint[j0 + 2];
+            jr[(j0 + 0) * kJointRec + 1] = joint_angle(tq, q0, J0);
+            jr[(j0 + 0) * kJointRec + 2] = joint_rate(tq, tw, w0, J0);
+            jr[(j0 + 1) * kJointRec + 1] = joint_angle(q0, q1, J1);
+            jr[(j0 + 1) * kJointRec + 2] = joint_rate(q0, w0, w1, J1);
+            jr[(j0 + 2) * kJointRec + 1] = joint_angle(q1, q2, J2);
+            jr[(j0 + 2) * kJointRec + 2] = joint_rate(q1, w1, w2, J2);
+            jr[(j0 + 0) * kJointRec + 3] = tacc0 / F(M.substeps);
+            jr[(j0 + 1) * kJointRec + 3] = tacc1 / F(M.substeps);
+            jr[(j0 + 2) * kJointRec + 3] = tacc2 / F(M.substeps);
+            auto put = [&](Ref r, F* d) {
+                const V x = getv(r, kX), v = getv(r, kV), w = getv(r, kW);
+                const Q q = getq(r, kQP);
+                bad |= body_unstable(x, v, w);
+                d[0] = x.x; d[1] = x.y; d[2] = x.z;
+                d[3] = q.w; d[4] = q.x; d[5] = q.y; d[6] = q.z;
+                d[7] = v.x; d[8] = v.y; d[9] = v.z;
+                d[10] = w.x; d[11] = w.y; d[12] = w.z;
+            };
+#pragma unroll 1
+            for (int i = 0; i < 3; ++i)
+                put(body_ref(i), rec + (b_c + i) * kBodyRec);
+            uint32_t* sphw = W.sph + (size_t)world * 21;
+#pragma unroll
+            for (int s = 0; s < 5; ++s) {
+                F* a = sr + (5 * leg + 1 + s) * kSphereRec;
+#pragma unroll
+                for (int c = 0; c < 6; ++c)
+                    a[c] = sm.anch[leg][6 * s + c][j];
+                sphw[5 * leg + 1 + s] = (uint32_t)((touches >> (10 * s)) & 1023u) | (((anch >> s) & 1u) << 16);
+            }
+            if (leg == 0)
+                put(torso, rec);
+            if (leg == torso_warp) {
+#pragma unroll
+                for (int c = 0; c < 6; ++c)
+                    sr[c] = torso[kBodyF + c];
+                sphw[0] = (uint32_t)((touches >> 50) & 1023u) | (((anch >> 5) & 1u) << 16);
+            }
+        }
+        sm.bad[leg][j] = bad;
+        __syncthreads();
+        if (active && leg == 0) {
+            W.time[world] += M.step_dt;
+            if (sm.bad[0][j] | sm.bad[1][j] | sm.bad[2][j] | sm.bad[3][j])
+                W.unstable[world] = 1;
+        }
+        if (!queue)
+            break;
+        if (tid == 0)
+            s_next = (int)gridDim.x + atomicAdd(queue, 1);
+        __syncthreads();
+        group = s_next;
     }
-    sm.bad[leg][j] = bad;
-    __syncthreads();
-    if (active && leg == 0) {
-        W.time[world] += M.step_dt;
-        if (sm.bad[0][j] | sm.bad[1][j] | sm.bad[2][j] | sm.bad[3][j])
-            W.unstable[world] = 1;
+    if (queue) {
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            if (atomicAdd(queue + 1, 1) == (int)gridDim.x - 1) {
+                queue[0] = 0;
+                queue[1] = 0;
+                __threadfence();
+            }
+        }
     }
 }
 
@@ -686,9 +714,10 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
 size_t warps_smem_bytes() { return sizeof(wl::Smem); }
 
 cudaError_t launch_step_warps(const DevModel<float>& M, const Worlds<float>& W, const Actuation& A, float* spill,
-                              int spill_per_lane, int lane_cap, cudaStream_t stream)
+                              int spill_per_lane, int lane_cap, const int* ids, int n_items, int* queue,
+                              cudaStream_t stream)
 {
-    if (W.n <= 0)
+    if (W.n <= 0 || n_items <= 0)
         return cudaSuccess;
     if (!M.leaper)
         return cudaErrorInvalidValue;
@@ -701,8 +730,26 @@ cudaError_t launch_step_warps(const DevModel<float>& M, const Worlds<float>& W, 
             return e;
         configured = true;
     }
-    const int grid = (W.n + wl::kWorlds - 1) / wl::kWorlds;
-    wl::k_step_warps<<<grid, wl::kThreads, smem, stream>>>(M, W, A, spill, spill_per_lane, lane_cap);
+    const int groups = (n_items + wl::kWorlds - 1) / wl::kWorlds;
+    int grid = groups;
+    if (queue) {
+        // one wave of resident CTAs
+        static int resident = 0;
+        if (!resident) {
+            int dev = 0, sms = 0, per_sm = 0;
+            cudaError_t e = cudaGetDevice(&dev);
+            if (e == cudaSuccess)
+                e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (e == cudaSuccess)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wl::k_step_warps, wl::kThreads, smem);
+            if (e != cudaSuccess)
+                return e;
+            resident = sms * (per_sm > 0 ? per_sm : 1);
+        }
+        grid = groups < resident ? groups : resident;
+    }
+    wl::k_step_warps<<<grid, wl::kThreads, smem, stream>>>(M, W, A, spill, spill_per_lane, lane_cap, ids, n_items,
+                                                           queue);
     return cudaGetLastError();
 }
 

@@ -95,6 +95,9 @@ def sim_lib() -> ctypes.CDLL:
     d("arc_sim_step_actions", _int, _vp, _vp, _vp)
     d("arc_sim_observe_device", _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp)
     d("arc_sim_synchronize", _int, _vp)
+    d("arc_sim_create_sized", _vp, _int, _i32, _dbl, _int, _dbl, _uint)
+    d("arc_sim_step_ids", _int, _vp, _vp, _int, _vp, _vp, _vp)
+    d("arc_sim_set_work_queue", _int, _vp, _int)
     return lib
 
 
@@ -138,8 +141,15 @@ class Sim:
 
     def __init__(self, num_worlds: int, dt: float = 1.0 / 30.0, substeps: int = 20,
                  grid: int = 64, cell: float = 0.4, threads: int = 1, *, fp64: bool = False,
-                 plain: bool = False, model: Model | None = None):
+                 plain: bool = False, model: Model | None = None, grids=None):
+        """grids: optional per-world terrain sizes (1..64); grid is then
+        their maximum and world i holds grids[i] x grids[i] columns."""
         self._lib = sim_lib()
+        if grids is not None:
+            grids = np.ascontiguousarray(grids, dtype=np.int32)
+            assert len(grids) == num_worlds
+            grid = int(grids.max()) if num_worlds else grid
+        self.grids = grids
         self.num_worlds = num_worlds
         self.grid = min(grid, 64)
         self.cell = cell
@@ -149,6 +159,8 @@ class Sim:
         flags = (FP64 if fp64 else 0) | (PLAIN if plain else 0)
         if model is not None:
             self._ptr = self._lib.arc_sim_create_model(model.ptr, num_worlds, dt, substeps, grid, cell, flags)
+        elif grids is not None:
+            self._ptr = self._lib.arc_sim_create_sized(num_worlds, grids, dt, substeps, cell, flags)
         else:
             self._ptr = self._lib.arc_sim_create_ex(num_worlds, dt, substeps, grid, cell, flags)
         if not self._ptr:
@@ -300,3 +312,12 @@ class Sim:
 
     def synchronize(self) -> None:
         self._check(self._lib.arc_sim_synchronize(self._ptr))
+
+    def step_ids(self, d_ids: int, n_ids: int, d_targets: int = 0, d_actions: int = 0, stream: int = 0) -> None:
+        """Steps the n_ids worlds listed at device address d_ids, with device
+        targets (N x 12 FP64) or actions (N x 12 FP32); asynchronous."""
+        self._check(self._lib.arc_sim_step_ids(self._ptr, d_ids or None, n_ids, d_targets or None,
+                                               d_actions or None, stream or None))
+
+    def set_work_queue(self, on: bool) -> None:
+        self._check(self._lib.arc_sim_set_work_queue(self._ptr, int(bool(on))))

@@ -100,9 +100,17 @@ const arc_world *arc_sim_world(const arc_sim *s, int i);
 /* kernels */
 #define ARC_KERNEL_PLAIN 0      /* one thread per world */
 #define ARC_KERNEL_LEGS 1       /* four lanes per world (one per leg), shared-memory staging */
-#define ARC_KERNEL_WARPS 2      /* FP32: four warps per 32 worlds (one warp per leg), leg state in registers */
+#define ARC_KERNEL_WARPS 2      /* FP32: four warps per 32 worlds (one warp per leg), state in shared memory */
 
 arc_sim *arc_sim_create_ex(int n_worlds, double dt, int substeps, int grid, double cell, unsigned flags);
+
+/* Worlds whose terrain grids differ: world i holds grids[i] x grids[i]
+ * columns (1..64), all packed in one pool, and arc_sim_reset generates a
+ * grids[i]-sized terrain for it (the reference's arc_terrain takes nx, ny
+ * per world, csrc/arc_terrain.h:13-20; its arc_sim has one grid for all,
+ * csrc/arc_sim.c:36). arc_sim_set_terrain may then write at most
+ * grids[i]^2 columns. NULL on a size outside 1..64 or no device. */
+arc_sim *arc_sim_create_sized(int n_worlds, const int *grids, double dt, int substeps, double cell, unsigned flags);
 
 /* Last error of any call on s (0 if none) and its message; clears nothing. */
 int arc_sim_last_error(const arc_sim *s);
@@ -166,6 +174,16 @@ int arc_sim_step_actions(arc_sim *s, const float *d_actions, void *stream);
 int arc_sim_observe_device(const arc_sim *s, double *root, double *rot, double *joints, double *contacts, int *flags,
                            void *stream);
 int arc_sim_synchronize(const arc_sim *s);
+/* Steps only the n_ids worlds d_ids[0..n_ids) (device ints, distinct; ids
+ * outside 0..N-1 are skipped), with exactly one of d_targets (N x 12 FP64)
+ * or d_actions (N x 12 FP32, as arc_sim_step_actions), read at the listed
+ * rows only. FP32 quadruped batches use the warp-per-leg kernel, others the
+ * plain one. */
+int arc_sim_step_ids(arc_sim *s, const int *d_ids, int n_ids, const double *d_targets, const float *d_actions,
+                     void *stream);
+/* on != 0: the warp-per-leg kernel runs one wave of resident CTAs that take
+ * groups of 32 worlds from a device work queue, instead of one CTA per group */
+int arc_sim_set_work_queue(arc_sim *s, int on);
 
 /* Measured FP32 FMA throughput of the current device (FLOP/s, an FMA
  * counted as 2): the roofline denominator of the step kernels. */

@@ -1,4 +1,4 @@
-"""Parity of the CUDA step (both kernels, FP32 and FP64) with the CPU checkers.
+"""Parity of the CUDA step kernels (FP32 and FP64) with the CPU checkers.
 
 Checkers: the reference's own csrc/ built from its sources (oracle/_ref,
 FP64 as shipped) and the C restatement (oracle/, FP64 and FP32).
@@ -16,11 +16,11 @@ Tolerances (the parity contract):
   itself, not the kernels. Threshold events (contact on/off, friction
   anchor reset, limit activation) flip on differences below FP32
   resolution, so the touch-count mismatch rate is bounded (<= 1%) too.
-- The two kernels (plain, leg-parallel) run the same solver in the same
-  per-body order: in FP64 they agree to 1e-10; in FP32 to FP32 rounding
-  (FMA placement differs between the two compiled kernels). The
-  leg-parallel kernel at different worlds-per-CTA runs identical per-world
-  code and must agree bit for bit.
+- The kernels (plain, leg-parallel, warp-per-leg) run the same solver in
+  the same per-body order: in FP64 they agree to 1e-10; in FP32 to FP32
+  rounding (FMA placement differs between the compiled kernels). One
+  kernel at different worlds-per-CTA, on a subset of the worlds or from a
+  work queue runs identical per-world code and must agree bit for bit.
 """
 
 import numpy as np
@@ -323,3 +323,59 @@ def test_unstable_worlds_are_flagged_and_skipped():
     assert np.array_equal(before[1:4, : NB * 13], after[1:4, : NB * 13], equal_nan=True)
     tgt = after[:, NB * 13 + NS * 8:: 4][:, :12]
     assert np.allclose(tgt[1], g.hi.astype(np.float32), atol=1e-6)
+
+
+def _device_buffers(ids, targets):
+    import torch
+
+    d_ids = torch.as_tensor(np.asarray(ids, dtype=np.int32), device="cuda")
+    d_t = torch.as_tensor(np.ascontiguousarray(targets, dtype=np.float64), device="cuda")
+    torch.cuda.synchronize()
+    return d_ids, d_t
+
+
+@pytest.mark.parametrize("queue", [False, True])
+def test_subset_step_equals_batch_step(queue):
+    """Stepping a list of worlds gives, for those worlds, exactly what the
+    whole-batch step gives (worlds never interact and run the same code),
+    and leaves the other worlds untouched; with or without the work queue."""
+    n = 200
+    seeds, diffs = seeds_diffs(n, 21)
+    a, b = Sim(n), Sim(n)
+    for s in (a, b):
+        s.set_kernel(KERNEL_WARPS)
+        s.reset(np.arange(n), seeds, diffs)
+    a.set_work_queue(queue)
+    rng = np.random.default_rng(3)
+    ids = np.sort(rng.choice(n, 77, replace=False)).astype(np.int32)[::-1].copy()  # any order
+    for _ in range(3):
+        t = a.default_angles + 0.6 * rng.uniform(-1, 1, (n, 12))
+        before = a.get_state()
+        d_ids, d_t = _device_buffers(ids, t)
+        a.step_ids(d_ids.data_ptr(), len(ids), d_targets=d_t.data_ptr())
+        a.synchronize()
+        b.set_state(before)
+        b.step(t)
+        sa, sb = a.get_state(), b.get_state()
+        assert np.array_equal(sa[ids], sb[ids])
+        rest = np.setdiff1d(np.arange(n), ids)
+        assert np.array_equal(sa[rest], before[rest])
+
+
+def test_work_queue_matches_one_cta_per_group():
+    """The persistent form (resident CTAs taking groups from a queue, reset
+    by the last CTA) steps every world exactly as one CTA per group does,
+    launch after launch."""
+    n = 70 * 32 + 5
+    seeds, diffs = seeds_diffs(n, 22)
+    a, b = Sim(n), Sim(n)
+    for s in (a, b):
+        s.set_kernel(KERNEL_WARPS)
+        s.reset(np.arange(n), seeds, diffs)
+    a.set_work_queue(True)
+    rng = np.random.default_rng(4)
+    for _ in range(4):
+        t = a.default_angles + 0.6 * rng.uniform(-1, 1, (n, 12))
+        a.step(t)
+        b.step(t)
+    assert np.array_equal(a.get_state(), b.get_state())
