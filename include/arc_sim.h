@@ -189,6 +189,32 @@ int arc_sim_set_work_queue(arc_sim *s, int on);
  * counted as 2): the roofline denominator of the step kernels. */
 int arc_probe_fp32_peak(double *flops_per_s, double *seconds);
 
+/* ---- serving engine. No counterpart in the reference. A fixed pool of
+ * `capacity` world slots (the state budget) and one engine thread doing
+ * continuous batching: queued requests are admitted first come, first
+ * served, while free slots hold them, and their worlds reset; each tick
+ * steps every admitted world of every request in one launch; a request
+ * whose steps are done has its final states read back and its slots freed.
+ * Thread-safe: any number of client threads may submit and wait. */
+typedef struct arc_server arc_server;
+arc_server *arc_server_create(int capacity, double dt, int substeps, int grid, double cell);
+/* Stops the engine; requests still queued fail. */
+void arc_server_destroy(arc_server *sv);
+/* A request: n_worlds fresh episodes (seeds, difficulty as arc_sim_reset)
+ * stepped n_steps control steps with actions (n_steps x n_worlds x 12 FP32,
+ * as arc_sim_step_actions; copied) or, with actions NULL, an
+ * Ornstein-Uhlenbeck process per world (theta 0.15, sigma 0.3, clipped to
+ * [-1, 1]) seeded by ou_seed. Returns the request id (>= 0) or < 0. */
+long long arc_server_submit(arc_server *sv, int n_worlds, int n_steps, const unsigned *seeds,
+                            const double *difficulty, const float *actions, unsigned long long ou_seed);
+/* Waits up to timeout_s for request id: 1 when done (out: n_worlds x
+ * arc_sim_state_size final states; times: seconds queued, running, total;
+ * either may be NULL), 0 on timeout, < 0 on error. An id is returned once. */
+int arc_server_wait(arc_server *sv, long long id, double timeout_s, double *out, double *times);
+/* stats: ticks, world-steps, engine busy seconds, most worlds in one tick,
+ * completed requests, queued requests. Returns the engine's error (0 ok). */
+int arc_server_stats(arc_server *sv, double *stats);
+
 /* ---- one control step without any device allocation. No counterpart in
  * the reference: for callers that cannot call cudaMalloc (a host runtime
  * that owns all device memory through its own arena; a control loop that
