@@ -42,6 +42,11 @@ METRIC = "env-steps/s at 65536 worlds vs plain GPU kernel and OpenMP; p50/p99 st
 WORLDS = 65536
 FLOP_PER_ENV_STEP = 415.6e3   # scalar FP ops of one control step, counted on the reference
 HBM_BYTES_PER_ENV_STEP = 3.9e3  # algorithmic HBM traffic of one env-step (state, actions, obs)
+# DRAM bytes (read + write) one world costs a launch of the warp-per-leg step
+# kernel: ncu's dram__bytes_read.sum + dram__bytes_write.sum over a
+# 16,384-world launch (42.24 MB + 0.15 MB), divided by the worlds; each world
+# reads its own record and terrain cells, so the traffic scales with them.
+WARPS_DRAM_BYTES_PER_WORLD = (42.237e6 + 0.152e6) / 16384
 
 
 def parse():
@@ -315,7 +320,8 @@ def run_ours(args) -> dict | None:
         "roofline": {"bound": "fp32", "achieved": round(achieved / 1e12, 3),
                      "peak": round(peak.value / 1e12, 3), "unit": "TFLOP/s",
                      "frac": round(achieved / peak.value, 4) if peak.value else None,
-                     "traffic": None,
+                     "traffic": round(n * WARPS_DRAM_BYTES_PER_WORLD) if best_wpc == "warps" else None,
+                     "traffic_unit": "bytes per launch (ncu, scaled from 16,384 worlds)",
                      "kernel": ("warp-per-leg" if best_wpc == "warps" else "leg-parallel") + " step",
                      "kernel_ms": round(step_kernel_ms, 4),
                      "flop_per_env_step": FLOP_PER_ENV_STEP,

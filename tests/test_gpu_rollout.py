@@ -1,0 +1,61 @@
+"""The batched-uneven configuration: 4,096 worlds, difficulty U[0, 1] per
+world, Ornstein-Uhlenbeck actions (theta 0.15, sigma 0.3, clipped to
+[-1, 1], seed 1, one control step per OU step), every world reset when its
+episode ends by a fall (the task layer's terminations, arc/task.py:185-212)
+or at max_steps (truncation), each control step one CUDA-graph launch.
+
+Per-step parity of the task math is teacher-forced in test_gpu_task.py; this
+test runs the loop at scale and checks its bookkeeping on every step: the
+observation stays finite, the ended-world list is exactly the worlds that
+terminated or truncated, every termination carries a cause, and an ended
+world starts a fresh episode (step counter 0, episode count + 1).
+"""
+
+import numpy as np
+import pytest
+
+from arc_demo_b200.task import TaskConfig
+
+pytestmark = pytest.mark.gpu
+
+
+def ou_actions(n, steps, seed=1, theta=0.15, sigma=0.3):
+    rng = np.random.default_rng(seed)
+    x = np.zeros((n, 12))
+    for _ in range(steps):
+        x += theta * (0.0 - x) + sigma * rng.standard_normal((n, 12))
+        yield np.clip(x, -1.0, 1.0).astype(np.float32)
+
+
+@pytest.mark.parametrize("max_steps", [1000, 40])
+def test_ou_rollout_4096_worlds_with_resets(max_steps):
+    import torch
+    from arc_demo_b200.torch_env import DeviceVecEnv
+
+    n, steps = 4096, 120 if max_steps == 1000 else 90
+    env = DeviceVecEnv(n, TaskConfig(curriculum=False, max_steps=max_steps), seed=1)
+    env.set_levels(np.random.default_rng(1).uniform(0.0, 1.0, n))
+    env.reset()
+    ended_total, terminated_total = 0, 0
+    st = env.gpu.get_state()
+    for a in ou_actions(n, steps):
+        obs, rew, term, trunc = env.step(torch.from_numpy(a).cuda(), graph=True)
+        torch.cuda.synchronize()
+        ended = (term.bool() | trunc.bool()).cpu().numpy()
+        cause = env.cause.cpu().numpy()
+        count = int(env.done_count.item())
+        assert torch.isfinite(obs).all() and torch.isfinite(rew).all()
+        assert count == int(ended.sum())
+        assert np.array_equal(np.sort(env.done_list[:count].cpu().numpy()), np.flatnonzero(ended))
+        assert np.all(cause[term.bool().cpu().numpy()] > 0)
+        st1 = env.gpu.get_state()
+        assert np.all(st1[ended, 18] == 0)                      # fresh episodes
+        assert np.array_equal(st1[ended, 23], st[ended, 23] + 1)
+        assert np.array_equal(st1[~ended, 18], st[~ended, 18] + 1)
+        st = st1
+        ended_total += count
+        terminated_total += int(term.sum().item())
+    assert terminated_total > 0  # falls happen under OU actions on rough terrain
+    if max_steps < steps:
+        # every episode ends by max_steps at the latest
+        assert ended_total >= n * (steps // max_steps)
