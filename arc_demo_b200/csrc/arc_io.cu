@@ -11,28 +11,32 @@ namespace arc {
 template <class R>
 __global__ void k_observe(const __grid_constant__ DevModel<R> M, Worlds<R> W, double* __restrict__ root,
                           double* __restrict__ rot, double* __restrict__ joints, double* __restrict__ contacts,
-                          int* __restrict__ flags)
+                          int* __restrict__ flags, const int* __restrict__ ids, int n_items)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= W.n)
+    // output row k holds world ids[k] (world k without ids)
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_items)
+        return;
+    const int i = ids ? ids[k] : k;
+    if (i < 0 || i >= W.n)
         return;
     const R* rec = W.rec + (size_t)i * W.stride;
     if (root) {
-        double* r = root + (size_t)i * 13;
+        double* r = root + (size_t)k * 13;
         for (int k = 0; k < 13; ++k)
             r[k] = (double)rec[k];
     }
     if (rot) {
         Q4<double> q{(double)rec[3], (double)rec[4], (double)rec[5], (double)rec[6]};
         M3<double> m = m3_from_quat(q);
-        double* o = rot + (size_t)i * 9;
+        double* o = rot + (size_t)k * 9;
         for (int a = 0; a < 3; ++a)
             for (int c = 0; c < 3; ++c)
                 o[a * 3 + c] = m.m[a][c];
     }
     if (joints) {
         const R* jr = rec + W.off_joint;
-        double* o = joints + (size_t)i * 3 * M.nj;
+        double* o = joints + (size_t)k * 3 * M.nj;
         for (int j = 0; j < M.nj; ++j) {
             o[j] = (double)jr[j * kJointRec + 1];
             o[M.nj + j] = (double)jr[j * kJointRec + 2];
@@ -40,7 +44,7 @@ __global__ void k_observe(const __grid_constant__ DevModel<R> M, Worlds<R> W, do
         }
     }
     if (contacts) {
-        double* o = contacts + (size_t)i * M.n_channels;
+        double* o = contacts + (size_t)k * M.n_channels;
         const double inv = 1.0 / M.substeps;
         const uint32_t* sph = W.sph + (size_t)i * M.ns;
         for (int c = 0; c < M.n_channels; ++c)
@@ -52,7 +56,7 @@ __global__ void k_observe(const __grid_constant__ DevModel<R> M, Worlds<R> W, do
         }
     }
     if (flags)
-        flags[i] = W.unstable[i];
+        flags[k] = W.unstable[i];
 }
 
 // Height of the column under (x, y) in FP64 (csrc/arc_terrain.h:42-50).
@@ -377,11 +381,14 @@ static inline int blocks_for(long long n, int threads) { return (int)((n + threa
 
 template <class R>
 cudaError_t launch_observe(const DevModel<R>& M, const Worlds<R>& W, double* root, double* rot, double* joints,
-                           double* contacts, int* flags, cudaStream_t stream)
+                           double* contacts, int* flags, cudaStream_t stream, const int* ids, int n_items)
 {
-    if (W.n <= 0)
+    if (!ids)
+        n_items = W.n;
+    if (W.n <= 0 || n_items <= 0)
         return cudaSuccess;
-    k_observe<R><<<blocks_for(W.n, 128), 128, 0, stream>>>(M, W, root, rot, joints, contacts, flags);
+    k_observe<R><<<blocks_for(n_items, 128), 128, 0, stream>>>(M, W, root, rot, joints, contacts, flags, ids,
+                                                               n_items);
     return cudaGetLastError();
 }
 
@@ -447,7 +454,7 @@ cudaError_t launch_set_terrain(const Worlds<R>& W, TerrainGeom<R>* tg, TerrainGe
 
 #define ARC_INSTANTIATE_IO(R)                                                                                      \
     template cudaError_t launch_observe<R>(const DevModel<R>&, const Worlds<R>&, double*, double*, double*,      \
-                                           double*, int*, cudaStream_t);                                         \
+                                           double*, int*, cudaStream_t, const int*, int);                        \
     template cudaError_t launch_heights<R>(const Worlds<R>&, const double*, int, double*, cudaStream_t);          \
     template cudaError_t launch_terrain_at<R>(const Worlds<R>&, const int*, const double*, int, double*,          \
                                               cudaStream_t);                                                     \

@@ -49,9 +49,11 @@ constexpr int kMinOnChipContacts = kWarpsOnChipContacts;
 constexpr int kFastMaxSubsteps = 1023;  // touch counters of the leg-parallel kernel
 
 // ----- outputs of the reference ABI (double precision, any pointer may be null)
+// rows in world order, or with ids the n_items worlds ids[0..n_items) in list order
 template <class R>
 cudaError_t launch_observe(const DevModel<R>& M, const Worlds<R>& W, double* root, double* rot, double* joints,
-                           double* contacts, int* flags, cudaStream_t stream);
+                           double* contacts, int* flags, cudaStream_t stream, const int* ids = nullptr,
+                           int n_items = 0);
 template <class R>
 cudaError_t launch_heights(const Worlds<R>& W, const double* offsets, int k, double* out, cudaStream_t stream);
 template <class R>

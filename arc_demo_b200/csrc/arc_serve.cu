@@ -37,6 +37,10 @@
 namespace {
 
 constexpr int kJ = 12;
+constexpr int kReadChunk = 16384;  // worlds per read-back of final states
+// an observation row: root 13, rotation 9, joints 36, contacts 6, flag 1
+// (the blocks of arc_sim_observe, csrc/arc_sim.h:17-21)
+constexpr int kObsRow = 13 + 9 + 36 + 6 + 1;
 
 // Counter-based normal draws for the OU actions: splitmix64 of (seed, count)
 // gives two uniforms, Box-Muller gives the normal.
@@ -105,7 +109,9 @@ struct Request {
     std::vector<float> actions;  // steps x n x 12, or empty: OU
     unsigned long long ou_seed = 0;
     std::vector<int> slots;
-    std::vector<double> out;
+    double* user_out = nullptr;  // the caller's result buffer, or NULL
+    std::vector<double> out;     // the result when the caller gave none
+    double* dest() { return user_out ? user_out : out.data(); }
     Clock::time_point t_submit, t_admit, t_done;
     bool done = false;
     int status = 0;
@@ -125,6 +131,7 @@ template <class T> struct HostArray {
 struct arc_server {
     arc_sim* sim = nullptr;
     int capacity = 0, state_size = 0, device = 0;
+    int result = ARC_SERVE_STATE, row = 0;  // doubles per world in a result
     std::vector<int> free_slots;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -145,10 +152,14 @@ struct arc_server {
     HostArray<float> h_given;
     HostArray<unsigned char> h_use;
     HostArray<unsigned long long> h_admit_seeds;
+    HostArray<double> h_state;  // kReadChunk final states or observation blocks, pinned
+    HostArray<int> h_read_ids, h_flags;
+    DevArray<int> d_read_ids, d_flags;
+    DevArray<double> d_obs;     // root, rot, joints, contacts blocks of kReadChunk rows
     // statistics (under mu)
     long long ticks = 0, world_steps = 0, completed = 0;
     int max_active = 0;
-    double busy_s = 0.0;
+    double busy_s = 0.0, admit_s = 0.0, step_s = 0.0, evict_s = 0.0;
     int error = 0;
 };
 
@@ -211,6 +222,7 @@ bool admit(arc_server* sv)
 // One control step of every active world; completes finished requests.
 bool tick(arc_server* sv)
 {
+    const auto t0 = Clock::now();
     int n = 0;
     bool any_given = false;
     for (auto& r : sv->active) {
@@ -242,16 +254,75 @@ bool tick(arc_server* sv)
         return false;
     if (!ok(cudaStreamSynchronize(st), sv, "tick"))
         return false;
+    const auto t1 = Clock::now();
     // evict finished requests
     std::vector<std::shared_ptr<Request>> keep, finished;
     for (auto& r : sv->active)
         (++r->done_steps >= r->steps ? finished : keep).push_back(r);
-    for (auto& r : finished) {
-        r->out.resize((size_t)r->n * sv->state_size);
-        r->status = arc_sim_get_state(sv->sim, r->slots.data(), r->n, r->out.data());
+    // results of every finished request, in pinned chunks
+    const size_t row_n = (size_t)sv->row;
+    for (auto& r : finished)
+        if (!r->user_out)
+            r->out.resize((size_t)r->n * row_n);
+    size_t total = 0;
+    for (auto& r : finished)
+        total += r->n;
+    std::vector<std::pair<Request*, int>> owners;  // (request, world index) of each row of the chunk
+    size_t row = 0, ri = 0, wi = 0;
+    while (row < total) {
+        const int m = (int)std::min<size_t>(kReadChunk, total - row);
+        owners.resize(m);
+        for (int k = 0; k < m; ++k) {
+            Request* r = finished[ri].get();
+            sv->h_read_ids.p[k] = r->slots[wi];
+            owners[k] = {r, (int)wi};
+            if (++wi == (size_t)r->n) {
+                wi = 0;
+                ++ri;
+            }
+        }
+        int rc = ARC_OK;
+        if (sv->result == ARC_SERVE_STATE) {
+            rc = arc_sim_get_state(sv->sim, sv->h_read_ids.p, m, sv->h_state.p);
+        } else {
+            double* d = sv->d_obs.p;
+            double *d_root = d, *d_rot = d + (size_t)m * 13, *d_j = d_rot + (size_t)m * 9,
+                   *d_c = d_j + (size_t)m * 36;
+            rc = (ok(cudaMemcpyAsync(sv->d_read_ids.p, sv->h_read_ids.p, sizeof(int) * m, cudaMemcpyHostToDevice,
+                                     sv->stream), sv, "read ids")
+                      ? arc_sim_observe_ids(sv->sim, sv->d_read_ids.p, m, d_root, d_rot, d_j, d_c, sv->d_flags.p,
+                                            sv->stream)
+                      : ARC_ERR_CUDA);
+            if (rc == ARC_OK &&
+                !(ok(cudaMemcpyAsync(sv->h_state.p, d, sizeof(double) * (size_t)m * (kObsRow - 1),
+                                     cudaMemcpyDeviceToHost, sv->stream), sv, "observations") &&
+                  ok(cudaMemcpyAsync(sv->h_flags.p, sv->d_flags.p, sizeof(int) * m, cudaMemcpyDeviceToHost,
+                                     sv->stream), sv, "flags") &&
+                  ok(cudaStreamSynchronize(sv->stream), sv, "read back")))
+                rc = ARC_ERR_CUDA;
+        }
+        for (int k = 0; k < m; ++k) {
+            Request* r = owners[k].first;
+            double* dst = r->dest() + (size_t)owners[k].second * row_n;
+            if (rc) {
+                r->status = rc;
+            } else if (sv->result == ARC_SERVE_STATE) {
+                std::memcpy(dst, sv->h_state.p + (size_t)k * row_n, sizeof(double) * row_n);
+            } else {
+                const double* h = sv->h_state.p;
+                std::memcpy(dst, h + (size_t)k * 13, sizeof(double) * 13);
+                std::memcpy(dst + 13, h + (size_t)m * 13 + (size_t)k * 9, sizeof(double) * 9);
+                std::memcpy(dst + 22, h + (size_t)m * 22 + (size_t)k * 36, sizeof(double) * 36);
+                std::memcpy(dst + 58, h + (size_t)m * 58 + (size_t)k * 6, sizeof(double) * 6);
+                dst[64] = (double)sv->h_flags.p[k];
+            }
+        }
+        row += m;
     }
     sv->active.swap(keep);
     std::lock_guard<std::mutex> lock(sv->mu);
+    sv->step_s += std::chrono::duration<double>(t1 - t0).count();
+    sv->evict_s += std::chrono::duration<double>(Clock::now() - t1).count();
     ++sv->ticks;
     sv->world_steps += n;
     sv->max_active = std::max(sv->max_active, n);
@@ -279,7 +350,12 @@ void engine_loop(arc_server* sv)
                 return;
         }
         const auto t0 = Clock::now();
-        const bool good = admit(sv) && tick(sv);
+        bool good = admit(sv);
+        {
+            std::lock_guard<std::mutex> lock(sv->mu);
+            sv->admit_s += std::chrono::duration<double>(Clock::now() - t0).count();
+        }
+        good = good && tick(sv);
         std::lock_guard<std::mutex> lock(sv->mu);
         sv->busy_s += std::chrono::duration<double>(Clock::now() - t0).count();
         if (!good) {
@@ -304,9 +380,9 @@ void engine_loop(arc_server* sv)
 
 }  // namespace
 
-extern "C" arc_server* arc_server_create(int capacity, double dt, int substeps, int grid, double cell)
+extern "C" arc_server* arc_server_create(int capacity, double dt, int substeps, int grid, double cell, int result)
 {
-    if (capacity <= 0)
+    if (capacity <= 0 || (result != ARC_SERVE_STATE && result != ARC_SERVE_OBSERVE))
         return nullptr;
     auto* sv = new arc_server();
     cudaGetDevice(&sv->device);
@@ -317,6 +393,9 @@ extern "C" arc_server* arc_server_create(int capacity, double dt, int substeps, 
     }
     sv->capacity = capacity;
     sv->state_size = arc_sim_state_size(sv->sim);
+    sv->result = result;
+    sv->row = result == ARC_SERVE_STATE ? sv->state_size : kObsRow;
+    const size_t chunk = (size_t)std::min(capacity, kReadChunk);
     arc_sim_set_kernel(sv->sim, ARC_KERNEL_WARPS, 32);
     sv->stream = static_cast<cudaStream_t>(arc_sim_stream(sv->sim));
     const size_t c = (size_t)capacity;
@@ -333,7 +412,13 @@ extern "C" arc_server* arc_server_create(int capacity, double dt, int substeps, 
                       cudaMallocHost(&sv->h_admit_ids.p, c * sizeof(int)) == cudaSuccess &&
                       cudaMallocHost(&sv->h_given.p, c * kJ * sizeof(float)) == cudaSuccess &&
                       cudaMallocHost(&sv->h_use.p, c) == cudaSuccess &&
-                      cudaMallocHost(&sv->h_admit_seeds.p, c * sizeof(unsigned long long)) == cudaSuccess;
+                      cudaMallocHost(&sv->h_admit_seeds.p, c * sizeof(unsigned long long)) == cudaSuccess &&
+                      cudaMallocHost(&sv->h_state.p, chunk * sv->row * sizeof(double)) == cudaSuccess &&
+                      cudaMallocHost(&sv->h_read_ids.p, chunk * sizeof(int)) == cudaSuccess &&
+                      cudaMallocHost(&sv->h_flags.p, chunk * sizeof(int)) == cudaSuccess &&
+                      cudaMalloc(&sv->d_read_ids.p, chunk * sizeof(int)) == cudaSuccess &&
+                      cudaMalloc(&sv->d_flags.p, chunk * sizeof(int)) == cudaSuccess &&
+                      cudaMalloc(&sv->d_obs.p, chunk * (kObsRow - 1) * sizeof(double)) == cudaSuccess;
     if (!good) {
         std::fprintf(stderr, "arc_server_create: allocation failed for %d slots\n", capacity);
         arc_sim_destroy(sv->sim);
@@ -369,7 +454,8 @@ extern "C" void arc_server_destroy(arc_server* sv)
 }
 
 extern "C" long long arc_server_submit(arc_server* sv, int n_worlds, int n_steps, const unsigned* seeds,
-                                       const double* difficulty, const float* actions, unsigned long long ou_seed)
+                                       const double* difficulty, const float* actions, unsigned long long ou_seed,
+                                       double* out)
 {
     if (!sv || n_worlds <= 0 || n_worlds > sv->capacity || n_steps <= 0 || !seeds || !difficulty)
         return ARC_ERR_ARG;
@@ -381,6 +467,7 @@ extern "C" long long arc_server_submit(arc_server* sv, int n_worlds, int n_steps
     if (actions)
         r->actions.assign(actions, actions + (size_t)n_steps * n_worlds * kJ);
     r->ou_seed = ou_seed;
+    r->user_out = out;
     r->t_submit = Clock::now();
     {
         std::lock_guard<std::mutex> lock(sv->mu);
@@ -413,7 +500,7 @@ extern "C" int arc_server_wait(arc_server* sv, long long id, double timeout_s, d
     }
     if (r->status)
         return r->status;
-    if (out)
+    if (out && !r->user_out)
         std::memcpy(out, r->out.data(), sizeof(double) * r->out.size());
     if (times) {
         times[0] = std::chrono::duration<double>(r->t_admit - r->t_submit).count();
@@ -434,5 +521,8 @@ extern "C" int arc_server_stats(arc_server* sv, double* stats)
     stats[3] = (double)sv->max_active;
     stats[4] = (double)sv->completed;
     stats[5] = (double)sv->queue.size();
+    stats[6] = sv->admit_s;
+    stats[7] = sv->step_s;
+    stats[8] = sv->evict_s;
     return sv->error;
 }

@@ -973,6 +973,21 @@ int arc_sim_observe_device(const arc_sim* s, double* root, double* rot, double* 
 
 int arc_sim_synchronize(const arc_sim* s) { return sync(s, "arc_sim_synchronize"); }
 
+int arc_sim_observe_ids(const arc_sim* s, const int* d_ids, int n_ids, double* root, double* rot, double* joints,
+                        double* contacts, int* flags, void* stream)
+{
+    if (n_ids < 0 || (n_ids > 0 && !d_ids))
+        return fail(s, ARC_ERR_ARG, "arc_sim_observe_ids: need device ids");
+    if (n_ids == 0)
+        return ARC_OK;
+    cudaStream_t st = stream_of(s, stream);
+    cudaError_t e = s->fp64 ? launch_observe<double>(s->md, view<double>(s), root, rot, joints, contacts, flags, st,
+                                                     d_ids, n_ids)
+                            : launch_observe<float>(s->mf, view<float>(s), root, rot, joints, contacts, flags, st,
+                                                    d_ids, n_ids);
+    return check(s, e, "observe kernel");
+}
+
 
 // ============================================================================
 // the task layer on the device

@@ -181,6 +181,10 @@ int arc_sim_synchronize(const arc_sim *s);
  * plain one. */
 int arc_sim_step_ids(arc_sim *s, const int *d_ids, int n_ids, const double *d_targets, const float *d_actions,
                      void *stream);
+/* observe of the listed worlds (device ids) into device buffers whose row k
+ * belongs to world d_ids[k] (same blocks as arc_sim_observe; any may be NULL) */
+int arc_sim_observe_ids(const arc_sim *s, const int *d_ids, int n_ids, double *root, double *rot, double *joints,
+                        double *contacts, int *flags, void *stream);
 /* on != 0: the warp-per-leg kernel runs one wave of resident CTAs that take
  * groups of 32 worlds from a device work queue, instead of one CTA per group */
 int arc_sim_set_work_queue(arc_sim *s, int on);
@@ -197,22 +201,33 @@ int arc_probe_fp32_peak(double *flops_per_s, double *seconds);
  * whose steps are done has its final states read back and its slots freed.
  * Thread-safe: any number of client threads may submit and wait. */
 typedef struct arc_server arc_server;
-arc_server *arc_server_create(int capacity, double dt, int substeps, int grid, double cell);
+/* results: the final state of each world (arc_sim_state_size doubles, the
+ * arc_sim_get_state layout) or its final observation (65 doubles: root 13,
+ * rot 9, joints 36, contacts 6, flag 1, as arc_sim_observe) */
+#define ARC_SERVE_STATE 0
+#define ARC_SERVE_OBSERVE 1
+arc_server *arc_server_create(int capacity, double dt, int substeps, int grid, double cell, int result);
 /* Stops the engine; requests still queued fail. */
 void arc_server_destroy(arc_server *sv);
 /* A request: n_worlds fresh episodes (seeds, difficulty as arc_sim_reset)
  * stepped n_steps control steps with actions (n_steps x n_worlds x 12 FP32,
  * as arc_sim_step_actions; copied) or, with actions NULL, an
  * Ornstein-Uhlenbeck process per world (theta 0.15, sigma 0.3, clipped to
- * [-1, 1]) seeded by ou_seed. Returns the request id (>= 0) or < 0. */
+ * [-1, 1]) seeded by ou_seed. out: n_worlds results (kept alive by the
+ * caller until the wait returns), or NULL to receive them through
+ * arc_server_wait. Returns the request id (>= 0) or < 0. */
 long long arc_server_submit(arc_server *sv, int n_worlds, int n_steps, const unsigned *seeds,
-                            const double *difficulty, const float *actions, unsigned long long ou_seed);
-/* Waits up to timeout_s for request id: 1 when done (out: n_worlds x
- * arc_sim_state_size final states; times: seconds queued, running, total;
- * either may be NULL), 0 on timeout, < 0 on error. An id is returned once. */
+                            const double *difficulty, const float *actions, unsigned long long ou_seed,
+                            double *out);
+/* Waits up to timeout_s for request id: 1 when done (out, for a request
+ * submitted without one: the n_worlds results; times:
+ * seconds queued, running, total; either may be NULL), 0 on timeout, < 0 on
+ * error. An id is returned once. */
 int arc_server_wait(arc_server *sv, long long id, double timeout_s, double *out, double *times);
-/* stats: ticks, world-steps, engine busy seconds, most worlds in one tick,
- * completed requests, queued requests. Returns the engine's error (0 ok). */
+/* stats (9 doubles): ticks, world-steps, engine busy seconds, most worlds
+ * in one tick, completed requests, queued requests, then the busy seconds
+ * split into admission (resets), stepping (actions and the step launch) and
+ * eviction (reading back final states). Returns the engine's error (0 ok). */
 int arc_server_stats(arc_server *sv, double *stats);
 
 /* ---- one control step without any device allocation. No counterpart in

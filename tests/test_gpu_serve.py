@@ -42,12 +42,12 @@ def test_mix_equals_alone():
             t.start()
         for t in threads:
             t.join()
-        mixed = [sv.wait(ids[i], len(reqs[i][0]))[0] for i in range(len(reqs))]
+        mixed = [sv.wait(ids[i])[0] for i in range(len(reqs))]
         st = sv.stats()
         assert st["error"] == 0 and st["completed"] == len(reqs)
     with Server(256) as sv:
         for i, (s, d, k, ou) in enumerate(reqs):
-            alone, times = sv.wait(sv.submit(s, d, k, ou_seed=ou), len(s))
+            alone, times = sv.wait(sv.submit(s, d, k, ou_seed=ou))
             assert np.array_equal(alone, mixed[i]), f"request {i} differs in the mix"
             assert times[2] >= times[1] >= 0
 
@@ -61,7 +61,7 @@ def test_given_actions_equal_direct_stepping():
     diff = rng.uniform(0, 1, n)
     actions = rng.uniform(-1.2, 1.2, (k, n, 12)).astype(np.float32)
     with Server(64) as sv:
-        served, _ = sv.wait(sv.submit(seeds, diff, k, actions=actions), n)
+        served, _ = sv.wait(sv.submit(seeds, diff, k, actions=actions))
     sim = Sim(n)
     sim.set_kernel(KERNEL_WARPS)
     sim.reset(np.arange(n), seeds, diff)
@@ -74,10 +74,32 @@ def test_given_actions_equal_direct_stepping():
     assert np.array_equal(served, sim.get_state())
 
 
+def test_observation_results_match_observe():
+    """A server returning observations gives, per world, the blocks
+    arc_sim_observe gives for the same worlds stepped the same way."""
+    rng = np.random.default_rng(3)
+    n, k = 37, 3
+    seeds = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    diff = rng.uniform(0, 1, n)
+    actions = rng.uniform(-1, 1, (k, n, 12)).astype(np.float32)
+    with Server(128, result="state") as a, Server(128, result="observe") as b:
+        state, _ = a.wait(a.submit(seeds, diff, k, actions=actions))
+        obs, _ = b.wait(b.submit(seeds, diff, k, actions=actions))
+    sim = Sim(n)
+    sim.set_state(state)
+    root, joints, contacts, flags = sim.observe()
+    assert obs.shape == (n, 65)
+    assert np.array_equal(obs[:, :13], root)
+    assert np.array_equal(obs[:, 13:22], sim.rot.reshape(n, 9))
+    assert np.array_equal(obs[:, 22:58], joints)
+    assert np.array_equal(obs[:, 58:64], contacts)
+    assert np.array_equal(obs[:, 64], flags.astype(np.float64))
+
+
 def test_request_larger_than_the_pool_is_refused():
     with Server(16) as sv:
         with pytest.raises(RuntimeError):
             sv.submit(np.arange(17, dtype=np.uint32), np.zeros(17), 1)
         # the engine keeps serving
-        out, _ = sv.wait(sv.submit(np.arange(16, dtype=np.uint32), np.zeros(16), 2), 16)
+        out, _ = sv.wait(sv.submit(np.arange(16, dtype=np.uint32), np.zeros(16), 2))
         assert np.isfinite(out).all()
