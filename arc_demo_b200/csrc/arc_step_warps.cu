@@ -190,7 +190,8 @@ __device__ __forceinline__ void joint_positions(P& bp, const BodyK<F>& kp, P& bc
 // second body and alpha = 0, :226-242). Returns 1 when the sphere touched.
 template <class Rec>
 __device__ __forceinline__ int collide(P& b, const BodyK<F>& k, V xprev, Q qprev, const SphereK<F>& sk,
-                                       SphereState<F>& ss, const TerrainView<F>& t, const StepK<F>& st, Rec&& record)
+                                       SphereState<F>& ss, const TerrainView<F>& t, F inv_cell, const StepK<F>& st,
+                                       Rec&& record)
 {
     const F rad = sk.radius;
     V c = b.x + mul(b.rot, sk.pos);
@@ -199,16 +200,14 @@ __device__ __forceinline__ int collide(P& b, const BodyK<F>& k, V xprev, Q qprev
         ss.anchored = 0;
         return 0;
     }
-    int ix0 = 0, ix1 = 0, iy0 = 0, iy1 = 0;
-#pragma unroll 1
-    for (int e = 0; e < 4; ++e) {
-        const F cv = e < 2 ? c.x : c.y, o = e < 2 ? t.ox : t.oy;
-        const int v = (int)r_floor((((e & 1) ? cv + rad : cv - rad) - o) / t.cell);
-        if (e == 0) ix0 = v;
-        else if (e == 1) ix1 = v;
-        else if (e == 2) iy0 = v;
-        else iy1 = v;
-    }
+    // the columns under the sphere's box (csrc/arc_phys.c:557-560), scaled by
+    // 1/cell instead of divided by cell: the two differ only when a box edge
+    // lies within an ulp of a column edge, where that column's face is the
+    // sphere's radius away and cannot make a contact either way
+    const int ix0 = (int)r_floor(((c.x - rad) - t.ox) * inv_cell);
+    const int ix1 = (int)r_floor(((c.x + rad) - t.ox) * inv_cell);
+    const int iy0 = (int)r_floor(((c.y - rad) - t.oy) * inv_cell);
+    const int iy1 = (int)r_floor(((c.y + rad) - t.oy) * inv_cell);
     F ln = F(0), depth_max = F(0);
     V n_max{F(0), F(0), F(1)};
     int touched = 0, ix = ix0, iy = iy0;
@@ -433,6 +432,7 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
         if (leg == torso_warp)
             anch |= ((sphr[0] >> 16) & 1u) << 5;
         const TerrainView<F> T = terrain_of(W, wi);
+        const F inv_cell = F(1) / T.cell;
         const StepK<F>& st = M.step;
         unsigned long long touches = 0;  // 10 bits per sphere: leg spheres 0..4, torso sphere at 50
         const uint32_t* ops = &kOps[capped ? 1 : 0][leg][0];
@@ -530,7 +530,7 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
                             const int bit = s == 0 ? 5 : s - 1;
                             const Ref ra{s == 0 ? &sm.torso[kBodyF][j] : &sm.anch[leg][6 * (s - 1)][j]};
                             SphereState<F> ss{getv(ra, 0), getv(ra, 3), (int)((anch >> bit) & 1u)};
-                            const int t = collide(pose, k, xp, qp, M.sphere[s == 0 ? 0 : 5 * leg + s], ss, T, st,
+                            const int t = collide(pose, k, xp, qp, M.sphere[s == 0 ? 0 : 5 * leg + s], ss, T, inv_cell, st,
                                                          [&](V l, V n) { record(bid, l, n); });
                             touches += (unsigned long long)t << (10 * bit);
                             anch = (anch & ~(1u << bit)) | ((uint32_t)(ss.anchored != 0) << bit);
