@@ -25,6 +25,10 @@ INCLUDE = HERE.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills", f"-I{INCLUDE}", f"-I{CSRC}"]
+# per-file flags: the warp-per-leg FP32 step divides and takes square roots
+# with the full-range approximate instructions (at most 2 ulp), whose errors
+# are far below the FP32 parity bounds its tests hold it to
+FILE_FLAGS = {"arc_step_warps.cu": ["-prec-div=false", "-prec-sqrt=false"]}
 
 
 def nvcc() -> str:
@@ -54,7 +58,7 @@ def build(verbose: bool = False, force: bool = False, extra: list[str] | None = 
     for src in sources():
         obj = BUILD / (src.stem + ".o")
         if force or _stale(obj, src):
-            jobs.append([cc, *ARCH, *FLAGS, *extra, "-c", str(src), "-o", str(obj)])
+            jobs.append([cc, *ARCH, *FLAGS, *FILE_FLAGS.get(src.name, []), *extra, "-c", str(src), "-o", str(obj)])
 
     def run(cmd):
         r = subprocess.run(cmd, capture_output=True, text=True)
