@@ -69,6 +69,8 @@ cudaError_t launch_set_state(const DevModel<R>& M, const Worlds<R>& W, const int
                              cudaStream_t stream);
 
 // ----- resets (FP64): seeded terrain + noisy stance (csrc/arc_sim.c:88-121)
+// The reset kernels' RNG skip table; once per device, before any reset.
+cudaError_t init_reset_tables(cudaStream_t stream);
 template <class R>
 cudaError_t launch_reset(const ResetModel& RM, const Worlds<R>& W, TerrainGeom<R>* tg, TerrainGeomD* tgd,
                          const int* ids, int n_ids, const unsigned* seeds, const double* difficulty,

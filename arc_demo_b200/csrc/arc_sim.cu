@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -259,6 +260,25 @@ void free_all(arc_sim* s)
     delete s->hworld;
 }
 
+// the reset kernels' skip table, built once on each device that creates a sim
+int ensure_reset_tables(arc_sim* s)
+{
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    if (check(s, cudaGetDevice(&dev), "cudaGetDevice"))
+        return ARC_ERR_CUDA;
+    if (dev < 0 || dev >= 64)
+        return fail(s, ARC_ERR_UNSUPPORTED, "more than 64 devices");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!done[dev]) {
+        if (check(s, init_reset_tables(s->stream), "reset tables"))
+            return ARC_ERR_CUDA;
+        done[dev] = true;
+    }
+    return ARC_OK;
+}
+
 arc_sim* create_with_model(const ModelHost& model, int n, double dt, int substeps, int grid, double cell,
                            unsigned flags, const int* grids = nullptr)
 {
@@ -309,6 +329,7 @@ arc_sim* create_with_model(const ModelHost& model, int n, double dt, int substep
     ok = ok && cudaMalloc((void**)&s->tgd, nn * sizeof(TerrainGeomD)) == cudaSuccess;
     ok = ok && cudaMalloc((void**)&s->grid_of, nn * sizeof(int)) == cudaSuccess;
     ok = ok && ensure_spill(s, cell) == ARC_OK;
+    ok = ok && ensure_reset_tables(s) == ARC_OK;
     if (ok && n > 0)
         ok = (s->fp64 ? init_worlds<double>(s) : init_worlds<float>(s)) == ARC_OK;
     if (!ok) {

@@ -34,6 +34,51 @@ struct Xorshift {
     }
 };
 
+// Jumping ahead in the stream. xorshift128 is linear over GF(2): one step
+// is a 128 x 128 bit matrix M acting on the state (s0 s1 s2 s3). Column b
+// of M^(2^k), for k < kJumpBits, is g_jump[k][b] (built once per device by
+// k_jump_init), so skipping d draws costs one XOR of a column per set state
+// bit, for each set bit of d; the draws that follow are the stream's own,
+// bit for bit.
+constexpr int kJumpBits = 13;  // skips below 8,192 draws (a 64 x 64 terrain takes 4,742)
+__device__ uint4 g_jump[kJumpBits][128];
+
+__global__ void k_jump_init()
+{
+    const int k = blockIdx.x, b = threadIdx.x;
+    Xorshift r;
+    for (int w = 0; w < 4; ++w)
+        r.s[w] = (b >> 5) == w ? 1u << (b & 31) : 0u;
+    for (int it = 0; it < (1 << k); ++it)
+        r.next();
+    g_jump[k][b] = make_uint4(r.s[0], r.s[1], r.s[2], r.s[3]);
+}
+
+__device__ __forceinline__ void rng_skip(Xorshift& r, uint32_t d)
+{
+    for (int k = 0; d; ++k, d >>= 1) {
+        if (!(d & 1u))
+            continue;
+        uint32_t o[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            uint32_t bits = r.s[w];
+            while (bits) {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1u;
+                const uint4 c = g_jump[k][w * 32 + b];
+                o[0] ^= c.x;
+                o[1] ^= c.y;
+                o[2] ^= c.z;
+                o[3] ^= c.w;
+            }
+        }
+#pragma unroll
+        for (int w = 0; w < 4; ++w)
+            r.s[w] = o[w];
+    }
+}
+
 // rng_range(lo, hi) of a raw draw u (csrc/arc_rng.h:45-53)
 __device__ __forceinline__ double range_of(uint32_t u, double lo, double hi)
 {
@@ -322,16 +367,22 @@ __global__ void k_task_observe(const __grid_constant__ DevModel<R> M, Worlds<R> 
 
 // ---------------------------------------------------------------------------
 // warp-cooperative reset (csrc/arc_sim.c:88-110, csrc/arc_terrain.c:35-71):
-// lane 0 draws the world's RNG stream into shared memory, all lanes build
-// the terrain columns, lane 0 poses the robot.
+// each lane draws one consecutive slice of the world's RNG stream (skipping
+// ahead to it), all lanes build the terrain columns, lane 0 poses the robot.
+// The columns' jitter draws go straight into the world's own terrain array,
+// each to the slot its height later overwrites, so a warp needs only ~7 KB
+// of shared memory and dozens of worlds reset side by side on every SM.
 
 constexpr int kLat1 = (kGridMax / 8 + 2) * (kGridMax / 8 + 2);   // 100
 constexpr int kLat2 = (kGridMax / 3 + 2) * (kGridMax / 3 + 2);   // 529
-constexpr int kMaxDraws = kLat1 + kLat2 + kGridMax * kGridMax + kMaxJoints + 1;
 
 struct ResetSmem {
-    uint32_t draws[kMaxDraws];
     double lat[kLat1 + kLat2];
+    // lattice coordinates of column index i for the two spacings (8, 3):
+    // integer part and smoothed fraction (csrc/arc_terrain.c:41-45)
+    double frac[2][kGridMax];
+    int whole[2][kGridMax];
+    uint32_t pose[kMaxJoints + 1];  // the stance noise and yaw draws
 };
 
 // The generator's arithmetic is written with explicitly rounded FP64
@@ -343,11 +394,18 @@ __device__ __forceinline__ double smooth(double t)
     return __dmul_rn(__dmul_rn(t, t), __dsub_rn(3.0, __dmul_rn(2.0, t)));
 }
 
-__device__ __forceinline__ double noise_at(const double* lat, int m, int spacing, int ix, int iy)
+__device__ __forceinline__ void lattice_coord(int spacing, int i, int& g, double& t)
 {
-    double fx = __ddiv_rn((double)ix, (double)spacing), fy = __ddiv_rn((double)iy, (double)spacing);
-    int gx = (int)fx, gy = (int)fy;
-    double tx = smooth(__dsub_rn(fx, (double)gx)), ty = smooth(__dsub_rn(fy, (double)gy));
+    const double f = __ddiv_rn((double)i, (double)spacing);
+    g = (int)f;
+    t = smooth(__dsub_rn(f, (double)g));
+}
+
+__device__ __forceinline__ double noise_at(const double* lat, int m, const double* frac, const int* whole, int ix,
+                                           int iy)
+{
+    const int gx = whole[ix], gy = whole[iy];
+    const double tx = frac[ix], ty = frac[iy];
     double a = lat[gx + gy * m], b = lat[gx + 1 + gy * m];
     double c = lat[gx + (gy + 1) * m], d = lat[gx + 1 + (gy + 1) * m];
     double top = __dadd_rn(a, __dmul_rn(__dsub_rn(b, a), tx));
@@ -356,11 +414,12 @@ __device__ __forceinline__ double noise_at(const double* lat, int m, int spacing
 }
 
 // one column: hills + bumps + jitter, quantised (csrc/arc_terrain.c:93-118)
-__device__ __forceinline__ double column_height(const double* lat1, int m1, const double* lat2, int m2, int ix,
-                                                int iy, double amp1, double amp2, double ampj, uint32_t draw)
+__device__ __forceinline__ double column_height(const ResetSmem& sm, const double* lat1, int m1, const double* lat2,
+                                                int m2, int ix, int iy, double amp1, double amp2, double ampj,
+                                                uint32_t draw)
 {
-    double v = __dadd_rn(0.0, __dmul_rn(amp1, noise_at(lat1, m1, 8, ix, iy)));
-    v = __dadd_rn(v, __dmul_rn(amp2, noise_at(lat2, m2, 3, ix, iy)));
+    double v = __dadd_rn(0.0, __dmul_rn(amp1, noise_at(lat1, m1, sm.frac[0], sm.whole[0], ix, iy)));
+    v = __dadd_rn(v, __dmul_rn(amp2, noise_at(lat2, m2, sm.frac[1], sm.whole[1], ix, iy)));
     const double u = __dmul_rn((double)draw, 1.0 / 4294967296.0);
     const double jitter = __dadd_rn(-1.0, __dmul_rn(2.0, u));
     const double hj = __dadd_rn(v, __dmul_rn(ampj, jitter));
@@ -391,16 +450,35 @@ __device__ void reset_world_warp(ResetSmem& sm, const ResetModel& RM, const Worl
     const int m1 = n / 8 + 2, m2 = n / 3 + 2;
     const int L = rough ? m1 * m1 + m2 * m2 : 0;
     const int J = rough ? n * n : 0;
-    const int total = L + J + RM.nj + 1;
-    if (lane == 0) {
+    R* h = W.th + W.toff[i];
+    // the raw jitter draw of column c sits in the low word of h[c] until the
+    // column's height replaces it
+    uint32_t* hdraw = reinterpret_cast<uint32_t*>(h);
+    constexpr int kStep = sizeof(R) / sizeof(uint32_t);
+    {
+        // slices of 2^kSliceBits draws: a lane skips by its index times a
+        // power of two, a few columns of five tables
+        constexpr int kSliceBits = 8;
+        const int total = L + J + RM.nj + 1;
+        const int per = total <= 32 << kSliceBits ? 1 << kSliceBits : (total + 31) / 32;
+        const int first = lane * per, last = first + per < total ? first + per : total;
         Xorshift rng;
         rng.seed(seed);
-        for (int k = 0; k < total; ++k)
-            sm.draws[k] = rng.next();
+        if (first < last)
+            rng_skip(rng, (uint32_t)first);
+        for (int k = first; k < last; ++k) {
+            const uint32_t u = rng.next();
+            if (k < L)
+                sm.lat[k] = __dadd_rn(-1.0, __dmul_rn(2.0, __dmul_rn((double)u, 1.0 / 4294967296.0)));
+            else if (k < L + J)
+                hdraw[(k - L) * kStep] = u;
+            else
+                sm.pose[k - L - J] = u;
+        }
     }
-    __syncwarp();
-    for (int k = lane; k < L; k += 32)
-        sm.lat[k] = __dadd_rn(-1.0, __dmul_rn(2.0, __dmul_rn((double)sm.draws[k], 1.0 / 4294967296.0)));
+    for (int c = lane; c < 2 * kGridMax; c += 32)
+        lattice_coord(c < kGridMax ? 8 : 3, c % kGridMax, sm.whole[c / kGridMax][c % kGridMax],
+                      sm.frac[c / kGridMax][c % kGridMax]);
     __syncwarp();
 
     TerrainGeomD g;
@@ -413,7 +491,6 @@ __device__ void reset_world_warp(ResetSmem& sm, const ResetModel& RM, const Worl
         tgd[i] = g;
         tg[i] = TerrainGeom<R>{n, n, (R)g.cell, (R)g.ox, (R)g.oy, (R)g.outside};
     }
-    R* h = W.th + W.toff[i];
     const double reach = RM.footprint + 0.1, step = 0.5 * cell;
     bool out_x = false, out_y = false;
     const unsigned long long mx = scan_cells(reach, step, g.ox, cell, n, out_x);
@@ -432,13 +509,14 @@ __device__ void reset_world_warp(ResetSmem& sm, const ResetModel& RM, const Worl
         double base = g.outside;
         if (f0x >= 0.0 && f0y >= 0.0 && f0x < n && f0y < n) {
             const int ix = (int)f0x, iy = (int)f0y;
-            base = column_height(lat1, m1, lat2, m2, ix, iy, amp1, amp2, ampj, sm.draws[L + ix + iy * n]);
+            base = column_height(sm, lat1, m1, lat2, m2, ix, iy, amp1, amp2, ampj, hdraw[(ix + iy * n) * kStep]);
         }
+        __syncwarp();  // every lane has read the base column's draw
         double gmax = -1e300;
         for (int c = lane; c < n * n; c += 32) {
             const int ix = c % n, iy = c / n;
             const double hf =
-                __dsub_rn(column_height(lat1, m1, lat2, m2, ix, iy, amp1, amp2, ampj, sm.draws[L + c]), base);
+                __dsub_rn(column_height(sm, lat1, m1, lat2, m2, ix, iy, amp1, amp2, ampj, hdraw[c * kStep]), base);
             h[c] = (R)hf;
             if (((mx >> ix) & 1) && ((my >> iy) & 1))
                 gmax = gmax > hf ? gmax : hf;
@@ -456,10 +534,10 @@ __device__ void reset_world_warp(ResetSmem& sm, const ResetModel& RM, const Worl
     // noisy stance, yaw, forward kinematics (csrc/arc_sim.c:99-109, csrc/arc_phys.c:749-782)
     double angles[kMaxJoints];
     for (int j = 0; j < RM.nj; ++j) {
-        double a = RM.default_angles[j] + range_of(sm.draws[L + J + j], -0.1, 0.1);
+        double a = RM.default_angles[j] + range_of(sm.pose[j], -0.1, 0.1);
         angles[j] = a < RM.lo[j] ? RM.lo[j] : (a > RM.hi[j] ? RM.hi[j] : a);
     }
-    const double yaw = range_of(sm.draws[L + J + RM.nj], -kPi, kPi);
+    const double yaw = range_of(sm.pose[RM.nj], -kPi, kPi);
     V3<double> xs[kMaxBodies];
     Q4<double> qs[kMaxBodies];
     const double sy = sin(0.5 * yaw), cyw = cos(0.5 * yaw);
@@ -583,7 +661,7 @@ int reset_grid(int n)
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int cap = sms * 8;
+    const int cap = sms * 32;  // one warp per world, up to 32 resident per SM
     return n < cap ? (n > 0 ? n : 1) : cap;
 }
 
@@ -638,6 +716,13 @@ cudaError_t launch_task_set_targets(const Worlds<R>& W, const TaskParams& P, con
         return cudaSuccess;
     k_task_set_targets<R><<<(n + 127) / 128, 128, 0, stream>>>(W, P, S, ids, xy, n);
     return cudaGetLastError();
+}
+
+cudaError_t init_reset_tables(cudaStream_t stream)
+{
+    k_jump_init<<<kJumpBits, 128, 0, stream>>>();
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? cudaStreamSynchronize(stream) : e;
 }
 
 template <class R>
