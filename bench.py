@@ -179,6 +179,23 @@ def autotune(env, torch, stream, candidates=("warps", 8, 16), steps=4):
     return best, table
 
 
+def max_over_ranks(torch, dist, x: float) -> float:
+    """The largest x over all ranks, on every rank (x itself without a
+    process group): multi-GPU times are the slowest rank's."""
+    if dist is None:
+        return x
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, worlds_per_rank: int, steps: int, ms: float) -> float:
+    """env-steps/s of the whole job: every rank's worlds over the slowest
+    rank's time (weak scaling: each rank owns worlds_per_rank worlds)."""
+    return world * worlds_per_rank * steps / (ms * 1e-3)
+
+
 def run_ours(args) -> dict | None:
     import torch
     rank = int(os.environ.get("RANK", "0"))
@@ -241,11 +258,7 @@ def run_ours(args) -> dict | None:
             torch.cuda.synchronize()
         if dist:
             dist.barrier()
-        ms_total = t0.elapsed_time(t1)
-        if dist:
-            t = torch.tensor([ms_total], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_total = float(t.item())
+        ms_total = max_over_ranks(torch, dist, t0.elapsed_time(t1))
         lat = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
         clock = clocks.summary()
         ended = int(env.done_count.item())
@@ -291,7 +304,11 @@ def run_ours(args) -> dict | None:
             else:
                 env.set_kernel(KERNEL_LEGS, best_wpc)
 
-        e2e = None if args.no_e2e else run_e2e(torch, env, params, stream, max(3, min(K, 50)))
+        e2e = None
+        if not args.no_e2e:
+            e2e = run_e2e(torch, env, params, stream, max(3, min(K, 50)))
+            e2e["ms_per_step"] = round(max_over_ranks(torch, dist, e2e["ms_per_step"]), 4)
+            e2e["value"] = round(whole_job_rate(world, n, 1, e2e["ms_per_step"]), 1)
 
     peak = ctypes.c_double(0.0)
     sim_lib().arc_probe_fp32_peak(ctypes.byref(peak), None)
@@ -301,7 +318,7 @@ def run_ours(args) -> dict | None:
     if rank != 0:
         return None
 
-    value = world * n * K / (ms_total * 1e-3)
+    value = whole_job_rate(world, n, K, ms_total)
     achieved = n * FLOP_PER_ENV_STEP / (step_kernel_ms * 1e-3)
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "env-steps/s", "n_gpus": world, "steps": K,
