@@ -304,7 +304,11 @@ arc_sim* create_with_model(const ModelHost& model, int n, double dt, int substep
     s->fp64 = (flags & ARC_SIM_FP64) != 0;
     s->model = model;
     rebuild_models(s);
-    s->kernel = (flags & ARC_SIM_PLAIN) || !s->model.leaper ? ARC_KERNEL_PLAIN : ARC_KERNEL_LEGS;
+    // the fastest form that steps the model: warp-per-leg (FP32 quadruped),
+    // leg-parallel (FP64 quadruped), plain (any model)
+    s->kernel = (flags & ARC_SIM_PLAIN) || !s->model.leaper ? ARC_KERNEL_PLAIN
+                : s->fp64                                 ? ARC_KERNEL_LEGS
+                                                          : ARC_KERNEL_WARPS;
     const int rs = real_size(s);
     s->off_sphere = s->model.nb * kBodyRec;
     s->off_joint = s->off_sphere + s->model.ns * kSphereRec;
@@ -708,7 +712,7 @@ int arc_sim_get_kernel(const arc_sim* s, int* kernel, int* worlds_per_cta)
     if (kernel)
         *kernel = s->kernel;
     if (worlds_per_cta)
-        *worlds_per_cta = s->wpc;
+        *worlds_per_cta = s->kernel == ARC_KERNEL_WARPS ? 32 : (s->kernel == ARC_KERNEL_PLAIN ? 1 : s->wpc);
     return ARC_OK;
 }
 

@@ -44,9 +44,9 @@ FLOP_PER_ENV_STEP = 415.6e3   # scalar FP ops of one control step, counted on th
 HBM_BYTES_PER_ENV_STEP = 3.9e3  # algorithmic HBM traffic of one env-step (state, actions, obs)
 # DRAM bytes (read + write) one world costs a launch of the warp-per-leg step
 # kernel: ncu's dram__bytes_read.sum + dram__bytes_write.sum over a
-# 16,384-world launch (42.24 MB + 0.15 MB), divided by the worlds; each world
+# 16,384-world launch (42.24 MB + 0.17 MB), divided by the worlds; each world
 # reads its own record and terrain cells, so the traffic scales with them.
-WARPS_DRAM_BYTES_PER_WORLD = (42.237e6 + 0.152e6) / 16384
+WARPS_DRAM_BYTES_PER_WORLD = (42.240e6 + 0.175e6) / 16384
 
 
 def parse():

@@ -38,7 +38,7 @@ typedef struct arc_sim arc_sim;
 /* Replaces csrc/arc_sim.h:25 (csrc/arc_sim.c:26-54). n_worlds worlds of
  * the quadruped on flat grid x grid terrain; grid is clamped to 64.
  * Returns NULL if no CUDA device is usable or memory runs out. Steps in
- * FP32 with the leg-parallel kernel (see arc_sim_create_ex). */
+ * FP32 with the warp-per-leg kernel (see arc_sim_create_ex). */
 arc_sim *arc_sim_create(int n_worlds, double dt, int substeps, int grid, double cell);
 
 /* Replaces csrc/arc_sim.h:26. NULL-safe. */
