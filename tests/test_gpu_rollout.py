@@ -59,3 +59,26 @@ def test_ou_rollout_4096_worlds_with_resets(max_steps):
     if max_steps < steps:
         # every episode ends by max_steps at the latest
         assert ended_total >= n * (steps // max_steps)
+
+
+def test_vec_normalize_over_the_device_env():
+    """The SB3-style adapter and VecNormalize keep everything on the device:
+    normalised observations inside +-10, statistics that move, terminal
+    observations of ended worlds normalised with the same statistics."""
+    import torch
+    from arc_demo_b200.torch_env import DeviceVecEnv
+    from arc_demo_b200.vec_env import DeviceVecEnvAdapter, DeviceVecNormalize
+
+    n = 512
+    env = DeviceVecNormalize(DeviceVecEnvAdapter(DeviceVecEnv(n, TaskConfig(curriculum=False, max_steps=15), seed=4)))
+    obs = env.reset()
+    assert obs.is_cuda and obs.shape == (n, 195)
+    count0 = env.obs_rms.count
+    for a in ou_actions(n, 20, seed=2):
+        obs, rew, done, info = env.step(torch.from_numpy(a).cuda())
+        assert obs.is_cuda and rew.is_cuda and done.is_cuda
+        assert torch.isfinite(obs).all() and obs.abs().max() <= 10.0
+        assert torch.isfinite(rew).all() and rew.abs().max() <= 10.0
+        assert info["terminal_observation"].abs().max() <= 10.0
+    assert env.obs_rms.count == count0 + 20 * n
+    assert bool(done.any())  # max_steps 15: every world has ended once

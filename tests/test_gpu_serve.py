@@ -103,3 +103,32 @@ def test_request_larger_than_the_pool_is_refused():
         # the engine keeps serving
         out, _ = sv.wait(sv.submit(np.arange(16, dtype=np.uint32), np.zeros(16), 2))
         assert np.isfinite(out).all()
+
+
+def test_malformed_requests_are_refused_and_the_engine_keeps_serving():
+    """Faults made on the host: bad sizes are refused at submit, an unknown
+    request id at wait, and none of it disturbs the engine."""
+    import ctypes
+
+    from arc_demo_b200.serve import serve_lib
+
+    lib = serve_lib()
+    with Server(32) as sv:
+        seeds = np.arange(4, dtype=np.uint32)
+        diff = np.zeros(4)
+        for n, k in ((0, 1), (4, 0), (4, -3), (33, 1)):
+            rid = lib.arc_server_submit(sv._ptr, n, k, seeds, diff, None, 0, None)
+            assert rid < 0, (n, k)
+        assert lib.arc_server_wait(sv._ptr, 123456, 0.1, None, None) < 0
+        out, _ = sv.wait(sv.submit(seeds, diff, 3))
+        assert np.isfinite(out).all() and sv.stats()["error"] == 0
+
+
+def test_client_that_never_waits_leaves_the_server_clean():
+    """A client that submits and goes away: its request still runs, its
+    result is dropped with the server, and other clients are served."""
+    with Server(64) as sv:
+        sv.submit(np.arange(20, dtype=np.uint32), np.zeros(20), 5)     # never waited for
+        out, _ = sv.wait(sv.submit(np.arange(8, dtype=np.uint32), np.zeros(8), 2))
+        assert np.isfinite(out).all()
+    # the engine thread and every buffer were released by the close above
