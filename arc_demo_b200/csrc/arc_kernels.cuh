@@ -1,10 +1,32 @@
 // arc_kernels.cuh - launchers of every kernel of the library.
 #pragma once
 
+#include <atomic>
+
 #include <cuda_runtime.h>
 #include "arc_device.cuh"
 
 namespace arc {
+
+// Kernel attributes belong to a device: a launcher's `setup(dev)` runs once
+// for each device it is used on (two first calls racing may both run it,
+// which is harmless: it only sets attributes and reads properties).
+template <class Setup> cudaError_t once_per_device(std::atomic<unsigned long long>& done, Setup&& setup)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return e;
+    if (dev < 0 || dev >= 64)
+        return cudaErrorInvalidDevice;
+    const unsigned long long bit = 1ull << dev;
+    if (done.load(std::memory_order_acquire) & bit)
+        return cudaSuccess;
+    e = setup(dev);
+    if (e == cudaSuccess)
+        done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
 
 // FP64 data of the reset path (csrc/arc_sim.c:88-110, csrc/arc_phys.c:749-782):
 // forward-kinematics frames, default stance, limits.

@@ -417,14 +417,13 @@ static cudaError_t launch_fast_wpc(const DevModel<R>& M, const Worlds<R>& W, con
                                    int spill_per_lane, int lane_cap, cudaStream_t stream)
 {
     const size_t smem = fast::smem_bytes<R>(W.stride, WPC);
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(fast::k_step_fast<R, WPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem > 48 * 1024 ? (int)smem : 48 * 1024);
-        if (e != cudaSuccess)
-            return e;
-        configured = true;
-    }
+    static std::atomic<unsigned long long> configured{0};
+    cudaError_t e = once_per_device(configured, [&](int) {
+        return cudaFuncSetAttribute(fast::k_step_fast<R, WPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem > 48 * 1024 ? (int)smem : 48 * 1024);
+    });
+    if (e != cudaSuccess)
+        return e;
     const int grid = (W.n + WPC - 1) / WPC;
     fast::k_step_fast<R, WPC><<<grid, WPC * fast::kLanes, smem, stream>>>(M, W, A, spill, spill_per_lane, lane_cap);
     return cudaGetLastError();

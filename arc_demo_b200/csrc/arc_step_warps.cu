@@ -721,32 +721,32 @@ cudaError_t launch_step_warps(const DevModel<float>& M, const Worlds<float>& W, 
         return cudaSuccess;
     if (!M.leaper)
         return cudaErrorInvalidValue;
-    static bool configured = false;
     const int smem = (int)sizeof(wl::Smem);
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(wl::k_step_warps, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    // per device: the shared-memory attribute, and how many CTAs are resident
+    // at once (the work queue's wave)
+    static std::atomic<unsigned long long> configured{0};
+    static int resident[64] = {};
+    cudaError_t e = once_per_device(configured, [&](int dev) {
+        cudaError_t r = cudaFuncSetAttribute(wl::k_step_warps, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              smem > 48 * 1024 ? smem : 48 * 1024);
-        if (e != cudaSuccess)
-            return e;
-        configured = true;
-    }
+        int sms = 0, per_sm = 0;
+        if (r == cudaSuccess)
+            r = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (r == cudaSuccess)
+            r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wl::k_step_warps, wl::kThreads, smem);
+        if (r == cudaSuccess)
+            resident[dev] = sms * (per_sm > 0 ? per_sm : 1);
+        return r;
+    });
+    if (e != cudaSuccess)
+        return e;
     const int groups = (n_items + wl::kWorlds - 1) / wl::kWorlds;
     int grid = groups;
     if (queue) {
-        // one wave of resident CTAs
-        static int resident = 0;
-        if (!resident) {
-            int dev = 0, sms = 0, per_sm = 0;
-            cudaError_t e = cudaGetDevice(&dev);
-            if (e == cudaSuccess)
-                e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            if (e == cudaSuccess)
-                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wl::k_step_warps, wl::kThreads, smem);
-            if (e != cudaSuccess)
-                return e;
-            resident = sms * (per_sm > 0 ? per_sm : 1);
-        }
-        grid = groups < resident ? groups : resident;
+        int dev = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess)
+            return e;
+        grid = groups < resident[dev] ? groups : resident[dev];  // one wave of resident CTAs
     }
     wl::k_step_warps<<<grid, wl::kThreads, smem, stream>>>(M, W, A, spill, spill_per_lane, lane_cap, ids, n_items,
                                                            queue);

@@ -695,14 +695,12 @@ cudaError_t launch_task_reset(const DevModel<R>& M, const ResetModel& RM, const 
 {
     if (max_n <= 0)
         return cudaSuccess;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_task_reset<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)sizeof(ResetSmem));
-        if (e != cudaSuccess)
-            return e;
-        configured = true;
-    }
+    static std::atomic<unsigned long long> configured{0};
+    cudaError_t e = once_per_device(configured, [](int) {
+        return cudaFuncSetAttribute(k_task_reset<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(ResetSmem));
+    });
+    if (e != cudaSuccess)
+        return e;
     k_task_reset<R><<<reset_grid(max_n), 32, sizeof(ResetSmem), stream>>>(M, RM, W, tg, tgd, grid_of, cell, P, S, obs,
                                                                        ids, count_dev, max_n);
     return cudaGetLastError();
@@ -732,14 +730,12 @@ cudaError_t launch_reset_warp(const ResetModel& RM, const Worlds<R>& W, TerrainG
 {
     if (n_ids <= 0)
         return cudaSuccess;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_reset_warp<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)sizeof(ResetSmem));
-        if (e != cudaSuccess)
-            return e;
-        configured = true;
-    }
+    static std::atomic<unsigned long long> configured{0};
+    cudaError_t e = once_per_device(configured, [](int) {
+        return cudaFuncSetAttribute(k_reset_warp<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(ResetSmem));
+    });
+    if (e != cudaSuccess)
+        return e;
     k_reset_warp<R><<<reset_grid(n_ids), 32, sizeof(ResetSmem), stream>>>(RM, W, tg, tgd, ids, n_ids, seeds,
                                                                         difficulty, grid_of, cell);
     return cudaGetLastError();
