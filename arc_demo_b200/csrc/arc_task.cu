@@ -208,15 +208,35 @@ __device__ void write_obs(const TaskParams& P, const Worlds<R>& W, const TaskSta
     dst[k++] = obs_value(fwd / dist);
     dst[k++] = obs_value(left / dist);
     dst[k++] = obs_value((dist < 6.0 ? dist : 6.0) / 6.0);
-    // heights in the heading frame (csrc/arc_sim.c:185-203)
+    // heights in the heading frame (csrc/arc_sim.c:185-203), kChunk samples
+    // at a time: their terrain loads are all issued before any is used
     V3<double> f = qrotate(o.q, V3<double>{1.0, 0.0, 0.0});
     const double yaw = atan2(f.y, f.x), cy = cos(yaw), sy = sin(yaw);
-    for (int m = 0; m < kNumOffsets; ++m) {
-        const double fo = P.offsets[m][0], lo = P.offsets[m][1];
-        double h = height_at(W, i, o.x.x + cy * fo - sy * lo, o.x.y + sy * fo + cy * lo);
-        double rel = o.x.z - P.stand_height - h;
-        rel = rel < -1.0 ? -1.0 : (rel > 1.0 ? 1.0 : rel);
-        dst[k++] = obs_value(rel);
+    const TerrainGeomD g = W.tgd[i];
+    const R* th = W.th + W.toff[i];
+    constexpr int kChunk = 8;
+    for (int m0 = 0; m0 < kNumOffsets; m0 += kChunk) {
+        double h[kChunk];
+#pragma unroll
+        for (int u = 0; u < kChunk; ++u) {
+            const int m = m0 + u < kNumOffsets ? m0 + u : kNumOffsets - 1;
+            const double fo = P.offsets[m][0], lo = P.offsets[m][1];
+            const double x = o.x.x + cy * fo - sy * lo, y = o.x.y + sy * fo + cy * lo;
+            // csrc/arc_terrain.h:42-50
+            const double fx = floor((x - g.ox) / g.cell), fy = floor((y - g.oy) / g.cell);
+            const bool in = fx >= 0.0 && fy >= 0.0 && fx < g.nx && fy < g.ny;
+            const int idx = in ? (int)fx + (int)fy * g.nx : 0;
+            const double top = (double)__ldg(th + idx);
+            h[u] = in ? top : g.outside;
+        }
+#pragma unroll
+        for (int u = 0; u < kChunk; ++u) {
+            if (m0 + u >= kNumOffsets)
+                break;
+            double rel = o.x.z - P.stand_height - h[u];
+            rel = rel < -1.0 ? -1.0 : (rel > 1.0 ? 1.0 : rel);
+            dst[k++] = obs_value(rel);
+        }
     }
     for (int l = 0; l < kNumLegs; ++l)
         dst[k++] = obs_value(o.contact[l]);
