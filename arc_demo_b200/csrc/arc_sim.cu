@@ -76,7 +76,7 @@ struct arc_sim {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t graph_stream = nullptr;
-    int graph_kernel = -1, graph_wpc = -1;
+    int graph_kernel = -1, graph_wpc = -1, graph_queue = -1;  // the step form the graph captured
     mutable int err = 0;
     mutable std::string msg;
     mutable bool reported = false;
@@ -1250,7 +1250,8 @@ int arc_env_step(arc_sim* s, const float* d_actions, void* stream)
     if (d_actions)
         return env_step_launches(s, d_actions, st);
     // graph of the whole control step over the ARC_ENV_ACTIONS buffer
-    if (s->graph_exec && (s->graph_kernel != s->kernel || s->graph_wpc != s->wpc)) {
+    if (s->graph_exec &&
+        (s->graph_kernel != s->kernel || s->graph_wpc != s->wpc || s->graph_queue != (int)s->use_queue)) {
         cudaGraphExecDestroy(s->graph_exec);
         cudaGraphDestroy(s->graph);
         s->graph_exec = nullptr;
@@ -1277,6 +1278,7 @@ int arc_env_step(arc_sim* s, const float* d_actions, void* stream)
         s->graph = g;
         s->graph_kernel = s->kernel;
         s->graph_wpc = s->wpc;
+        s->graph_queue = (int)s->use_queue;
         return ARC_OK;
     }
     return check(s, cudaGraphLaunch(s->graph_exec, st), "graph launch");

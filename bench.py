@@ -146,15 +146,17 @@ def policy_forward(torch, params, obs, out):
     torch.addmm(b3, h, w3.t(), out=out)
 
 
-def autotune(env, torch, stream, candidates=("warps", 8, 16), steps=4):
+def autotune(env, torch, stream, candidates=("warps", "warps+queue", 8, 16), steps=4):
     """Step kernel and worlds-per-CTA, by timing the step kernel: the
-    warp-per-leg kernel (32 worlds per CTA) and the leg-parallel kernel at
-    several worlds per CTA."""
+    warp-per-leg kernel (32 worlds per CTA; one CTA per group, or one wave of
+    resident CTAs taking groups from a work queue) and the leg-parallel kernel
+    at several worlds per CTA."""
     from arc_demo_b200.native import KERNEL_LEGS, KERNEL_WARPS
     lib, ptr = env.sim._lib, env.sim.ptr
     best, table = None, {}
     for wpc in candidates:
-        if wpc == "warps":
+        env.sim.set_work_queue(wpc == "warps+queue")
+        if wpc in ("warps", "warps+queue"):
             env.set_kernel(KERNEL_WARPS)
         else:
             env.set_kernel(KERNEL_LEGS, wpc)
@@ -172,7 +174,8 @@ def autotune(env, torch, stream, candidates=("warps", 8, 16), steps=4):
         table[str(wpc)] = round(ms, 4)
         if best is None or ms < table[str(best)]:
             best = wpc
-    if best == "warps":
+    env.sim.set_work_queue(best == "warps+queue")
+    if best in ("warps", "warps+queue"):
         env.set_kernel(KERNEL_WARPS)
     else:
         env.set_kernel(KERNEL_LEGS, best)
@@ -299,7 +302,7 @@ def run_ours(args) -> dict | None:
             plain_kernel_ms = q0.elapsed_time(q1) / 3
             plain = {"ms_per_step": round(plain_ms, 3), "env_steps_per_s": round(n / plain_ms * 1e3),
                      "step_kernel_ms": round(plain_kernel_ms, 3)}
-            if best_wpc == "warps":
+            if best_wpc in ("warps", "warps+queue"):
                 env.set_kernel(KERNEL_WARPS)
             else:
                 env.set_kernel(KERNEL_LEGS, best_wpc)
@@ -327,8 +330,10 @@ def run_ours(args) -> dict | None:
         "config": {"workload": f"{n} worlds of the quadruped per GPU, difficulty uniform in {{0,...,1.0}}, "
                                "checkpoints, auto-reset, random-init MLP policy 195-256-256-12 tanh FP32 in the loop",
                    "worlds_per_gpu": n, "substeps": 20, "dt": 1 / 30,
-                   "kernel": "warp-per-leg" if best_wpc == "warps" else "leg-parallel",
-                   "worlds_per_cta": 32 if best_wpc == "warps" else best_wpc, "autotune_step_kernel_ms": tune,
+                   "kernel": {"warps": "warp-per-leg", "warps+queue": "warp-per-leg, work queue"}.get(
+                       str(best_wpc), "leg-parallel"),
+                   "worlds_per_cta": 32 if str(best_wpc).startswith("warps") else best_wpc,
+                   "autotune_step_kernel_ms": tune,
                    "l2": "inputs larger than L2 (world records + 64x64 terrains: ~1.2 GB per GPU)"},
         "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 4),
                        "p99": round(float(np.percentile(lat, 99)), 4), "max": round(float(lat.max()), 4)},
@@ -337,9 +342,9 @@ def run_ours(args) -> dict | None:
         "roofline": {"bound": "fp32", "achieved": round(achieved / 1e12, 3),
                      "peak": round(peak.value / 1e12, 3), "unit": "TFLOP/s",
                      "frac": round(achieved / peak.value, 4) if peak.value else None,
-                     "traffic": round(n * WARPS_DRAM_BYTES_PER_WORLD) if best_wpc == "warps" else None,
+                     "traffic": round(n * WARPS_DRAM_BYTES_PER_WORLD) if str(best_wpc).startswith("warps") else None,
                      "traffic_unit": "bytes per launch (ncu, scaled from 16,384 worlds)",
-                     "kernel": ("warp-per-leg" if best_wpc == "warps" else "leg-parallel") + " step",
+                     "kernel": ("warp-per-leg" if str(best_wpc).startswith("warps") else "leg-parallel") + " step",
                      "kernel_ms": round(step_kernel_ms, 4),
                      "flop_per_env_step": FLOP_PER_ENV_STEP,
                      "peak_source": "measured FP32 FMA probe (arc_probe_fp32_peak) on this GPU",

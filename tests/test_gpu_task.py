@@ -134,11 +134,16 @@ def test_reset_places_checkpoints_by_the_reference_rule():
     assert st[0, 21] == 0.0 or not np.array_equal(h0, h1)
 
 
-def test_env_graph_step_equals_eager_step():
+@pytest.mark.parametrize("queue", [False, True])
+def test_env_graph_step_equals_eager_step(queue):
+    """The control step as one CUDA graph (captured once, replayed) equals
+    the same launches made eagerly, also with the step kernel's work queue
+    (its counter must come back to zero at the end of every replay)."""
     import torch
     from arc_demo_b200.torch_env import DeviceVecEnv
     n = 96
     envs = [DeviceVecEnv(n, TaskConfig(curriculum=True), seed=7) for _ in range(2)]
+    envs[0].sim.set_work_queue(queue)
     for e in envs:
         e.set_levels(np.linspace(0, 1, n))
         e.reset()
