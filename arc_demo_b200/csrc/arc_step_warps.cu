@@ -361,8 +361,8 @@ __constant__ uint32_t kOps[2][kWarps][kMaxOps] = {
 
 // Work items are worlds (ids[item], or item itself without ids), 32 to a
 // group; CTA b steps group b. With a queue (two ints, zero before the
-// launch), a CTA that finished its group takes the next unclaimed one, and
-// the last CTA to leave zeroes the queue again for the next launch.
+// launch), CTAs take groups from it until none is left, and the last CTA to
+// leave zeroes the queue again for the next launch.
 __global__ void __launch_bounds__(kThreads, 4)
 k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F* __restrict__ spill, int spill_per_lane,
              int lane_cap, const int* __restrict__ ids, int n_items, int* queue)
@@ -372,8 +372,18 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
     __shared__ int s_next;
     const int tid = threadIdx.x, leg = tid / kWorlds, j = tid % kWorlds;
     const int n_groups = (n_items + kWorlds - 1) / kWorlds;
+    // with a queue every group, the first included, is taken from it: a CTA
+    // that becomes resident only when others leave finds the queue empty
+    // instead of holding back a group of its own
+    int first = blockIdx.x;
+    if (queue) {
+        if (tid == 0)
+            s_next = atomicAdd(queue, 1);
+        __syncthreads();
+        first = s_next;
+    }
 #pragma unroll 1
-    for (int group = blockIdx.x; group < n_groups;) {
+    for (int group = first; group < n_groups;) {
         const int item = group * kWorlds + j;
         const int world = item < n_items ? (ids ? ids[item] : item) : -1;
         const bool valid = world >= 0 && world < W.n;
@@ -692,7 +702,7 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
         if (!queue)
             break;
         if (tid == 0)
-            s_next = (int)gridDim.x + atomicAdd(queue, 1);
+            s_next = atomicAdd(queue, 1);
         __syncthreads();
         group = s_next;
     }

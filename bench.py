@@ -150,11 +150,18 @@ def autotune(env, torch, stream, candidates=("warps", "warps+queue", 8, 16), ste
     """Step kernel and worlds-per-CTA, by timing the step kernel: the
     warp-per-leg kernel (32 worlds per CTA; one CTA per group, or one wave of
     resident CTAs taking groups from a work queue) and the leg-parallel kernel
-    at several worlds per CTA."""
+    at several worlds per CTA. Every candidate starts from the same world
+    states: the step's cost grows over the first steps after a reset, as the
+    robots settle and their contacts multiply, so timing the candidates one
+    after another from a running state would favour the first."""
     from arc_demo_b200.native import KERNEL_LEGS, KERNEL_WARPS
     lib, ptr = env.sim._lib, env.sim.ptr
     best, table = None, {}
+    stream.synchronize()
+    start = env.sim.get_state()
     for wpc in candidates:
+        env.sim.set_state(start)
+        torch.cuda.synchronize()
         env.sim.set_work_queue(wpc == "warps+queue")
         if wpc in ("warps", "warps+queue"):
             env.set_kernel(KERNEL_WARPS)
@@ -174,6 +181,8 @@ def autotune(env, torch, stream, candidates=("warps", "warps+queue", 8, 16), ste
         table[str(wpc)] = round(ms, 4)
         if best is None or ms < table[str(best)]:
             best = wpc
+    env.sim.set_state(start)
+    torch.cuda.synchronize()
     env.sim.set_work_queue(best == "warps+queue")
     if best in ("warps", "warps+queue"):
         env.set_kernel(KERNEL_WARPS)
