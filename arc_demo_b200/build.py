@@ -20,6 +20,9 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 LIB = HERE / "libarcsim.so"
+# the reference loads its renderer from a second library (arc/native.py:59-70);
+# this one only depends on libarcsim.so, which exports the arc_render_* calls
+RENDER_LIB = HERE / "libarcrender.so"
 INCLUDE = HERE.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -73,6 +76,10 @@ def build(verbose: bool = False, force: bool = False, extra: list[str] | None = 
     objs = [str(BUILD / (s.stem + ".o")) for s in sources()]
     if jobs or not LIB.exists():
         run([cc, *ARCH, "-shared", "-o", str(LIB), *objs, "-lcudart_static", "-lrt", "-ldl", "-lpthread"])
+    if jobs or not RENDER_LIB.exists():
+        cxx = shutil.which("gcc") or "gcc"
+        run([cxx, "-shared", "-fPIC", "-o", str(RENDER_LIB), "-x", "c", os.devnull, f"-L{HERE}",
+             "-Wl,--no-as-needed", "-larcsim", "-Wl,-rpath,$ORIGIN"])
     return LIB
 
 

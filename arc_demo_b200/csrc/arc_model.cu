@@ -48,6 +48,15 @@ int ModelHost::add_sphere(int body, V3<double> pos, double radius)
     return ns++;
 }
 
+int ModelHost::add_visual(int type, int body, V3<double> p0, V3<double> p1, double radius, double radius2,
+                          int material, const float* rgb)
+{
+    if (nv >= kMaxVisuals)
+        return -1;
+    v[nv] = Visual{type, body, material, p0, p1, radius, radius2, 1.0, {rgb[0], rgb[1], rgb[2]}};
+    return nv++;
+}
+
 int ModelHost::add_hinge(int parent, int child, V3<double> anchor, V3<double> axis_world)
 {
     if (nj >= kMaxJoints || child <= parent)
@@ -112,6 +121,70 @@ constexpr double kCoxaLen = 0.06, kFemurLen = 0.50, kTibiaLen = 0.95, kFootR = 0
 constexpr double kKp = 250.0, kKd = 6.0, kMaxTorque = 80.0;
 }  // namespace leaper
 
+// Surface colours (sRGB) of csrc/arc_robot.c:38-47.
+namespace paint {
+constexpr float kArmor[3] = {0.40f, 0.41f, 0.43f}, kHull[3] = {0.34f, 0.345f, 0.36f};
+constexpr float kDark[3] = {0.17f, 0.17f, 0.18f}, kSteel[3] = {0.52f, 0.53f, 0.55f};
+constexpr float kBezel[3] = {0.72f, 0.73f, 0.74f}, kCable[3] = {0.30f, 0.30f, 0.31f};
+constexpr float kBlack[3] = {0.06f, 0.06f, 0.065f}, kGlow[3] = {1.00f, 0.10f, 0.06f};
+constexpr float kDimGlow[3] = {0.62f, 0.05f, 0.03f};
+}  // namespace paint
+
+// A faceted armour plate along body z (csrc/arc_robot.c:55-61).
+static void add_plate(ModelHost& m, int body, V3<double> p0, V3<double> p1, double r0, double r1, double aspect)
+{
+    int i = m.add_visual(kVisTaper, body, p0, p1, r0, r1, kMatPaint, paint::kArmor);
+    if (i >= 0)
+        m.v[i].aspect = aspect;
+}
+
+// The visuals of one leg, in the order of csrc/arc_robot.c:114-142: hip
+// hinge and collar on the coxa; knee axle, armour plate, cable sleeve, knee
+// block, knee hinge and its two lights on the femur; two plates, a sleeve,
+// the ankle, its collars and the rubber foot on the tibia.
+static void add_leg_visuals(ModelHost& m, int bc, int bf, int bt, V3<double> d, double fl, double tl)
+{
+    using V = V3<double>;
+    using namespace paint;
+    m.add_visual(kVisCylinder, bc, scale(d, -0.05), scale(d, 0.035), 0.062, 0.0, kMatMetal, kDark);
+    m.add_visual(kVisRing, bc, scale(d, 0.02), d, 0.062, 0.012, kMatMetal, kSteel);
+    m.add_visual(kVisCylinder, bf, V{0, -0.07, -fl}, V{0, 0.07, -fl}, 0.045, 0.0, kMatMetal, kDark);
+    add_plate(m, bf, V{-0.012, 0, -fl + 0.02}, V{-0.012, 0, fl - 0.02}, 0.055, 0.08, 0.8);
+    m.add_visual(kVisCylinder, bf, V{0.055, 0, -fl + 0.06}, V{0.07, 0, fl - 0.07}, 0.022, 0.0, kMatRibs, kCable);
+    m.add_visual(kVisBox, bf, V{0, 0, fl}, V{0.085, 0.07, 0.075}, 0.0, 0.0, kMatPaint, kDark);
+    m.add_visual(kVisCylinder, bf, V{0, -0.085, fl}, V{0, 0.085, fl}, 0.048, 0.0, kMatMetal, kSteel);
+    m.add_visual(kVisCylinder, bf, V{0, 0.085, fl}, V{0, 0.089, fl}, 0.02, 0.0, kMatGlow, kGlow);
+    m.add_visual(kVisCylinder, bf, V{0, -0.089, fl}, V{0, -0.085, fl}, 0.02, 0.0, kMatGlow, kGlow);
+    add_plate(m, bt, V{-0.01, 0, -tl + 0.03}, V{-0.01, 0, -0.05}, 0.068, 0.082, 0.8);
+    add_plate(m, bt, V{-0.01, 0, -0.05}, V{-0.004, 0, tl - 0.11}, 0.082, 0.03, 0.85);
+    m.add_visual(kVisCylinder, bt, V{0.065, 0, -tl + 0.08}, V{0.045, 0, 0.25 * tl}, 0.02, 0.0, kMatRibs, kCable);
+    m.add_visual(kVisCylinder, bt, V{0, 0, tl - 0.12}, V{0, 0, tl - 0.035}, 0.026, 0.0, kMatMetal, kSteel);
+    m.add_visual(kVisRing, bt, V{0, 0, tl - 0.09}, V{0, 0, 1}, 0.03, 0.01, kMatMetal, kDark);
+    m.add_visual(kVisSphere, bt, V{0, 0, tl}, V{0, 0, 0}, leaper::kFootR, 0.0, kMatRubber, kBlack);
+    m.add_visual(kVisRing, bt, V{0, 0, tl - 0.02}, V{0, 0, 1}, 0.036, 0.011, kMatMetal, kSteel);
+}
+
+// The torso's visuals (csrc/arc_robot.c:158-170): panelled hull, two collars,
+// a bottom hatch, two side knobs, and the eye (glow ring, bezel, lens, inner
+// glow ring). The renderer's eye light is the first glowing ring on body 0.
+static void add_torso_visuals(ModelHost& m)
+{
+    using V = V3<double>;
+    using namespace paint;
+    m.add_visual(kVisSphere, 0, V{0, 0, 0}, V{0, 0, 0}, leaper::kBodyR, 0.0, kMatPanels, kHull);
+    m.add_visual(kVisRing, 0, V{0, 0, 0.135}, V{0, 0, 1}, 0.148, 0.02, kMatMetal, kDark);
+    m.add_visual(kVisRing, 0, V{0, 0, -0.125}, V{0, 0, 1}, 0.156, 0.024, kMatPaint, kDark);
+    m.add_visual(kVisCylinder, 0, V{0, 0, -0.2}, V{0, 0, -0.17}, 0.07, 0.0, kMatMetal, kDark);
+    for (int side = -1; side <= 1; side += 2) {
+        V k = normalize(V{0.45, 0.62 * side, -0.64});
+        m.add_visual(kVisCylinder, 0, scale(k, 0.17), scale(k, 0.215), 0.028, 0.0, kMatMetal, kSteel);
+    }
+    m.add_visual(kVisRing, 0, V{0.18, 0, 0}, V{1, 0, 0}, 0.08, 0.013, kMatGlow, kGlow);
+    m.add_visual(kVisRing, 0, V{0.168, 0, 0}, V{1, 0, 0}, 0.112, 0.02, kMatMetal, kBezel);
+    m.add_visual(kVisCylinder, 0, V{0.11, 0, 0}, V{0.178, 0, 0}, 0.095, 0.0, kMatLens, kBlack);
+    m.add_visual(kVisRing, 0, V{0.181, 0, 0}, V{1, 0, 0}, 0.032, 0.006, kMatGlow, kDimGlow);
+}
+
 static void set_drive(ModelHost::Joint& jt, double lo, double hi)
 {
     jt.lo = lo;
@@ -121,8 +194,8 @@ static void set_drive(ModelHost::Joint& jt, double lo, double hi)
     jt.max_torque = leaper::kMaxTorque;
 }
 
-// csrc/arc_robot.c:88-159 (collision and dynamics only; the render-only
-// visuals are not part of the simulated model)
+// csrc/arc_robot.c:88-142: bodies, hinges, collision spheres, then the
+// render-only visuals
 static void build_leg(ModelHost& m, int leg, double sx, double sy)
 {
     using namespace leaper;
@@ -153,6 +226,7 @@ static void build_leg(ModelHost& m, int leg, double sx, double sy)
     m.add_sphere(bt, V3<double>{0.0, 0.0, -0.3 * tl}, 0.055);
     m.add_sphere(bt, V3<double>{0.0, 0.0, 0.4 * tl}, 0.035);
     m.foot_sphere[leg] = m.add_sphere(bt, V3<double>{0.0, 0.0, tl}, kFootR);
+    add_leg_visuals(m, bc, bf, bt, d, fl, tl);
 }
 
 void build_leaper(ModelHost& m)
@@ -164,6 +238,7 @@ void build_leaper(ModelHost& m)
     m.add_body(kBodyMass, inertia_sphere(kBodyMass, kBodyR), V3<double>{0, 0, 0}, q_identity<double>());
     m.add_sphere(0, V3<double>{0, 0, 0}, kBodyR);
     m.n_torso_spheres = m.ns;
+    add_torso_visuals(m);
     for (int leg = 0; leg < kNumLegs; ++leg)
         build_leg(m, leg, SX[leg], SY[leg]);
     m.total_mass = 0.0;

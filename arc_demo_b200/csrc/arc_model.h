@@ -8,7 +8,14 @@
 
 #include "arc_kernels.cuh"
 
+struct arc_sim;
+
 namespace arc {
+
+// render-only visuals: shapes and surface looks of csrc/arc_phys.h:69-87
+constexpr int kMaxVisuals = 80;
+enum VisualType { kVisSphere = 0, kVisBox, kVisTaper, kVisCylinder, kVisRing };
+enum Material { kMatPaint = 0, kMatPanels, kMatMetal, kMatRubber, kMatLens, kMatRibs, kMatGlow };
 
 struct ModelHost {
     int nb = 0, nj = 0, ns = 0;
@@ -30,6 +37,15 @@ struct ModelHost {
         V3<double> pos;
         double radius;
     } s[kMaxSpheres];
+    // render-only geometry in the body frame (csrc/arc_phys.h:69-98); the
+    // solver never reads it
+    struct Visual {
+        int type, body, material;
+        V3<double> p0, p1;
+        double radius, radius2, aspect;
+        float color[3];
+    } v[kMaxVisuals];
+    int nv = 0;
     int channel[kMaxSpheres] = {};
     int n_channels = 6;
     // robot info (csrc/arc_robot.h:22-30)
@@ -43,6 +59,9 @@ struct ModelHost {
     int add_body(double mass, V3<double> inertia, V3<double> pos, Q4<double> q);
     int add_sphere(int body, V3<double> pos, double radius);
     int add_hinge(int parent, int child, V3<double> anchor_world, V3<double> axis_world);
+    // aspect 1; returns the new index or -1 (csrc/arc_phys.c:145-164)
+    int add_visual(int type, int body, V3<double> p0, V3<double> p1, double radius, double radius2, int material,
+                   const float* rgb);
     // forward kinematics of every body from the root pose and joint angles
     void pose(V3<double> root_x, Q4<double> root_q, const double* angles, V3<double>* xs,
               Q4<double>* qs) const;
@@ -56,6 +75,17 @@ void build_leaper(ModelHost& m);
 // chain torso -> coxa -> femur -> tibia of leg k, spheres on the torso,
 // femurs and tibias only.
 bool is_leaper_topology(const ModelHost& m);
+
+// What the renderer reads of an arc_sim (arc_sim.cu owns the struct).
+struct SimView {
+    const ModelHost* model;
+    Worlds<float> wf;
+    Worlds<double> wd;
+    bool fp64;
+    int n;
+    cudaStream_t stream;
+};
+SimView sim_view(const arc_sim* s);
 
 template <class R> DevModel<R> make_dev_model(const ModelHost& m, double dt, int substeps, double action_scale);
 ResetModel make_reset_model(const ModelHost& m);

@@ -667,6 +667,20 @@ const arc_world* arc_sim_world(const arc_sim* s, int i)
         o.lim[2] = std::cos(t.hi);
         o.lim[3] = std::sin(t.hi);
     }
+    w->n_visuals = m.nv;
+    for (int k = 0; k < m.nv; ++k) {
+        const ModelHost::Visual& v = m.v[k];
+        arcw_visual& o = w->visuals[k];
+        o.type = v.type;
+        o.body = v.body;
+        o.p0 = arcw_vec3{v.p0.x, v.p0.y, v.p0.z};
+        o.p1 = arcw_vec3{v.p1.x, v.p1.y, v.p1.z};
+        o.radius = v.radius;
+        o.radius2 = v.radius2;
+        o.aspect = v.aspect;
+        o.material = v.material;
+        std::memcpy(o.color, v.color, sizeof(o.color));
+    }
     w->unstable = p[0] != 0.0;
     w->time = p[1];
     w->terrain.nx = nxy[0];
@@ -891,6 +905,19 @@ int arc_model_add_hinge(arc_model* m, int parent, int child, const double* ancho
         return -1;
     return m->m.add_hinge(parent, child, V3<double>{anchor[0], anchor[1], anchor[2]},
                           V3<double>{axis[0], axis[1], axis[2]});
+}
+
+int arc_model_add_visual(arc_model* m, int type, int body, const double* p0, const double* p1, double radius,
+                         double radius2, double aspect, int material, const float* rgb)
+{
+    if (!m || body < 0 || body >= m->m.nb || type < kVisSphere || type > kVisRing || material < kMatPaint ||
+        material > kMatGlow || !p0 || !p1 || !rgb)
+        return -1;
+    int i = m->m.add_visual(type, body, V3<double>{p0[0], p0[1], p0[2]}, V3<double>{p1[0], p1[1], p1[2]}, radius,
+                            radius2, material, rgb);
+    if (i >= 0)
+        m->m.v[i].aspect = aspect;
+    return i;
 }
 
 arc_sim* arc_sim_create_model(const arc_model* m, int n_worlds, double dt, int substeps, int grid, double cell,
@@ -1541,3 +1568,8 @@ int arc_env_set_targets(arc_sim* s, const int* ids, int n_ids, const double* xy)
 }
 
 }  // extern "C"
+
+SimView arc::sim_view(const arc_sim* s)
+{
+    return SimView{&s->model, view<float>(s), view<double>(s), s->fp64, s->n, s->stream};
+}

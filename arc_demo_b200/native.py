@@ -88,6 +88,8 @@ def sim_lib() -> ctypes.CDLL:
     d("arc_model_add_body", _int, _vp, _dbl, _f64, _f64, _f64)
     d("arc_model_add_sphere", _int, _vp, _int, _f64, _dbl)
     d("arc_model_add_hinge", _int, _vp, _int, _int, _f64, _f64)
+    d("arc_model_add_visual", _int, _vp, _int, _int, _f64, _f64, _dbl, _dbl, _dbl, _int,
+      np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS"))
     d("arc_sim_create_model", _vp, _vp, _int, _dbl, _int, _int, _dbl, _uint)
     d("arc_sim_set_pose", _int, _vp, _int, _f64, _f64, _vp)
     d("arc_sim_stream", _vp, _vp)
@@ -102,9 +104,12 @@ def sim_lib() -> ctypes.CDLL:
 
 
 def header_symbols() -> list[str]:
-    """Every function declared in include/arc_sim.h."""
-    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
-    return sorted(set(re.findall(r"\b(arc_\w+)\s*\(", text)))
+    """Every function declared in the library's headers (include/*.h)."""
+    names = set()
+    for h in sorted(HEADER.parent.glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names.update(re.findall(r"\b(arc_\w+)\s*\(", text))
+    return sorted(names)
 
 
 class Model:
@@ -122,6 +127,12 @@ class Model:
 
     def add_hinge(self, parent, child, anchor, axis) -> int:
         return self._lib.arc_model_add_hinge(self.ptr, parent, child, _vec(anchor), _vec(axis))
+
+    def add_visual(self, type, body, p0, p1, radius, radius2=0.0, aspect=1.0, material=0,
+                   color=(0.5, 0.5, 0.5)) -> int:
+        """A render-only shape on `body` (types and materials as in include/arc_sim.h)."""
+        return self._lib.arc_model_add_visual(self.ptr, type, body, _vec(p0), _vec(p1), radius, radius2,
+                                              aspect, material, np.asarray(color, dtype=np.float32))
 
     def close(self):
         if self.ptr:

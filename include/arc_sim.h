@@ -154,6 +154,12 @@ void arc_model_destroy(arc_model *m);
 int arc_model_add_body(arc_model *m, double mass, const double *inertia, const double *pos, const double *q);
 int arc_model_add_sphere(arc_model *m, int body, const double *local_pos, double radius);
 int arc_model_add_hinge(arc_model *m, int parent, int child, const double *anchor, const double *axis);
+/* A render-only visual in the body's frame (csrc/arc_phys.h:69-98): type
+ * 0 sphere, 1 box, 2 taper, 3 cylinder, 4 ring; material 0 paint, 1 panels,
+ * 2 metal, 3 rubber, 4 lens, 5 ribs, 6 glow; rgb in [0, 1]. Returns the
+ * index or -1. */
+int arc_model_add_visual(arc_model *m, int type, int body, const double *p0, const double *p1, double radius,
+                         double radius2, double aspect, int material, const float *rgb);
 arc_sim *arc_sim_create_model(const arc_model *m, int n_worlds, double dt, int substeps, int grid, double cell,
                               unsigned flags);
 /* Places body 0 at (pos, q) and the others by forward kinematics from the

@@ -441,3 +441,40 @@ class RefSim(_SimBase):
 
     def __del__(self):
         self.close()
+
+
+# ---- the renderer's restatement (render_oracle.c)
+
+VIEW_YAW = (0.5, 1.4, 2.6)  # camera presets behind, side, front (csrc/arc_render.c:962-968)
+
+
+def render_lib() -> ctypes.CDLL:
+    path = HERE / "liborender.so"
+    if not path.exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
+    lib = ctypes.CDLL(str(path))
+    fn = lib.oracle_render
+    fn.restype = _int
+    fn.argtypes = [ctypes.POINTER(World), _vp, _int, _int, _f64, _dbl, _dbl, _dbl, _int, _int, _int, _vp]
+    return lib
+
+
+class RenderOracle:
+    """One camera following a world, as the reference's renderer keeps one:
+    frame(world, markers, active) -> (H, W, 3) uint8."""
+
+    def __init__(self, width: int, height: int, samples: int = 4, view: int = 0, dist: float = 4.0):
+        self.lib = render_lib()
+        self.width, self.height, self.samples = width, height, samples
+        self.yaw, self.pitch, self.dist = VIEW_YAW[view % 3], 0.3, dist
+        self.cam = np.zeros(5)
+
+    def frame(self, world: World, markers=None, active: int = -1) -> np.ndarray:
+        img = np.zeros((self.height, self.width, 3), dtype=np.uint8)
+        m_ptr, n = None, 0
+        if markers is not None and len(markers):
+            markers = np.ascontiguousarray(markers, dtype=np.float64).reshape(-1, 4)
+            m_ptr, n = markers.ctypes.data, len(markers)
+        self.lib.oracle_render(ctypes.byref(world), m_ptr, n, active, self.cam, self.yaw, self.pitch, self.dist,
+                               self.width, self.height, self.samples, img.ctypes.data)
+        return img

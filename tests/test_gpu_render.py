@@ -1,0 +1,155 @@
+"""The GPU renderer (csrc/arc_render.cu) against its CPU restatement
+(oracle/render_oracle.c), through the reference's renderer ABI.
+
+Tolerance. The two differ only in arithmetic: FP32 rays and shading on the
+GPU, FP64 in the oracle (both evaluate the shader's sin-based hash in
+float with the same rounding order). A sample whose ray passes within
+rounding of a silhouette or a column edge can land on different surfaces,
+and a channel within rounding of a half level can round either way. So a
+frame matches when its mean absolute difference is at most 0.1 levels and
+at most 0.3% of its channels differ by more than 2 levels (of 255).
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from arc_demo_b200.native import Sim
+from arc_demo_b200.render import Renderer
+from oracle.oracle import RefSim, RenderOracle, World
+
+pytestmark = pytest.mark.gpu
+
+W, H = 128, 72
+
+
+def world_of(sim: Sim, i: int) -> World:
+    lib = sim._lib
+    lib.arc_sim_world.restype = ctypes.POINTER(World)
+    lib.arc_sim_world.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    return lib.arc_sim_world(sim.ptr, i).contents
+
+
+def assert_frames_match(gpu: np.ndarray, ref: np.ndarray, what: str = ""):
+    assert gpu.shape == ref.shape and gpu.dtype == np.uint8
+    d = np.abs(gpu.astype(np.int32) - ref.astype(np.int32))
+    assert d.mean() <= 0.1, f"{what}: mean abs difference {d.mean():.3f}"
+    assert (d > 2).mean() <= 0.003, f"{what}: {(d > 2).mean():.4%} of channels differ by more than 2"
+    # the picture is not trivially empty: terrain and robot are lit
+    assert ref.mean() > 20.0
+
+
+def make_sim(n=4, grid=32, fp64=False):
+    sim = Sim(n, grid=grid, fp64=fp64)
+    seeds = np.arange(11, 11 + n, dtype=np.uint32)
+    sim.reset(np.arange(n), seeds, np.linspace(0.0, 1.0, n))
+    return sim
+
+
+def test_visuals_match_the_reference_robot():
+    sim = make_sim(1)
+    ref = RefSim(1)
+    a, b = world_of(sim, 0), ref.world(0)
+    assert a.n_visuals == b.n_visuals == 74
+    for i in range(a.n_visuals):
+        va, vb = a.visuals[i], b.visuals[i]
+        assert (va.type, va.body, va.material) == (vb.type, vb.body, vb.material), i
+        for f in ("p0", "p1"):
+            pa, pb = getattr(va, f), getattr(vb, f)
+            assert np.allclose([pa.x, pa.y, pa.z], [pb.x, pb.y, pb.z], rtol=0, atol=1e-12), (i, f)
+        assert np.allclose([va.radius, va.radius2, va.aspect], [vb.radius, vb.radius2, vb.aspect], rtol=0, atol=1e-12)
+        assert list(va.color) == list(vb.color), i
+
+
+@pytest.mark.parametrize("samples", [1, 4])
+@pytest.mark.parametrize("world", [0, 1, 2, 3])
+def test_frame_matches_oracle(samples, world):
+    sim = make_sim()
+    markers = np.array([[1.5, -1.0, 0.0, 0.5]])
+    active = 0 if world % 2 else -1
+    r = Renderer(W, H, visible=False)
+    r.set_samples(samples)
+    gpu = r.frame(sim, world, markers, active, rgb=True)
+    ref = RenderOracle(W, H, samples=samples).frame(world_of(sim, world), markers, active)
+    assert_frames_match(gpu, ref, f"world {world}, {samples} samples")
+
+
+@pytest.mark.parametrize("view", [1, 2, 5])
+def test_view_presets_match_oracle(view):
+    sim = make_sim()
+    r = Renderer(W, H, visible=False)
+    r.set_view(view)
+    r.set_samples(1)
+    gpu = r.frame(sim, 2, None, -1, rgb=True)
+    ref = RenderOracle(W, H, samples=1, view=view).frame(world_of(sim, 2))
+    assert_frames_match(gpu, ref, f"view {view}")
+
+
+def test_camera_follows_a_moving_robot():
+    """The camera's smoothing state carries from frame to frame as the
+    reference's does: five steps of random drive targets, one frame each."""
+    sim = make_sim(2)
+    rng = np.random.default_rng(5)
+    r = Renderer(W, H, visible=False)
+    r.set_samples(1)
+    ora = RenderOracle(W, H, samples=1)
+    markers = np.array([[3.0, 2.0, 0.2, 0.5], [-2.0, 1.0, 0.0, 0.4]])
+    for k in range(5):
+        targets = np.tile(sim.default_angles, (2, 1)) + rng.uniform(-0.6, 0.6, (2, 12))
+        for _ in range(3):
+            sim.step(targets)
+        gpu = r.frame(sim, 1, markers, k % 2, rgb=True)
+        ref = ora.frame(world_of(sim, 1), markers, k % 2)
+        assert_frames_match(gpu, ref, f"frame {k}")
+
+
+def test_fallen_robot_and_fp64_worlds():
+    """An upside-down robot on rough terrain, in an FP64 simulation."""
+    sim = make_sim(2, fp64=True)
+    s = np.sqrt(0.5)
+    sim.set_pose(1, (0.3, -0.2, 0.6), (0.0, s, s, 0.0), sim.default_angles)
+    r = Renderer(W, H, visible=False)
+    gpu = r.frame(sim, 1, None, -1, rgb=True)
+    ref = RenderOracle(W, H, samples=4).frame(world_of(sim, 1))
+    assert_frames_match(gpu, ref, "fallen")
+
+
+def test_batched_frames_equal_single_frames():
+    """arc_render_frames with fresh cameras gives, for each world, the bytes
+    arc_render_frame gives on a fresh renderer."""
+    import torch
+
+    sim = make_sim(5)
+    ids = torch.tensor([4, 0, 2], dtype=torch.int32, device="cuda")
+    markers = torch.tensor([[[1.0, 1.0, 0.0, 0.5]], [[-1.0, 2.0, 0.1, 0.3]], [[0.0, -2.0, 0.0, 0.6]]],
+                           dtype=torch.float32, device="cuda")
+    active = torch.tensor([0, -1, 0], dtype=torch.int32, device="cuda")
+    r = Renderer(W, H, visible=False)
+    batch = r.frames(sim, ids, markers, active).cpu().numpy()
+    for k, w in enumerate(ids.tolist()):
+        one = Renderer(W, H, visible=False)
+        img = one.frame(sim, w, markers[k].cpu().numpy().astype(np.float64), int(active[k]), rgb=True)
+        assert np.array_equal(batch[k], img), k
+
+
+def test_errors_are_reported_not_faults():
+    import torch
+
+    sim = make_sim(2)
+    with pytest.raises(RuntimeError):
+        Renderer(W, H, visible=True)
+    r = Renderer(W, H, visible=False)
+    with pytest.raises(ValueError):
+        r.set_samples(3)
+    from arc_demo_b200.native import ArcSimError
+    with pytest.raises(ArcSimError):
+        r.frame(sim, 7, None, -1, rgb=True)
+    lib = r._lib
+    out = torch.empty((2, H, W, 3), dtype=torch.uint8, device="cuda")
+    m = torch.zeros((2, 5, 4), dtype=torch.float32, device="cuda")
+    assert lib.arc_render_frames(r._ptr, sim.ptr, None, 2, m.data_ptr(), 5, None, out.data_ptr(), None) < 0
+    assert lib.arc_render_frames(r._ptr, sim.ptr, None, 3, None, 0, None, out.data_ptr(), None) < 0
+    assert r.keys() == []
+    # and it still renders
+    assert r.frame(sim, 1, None, -1, rgb=True).mean() > 20.0
