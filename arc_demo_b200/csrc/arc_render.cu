@@ -23,12 +23,14 @@
 // Departures from the rasteriser, all in fine detail: shapes are exact
 // (spheres, capped cylinders, chamfered prisms) or sphere traced (rounded
 // boxes, tori) where the reference tessellates them; the key light's shadow
-// is one ray toward the sun per sample where the reference filters four
-// taps of a 2048^2 shadow map; the four samples of a pixel are shaded one
-// by one where multisampling shades once per pixel and primitive; the
-// screen-space derivatives of the shader (fwidth) come from ray
-// differentials; the terrain's top quads are split along the diagonal from
-// their (-x, -y) corner for the interpolation of the vertex colours.
+// is one ray toward the sun where the reference filters four taps of a
+// 2048^2 shadow map; like multisampling, a pixel is shaded once per surface
+// its samples hit, but at the first such sample's hit point rather than at
+// the pixel centre, and a surface is a whole visual or column face rather
+// than one triangle of it; the screen-space derivatives of the shader
+// (fwidth) come from ray differentials; the terrain's top quads are split
+// along the diagonal from their (-x, -y) corner for the interpolation of
+// the vertex colours.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -37,6 +39,12 @@
 
 #include "arc_model.h"
 #include "../../include/arc_render.h"
+
+// CTAs of k_render resident per SM: 2 keeps its registers within 128
+// without spills
+#ifndef ARC_RENDER_MIN_BLOCKS
+#define ARC_RENDER_MIN_BLOCKS 2
+#endif
 
 namespace arc {
 namespace rd {
@@ -108,6 +116,7 @@ struct FrameK {
     float rot[kPoses][9];  // row major: world = rot * local + pos
     int nx, ny, n_items, n_glow;
     float cell, ox, oy, outside;
+    float body_c[kPoses][3], body_r[kPoses];  // world bounding sphere of each body's shadow casters
     VisK extra[2 * kMaxMarkers];  // marker beacons and rings, world frame
     GlowK glow[kMaxGlow];
 };
@@ -225,10 +234,11 @@ __device__ float trace_terrain(const TerrainF<R>& T, F3 o, F3 D, float tmax, int
     int iy = min(max((int)floorf((py - T.oy) / T.cell), 0), T.ny - 1);
     const int sx = D.x > 0.0f ? 1 : -1, sy = D.y > 0.0f ? 1 : -1;
     const float big = 1e30f;
-    const float tdx = fabsf(D.x) > 1e-12f ? T.cell / fabsf(D.x) : big;
-    const float tdy = fabsf(D.y) > 1e-12f ? T.cell / fabsf(D.y) : big;
-    float tx = fabsf(D.x) > 1e-12f ? (T.ox + (ix + (sx > 0)) * T.cell - o.x) / D.x : big;
-    float ty = fabsf(D.y) > 1e-12f ? (T.oy + (iy + (sy > 0)) * T.cell - o.y) / D.y : big;
+    const bool mx = fabsf(D.x) > 1e-12f, my = fabsf(D.y) > 1e-12f;
+    const float inx = mx ? 1.0f / D.x : 0.0f, iny = my ? 1.0f / D.y : 0.0f;
+    const float tdx = mx ? T.cell * fabsf(inx) : big, tdy = my ? T.cell * fabsf(iny) : big;
+    float tx = mx ? (T.ox + (ix + (sx > 0)) * T.cell - o.x) * inx : big;
+    float ty = my ? (T.oy + (iy + (sy > 0)) * T.cell - o.y) * iny : big;
     float t_in = t0;
     int f_in = entry == 0 ? kFaceX : (entry == 1 ? kFaceY : kFaceTop);
     int s_in = entry == 0 ? sx : sy;
@@ -487,10 +497,18 @@ __device__ bool shadowed(const FrameK& fr, const TerrainF<R>& T, const VisK* __r
     float bb = dot(oc, L), cc = dot(oc, oc) - fr.robot_r * fr.robot_r;
     if (bb * bb - cc < 0.0f || (bb > 0.0f && cc > 0.0f))
         return false;
+    // bodies whose casters' bounding sphere the ray meets
+    unsigned bodies = 0u;
+    for (int b = 0; b < kMaxBodies; ++b) {
+        F3 q = p - ld3(fr.body_c[b]);
+        float qb = dot(q, L), qc = dot(q, q) - fr.body_r[b] * fr.body_r[b];
+        if (fr.body_r[b] > 0.0f && qb * qb - qc >= 0.0f && !(qb > 0.0f && qc > 0.0f))
+            bodies |= 1u << b;
+    }
     int last_body = -1;
     F3 ol{0, 0, 0}, dl{0, 0, 0};
     for (int i = 0; i < nv; ++i) {
-        if (vis[i].glow || vis[i].type < 0)
+        if (vis[i].glow || vis[i].type < 0 || !((bodies >> vis[i].body) & 1u))
             continue;
         const int body = vis[i].body;
         // bounding sphere in the world
@@ -620,12 +638,13 @@ __device__ __forceinline__ int unorm8(float x) { return (int)floorf(clampf(x, 0.
 
 // Additive glow along the ray up to depth tdepth (csrc/arc_render.c:280-302,
 // 625-672): halos around glowing parts and beacons, and the beacons' beams.
-__device__ F3 glow_along(const FrameK& fr, F3 O, F3 D, float tdepth)
+// `mask`: the billboards that can cover the tile.
+__device__ F3 glow_along(const FrameK& fr, unsigned mask, F3 O, F3 D, float tdepth)
 {
     F3 g{0.0f, 0.0f, 0.0f};
     const F3 fwd = ld3(fr.fwd), right = ld3(fr.right), up = ld3(fr.up), eye = ld3(fr.eye);
-    for (int i = 0; i < fr.n_glow; ++i) {
-        const GlowK& k = fr.glow[i];
+    for (; mask; mask &= mask - 1u) {
+        const GlowK& k = fr.glow[__ffs(mask) - 1];
         const F3 c = ld3(k.c);
         float t, u, vv, w;
         if (!k.beam) {
@@ -668,7 +687,7 @@ __device__ F3 glow_along(const FrameK& fr, F3 O, F3 D, float tdepth)
 
 // One CTA per 32 x 8 tile of one world's frame (blockIdx.y: the world).
 template <class R>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, ARC_RENDER_MIN_BLOCKS)
     k_render(const VisK* __restrict__ vis, int nv, const FrameK* __restrict__ frames, Worlds<R> W,
              const int* __restrict__ ids, int width, int height, int tiles_x, int samples,
              unsigned char* __restrict__ out)
@@ -676,6 +695,7 @@ __global__ void __launch_bounds__(kThreads)
     __shared__ FrameK fr;
     __shared__ unsigned char list[kMaxItems];
     __shared__ int warp_n[kThreads / 32];
+    __shared__ unsigned glow_mask;
     const int tid = threadIdx.x, item = blockIdx.y;
     {
         const int* src = reinterpret_cast<const int*>(frames + item);
@@ -726,6 +746,25 @@ __global__ void __launch_bounds__(kThreads)
             base += warp_n[w];
         if (keep)
             list[base + __popc(m & ((1u << (tid & 31)) - 1u))] = (unsigned char)tid;
+        // the glow billboards' bounding spheres: a halo's square, a beam's quad
+        if (tid < 32) {
+            bool g = false;
+            if (tid < fr.n_glow) {
+                const GlowK& k = fr.glow[tid];
+                F3 c = ld3(k.c) - eye;
+                float rad = 1.4143f * k.s;
+                if (k.beam) {
+                    c.z += 1.75f;
+                    rad = sqrtf(1.75f * 1.75f + k.s * k.s);
+                }
+                g = true;
+                for (int q = 0; q < 4; ++q)
+                    g = g && dot(pn[q], c) <= rad;
+            }
+            const unsigned gm = __ballot_sync(0xffffffffu, g);
+            if (tid == 0)
+                glow_mask = gm;
+        }
     }
     __syncthreads();
     int n_list = 0;
@@ -755,6 +794,9 @@ __global__ void __launch_bounds__(kThreads)
     const float dither = (hash2(fmaf(fr.time, 61.0f, px + 0.5f), fmaf(fr.time, 61.0f, wy_pix + 0.5f)) - 0.5f) / 255.0f;
     const F3 dDx = scale(right, sx), dDy = scale(up, sy);
     int acc[3] = {0, 0, 0};
+    // the surfaces this pixel's samples hit so far and their colours
+    int gid0 = -1, gid1 = -1, gid2 = -1, gid3 = -1;
+    unsigned gc0 = 0u, gc1 = 0u, gc2 = 0u, gc3 = 0u;
     for (int si = 0; si < samples; ++si) {
         const float wx = samples == 1 ? px + 0.5f : px + spos[si][0];
         const float wy = samples == 1 ? wy_pix + 0.5f : wy_pix + spos[si][1];
@@ -779,6 +821,13 @@ __global__ void __launch_bounds__(kThreads)
                 ol = rot_tmul(fr.rot[v.body], eye - ld3(fr.pos[v.body]));
                 dl = rot_tmul(fr.rot[v.body], D);
             }
+            {
+                // the ray against the visual's bounding sphere first
+                const F3 oc = ol - ld3(v.bc);
+                const float b = dot(oc, dl), c = dot(oc, oc) - v.br * v.br;
+                if (b * b < c || (b > 0.0f && c > 0.0f))
+                    continue;
+            }
             float t;
             F3 n;
             if (hit_visual(v, ol, dl, best, t, n)) {
@@ -788,8 +837,29 @@ __global__ void __launch_bounds__(kThreads)
                 nl = n;
             }
         }
-        int s8[3] = {0, 0, 0};
-        if (kind >= 0) {
+        // Multisampling shades once per pixel and primitive: a sample that
+        // hits the surface an earlier sample of this pixel hit (the same
+        // visual, or the same face of the same column) takes its colour.
+        int sid = -1;
+        if (kind == 0)
+            sid = 1024 + ((cy * kGridMax + cx) << 3) + (face == kFaceTop ? 0 : (face == kFaceX ? 2 : 4) + (sgn > 0));
+        else if (kind == 1)
+            sid = hit_item;
+        unsigned packed = 0u;
+        bool fresh = false;
+        if (sid >= 0) {
+            if (sid == gid0)
+                packed = gc0;
+            else if (sid == gid1)
+                packed = gc1;
+            else if (sid == gid2)
+                packed = gc2;
+            else if (sid == gid3)
+                packed = gc3;
+            else
+                fresh = true;
+        }
+        if (fresh) {
             Surface s;
             s.p = eye + scale(D, best);
             s.pat = 0;
@@ -890,12 +960,25 @@ __global__ void __launch_bounds__(kThreads)
                 lit_k = mixf(1.0f, k, fade);
             }
             const F3 c = shade_scene(fr, s, lit_k);
-            s8[0] = unorm8(c.x + dither);
-            s8[1] = unorm8(c.y + dither);
-            s8[2] = unorm8(c.z + dither);
+            packed = (unsigned)unorm8(c.x + dither) | (unsigned)unorm8(c.y + dither) << 8 |
+                     (unsigned)unorm8(c.z + dither) << 16;
+            if (gid0 < 0) {
+                gid0 = sid;
+                gc0 = packed;
+            } else if (gid1 < 0) {
+                gid1 = sid;
+                gc1 = packed;
+            } else if (gid2 < 0) {
+                gid2 = sid;
+                gc2 = packed;
+            } else {
+                gid3 = sid;
+                gc3 = packed;
+            }
         }
+        const int s8[3] = {(int)(packed & 255u), (int)((packed >> 8) & 255u), (int)(packed >> 16)};
         // additive glow (depth tested, not written), then the vignette
-        const F3 g = glow_along(fr, eye, D, kind >= 0 ? best : 1e30f);
+        const F3 g = glow_along(fr, glow_mask, eye, D, kind >= 0 ? best : 1e30f);
         const float gg[3] = {g.x, g.y, g.z};
         for (int k = 0; k < 3; ++k) {
             int v8 = unorm8(s8[k] / 255.0f + gg[k]);
@@ -1073,8 +1156,9 @@ __global__ void k_frame_setup(Worlds<R> W, const VisK* __restrict__ vis, int nv,
         put3(f.beacon_pos, mk[0], mk[1], (double)mk[2] + kBeaconHeight);
         put3(f.beacon_col, k * c[0], k * c[1], k * c[2]);
     }
-    // robot bounding sphere of the shadow casters, glow billboards of the robot
-    double rr = 0.0;
+    // bounding spheres of the shadow casters: the robot's, and each body's
+    // (centred on the body), then the robot's glow billboards
+    double rr = 0.0, br[kPoses] = {};
     int ng = 0;
     for (int i = 0; i < nv; ++i) {
         const VisK& v = vis[i];
@@ -1084,6 +1168,7 @@ __global__ void k_frame_setup(Worlds<R> W, const VisK* __restrict__ vis, int nv,
             bx[v.body] + qrotate(bq[v.body], V3<double>{v.bc[0], v.bc[1], v.bc[2]});
         if (!v.glow) {
             rr = fmax(rr, len(cw - bx[0]) + v.br);
+            br[v.body] = fmax(br[v.body], len(cw - bx[v.body]) + v.br);
             continue;
         }
         if (ng >= kMaxGlow)
@@ -1105,6 +1190,11 @@ __global__ void k_frame_setup(Worlds<R> W, const VisK* __restrict__ vis, int nv,
         put3(g.col, v.col[0], v.col[1], v.col[2]);
         g.alpha = v.type == kVisRing ? 0.4f : 0.3f;
         g.beam = 0;
+    }
+    for (int b = 0; b < kPoses; ++b) {
+        const bool has = b < nb && b < kMaxBodies && br[b] > 0.0;
+        put3(f.body_c[b], has ? bx[b].x : 0.0, has ? bx[b].y : 0.0, has ? bx[b].z : 0.0);
+        f.body_r[b] = has ? (float)br[b] + 1e-3f : 0.0f;
     }
     f.robot_c[0] = (float)bx[0].x;
     f.robot_c[1] = (float)bx[0].y;

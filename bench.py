@@ -48,6 +48,12 @@ HBM_BYTES_PER_ENV_STEP = 3.9e3  # algorithmic HBM traffic of one env-step (state
 # reads its own record and terrain cells, so the traffic scales with them.
 WARPS_DRAM_BYTES_PER_WORLD = (42.240e6 + 0.175e6) / 16384
 
+# the renderer's workload: frames of the reference's rgb_array size
+# (arc/env.py:43), 4 rays per pixel, for a batch of worlds per launch
+RENDER_METRIC = "frames/s at 640x360, 4 samples per pixel"
+RENDER_WORLDS = 256
+RENDER_W, RENDER_H, RENDER_SAMPLES = 640, 360, 4
+
 
 def parse():
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
@@ -62,6 +68,9 @@ def parse():
     p.add_argument("--wpc", type=int, default=0, help="worlds per CTA (0: autotune)")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--kernel", choices=["auto", "warps"], default="auto")
+    p.add_argument("--workload", choices=["step", "render"], default="step",
+                   help="step: the world step (the headline); render: frames of the headless renderer")
+    p.add_argument("--render-worlds", type=int, default=RENDER_WORLDS)
     return p.parse_args()
 
 
@@ -497,8 +506,149 @@ def run_reference(args) -> dict | None:
                     "d2h_bytes_per_step": 0}}
 
 
+# ---------------------------------------------------------------------------
+# the renderer
+
+def render_scene(n: int, seed: int):
+    """n worlds of the step workload's terrain mix, each robot a few steps
+    into random drive targets, one checkpoint marker per world drawn as the
+    task draws them, half of them in view."""
+    from arc_demo_b200.native import Sim
+    rng = np.random.default_rng(seed)
+    sim = Sim(n)
+    sim.reset(np.arange(n), rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32), levels_for(n, seed))
+    targets = np.tile(sim.default_angles, (n, 1)) + rng.uniform(-0.5, 0.5, (n, 12))
+    for _ in range(10):
+        sim.step(targets)
+    half = 0.5 * sim.grid * sim.cell - 1.0
+    markers = np.zeros((n, 1, 4), dtype=np.float32)
+    markers[:, 0, :2] = rng.uniform(-half, half, (n, 2))
+    markers[:, 0, 3] = 0.5
+    active = np.where(rng.random(n) < 0.5, 0, -1).astype(np.int32)
+    return sim, markers, active
+
+
+def render_cpu_baseline(sim, markers, active) -> dict:
+    """The renderer's CPU restatement (brute force, one core) on one
+    160 x 90 frame with one sample, scaled to a 640 x 360 frame of 4 samples
+    by the number of rays."""
+    from oracle.oracle import RenderOracle
+    lib = sim._lib
+    from oracle.oracle import World
+    lib.arc_sim_world.restype = ctypes.POINTER(World)
+    lib.arc_sim_world.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    w = lib.arc_sim_world(sim.ptr, 0).contents
+    ora = RenderOracle(160, 90, samples=1)
+    t = time.perf_counter()
+    ora.frame(w, markers[0].astype(np.float64), int(active[0]))
+    el = time.perf_counter() - t
+    scale = (RENDER_W * RENDER_H * RENDER_SAMPLES) / (160 * 90)
+    return {"value": round(1.0 / (el * scale), 4), "unit": "frames/s", "cores": 1, "kind": "port",
+            "sample": f"one 160x90 frame with 1 sample in {el:.2f} s, scaled by rays to 640x360 with 4 samples "
+                      "(oracle/render_oracle.c: every column and visual tested against every ray)"}
+
+
+def run_render(args) -> dict | None:
+    """Frames/s of the batched renderer: `value` device-resident (one launch
+    renders every world's frame into HBM); `e2e` through the reference's
+    arc_render_frame, one world per call into a host buffer."""
+    import torch
+    from arc_demo_b200.render import Renderer
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    n = args.render_worlds
+    sim, markers, active = render_scene(n, 77 + rank)
+    stream = torch.cuda.Stream()
+    r = Renderer(RENDER_W, RENDER_H, visible=False)
+    r.set_samples(RENDER_SAMPLES)
+    d_markers = torch.from_numpy(markers).cuda()
+    d_active = torch.from_numpy(active).cuda()
+    out = torch.empty((n, RENDER_H, RENDER_W, 3), dtype=torch.uint8, device="cuda")
+    h = stream.cuda_stream
+    for _ in range(max(args.warmup, 3)):
+        r.frames(sim, None, d_markers, d_active, out=out, stream=h)
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    K = args.steps
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(K):
+            r.frames(sim, None, d_markers, d_active, out=out, stream=h)
+        t1.record(stream)
+        t1.synchronize()
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms_total = max_over_ranks(torch, dist, t0.elapsed_time(t1))
+    clock = clocks.summary()
+    # e2e: the reference's call, one world per call, frame copied to the host
+    m = min(n, 64)
+    img = np.empty((RENDER_H, RENDER_W, 3), dtype=np.uint8)
+    one = Renderer(RENDER_W, RENDER_H, visible=False)
+    for i in range(2):
+        one.frame(sim, i, markers[i].astype(np.float64), int(active[i]), rgb=True)
+    t = time.perf_counter()
+    for i in range(m):
+        one._lib.arc_render_frame(one._ptr, sim.ptr, i, markers[i].astype(np.float64).ctypes.data, 1,
+                                  int(active[i]), img.ctypes.data)
+    e2e_s = max_over_ranks(torch, dist, time.perf_counter() - t)
+    peak = ctypes.c_double(0.0)
+    from arc_demo_b200.native import sim_lib
+    sim_lib().arc_probe_fp32_peak(ctypes.byref(peak), None)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    value = world * n * K / (ms_total * 1e-3)
+    rays = RENDER_W * RENDER_H * RENDER_SAMPLES
+    res = {
+        "metric": RENDER_METRIC, "value": round(value, 1), "unit": "frames/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": round(ms_total / K, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{n} worlds per GPU rendered per step at {RENDER_W}x{RENDER_H}, "
+                               f"{RENDER_SAMPLES} rays per pixel, terrain difficulty uniform in {{0,...,1.0}}, "
+                               "one checkpoint marker per world",
+                   "frames_per_launch": n, "l2": f"output {n * rays // RENDER_SAMPLES * 3 / 1e6:.0f} MB per step, "
+                                                  "larger than L2"},
+        "primary_rays_per_s": round(value * rays, 1),
+        "roofline": {"bound": "fp32 issue", "kernel": "k_render",
+                     "note": "no dense contraction and little memory traffic: the ray casting and shading are "
+                             "issue bound; the issue fraction comes from ncu (profiles/render_640x360.md)",
+                     "peak_fp32_tflops": round(peak.value / 1e12, 3)},
+        "gpu_launches": 2 * K,
+        "clocks": clock,
+        "e2e": {"value": round(m / e2e_s, 1), "unit": "frames/s", "h2d_bytes_per_step": 4 * 4 + 8,
+                "d2h_bytes_per_step": RENDER_W * RENDER_H * 3,
+                "path": "arc_render_frame (the reference's ABI), one world per call into a host buffer"},
+    }
+    if world == 1 and not args.no_cpu:
+        res["cpu_baseline"] = render_cpu_baseline(sim, markers, active)
+    return res
+
+
 def main():
     args = parse()
+    if args.workload == "render":
+        if args.impl == "reference":
+            if int(os.environ.get("RANK", "0")) == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference renders with SDL2 and "
+                                  "OpenGL 2.1 (csrc/arc_render.c); unavailable on this box"}), flush=True)
+            return
+        out = run_render(args)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
     out = run_reference(args) if args.impl == "reference" else run_ours(args)
     if out is not None:
         print(json.dumps(out), flush=True)

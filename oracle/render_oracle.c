@@ -10,8 +10,8 @@
  * cannot run on these machines. This file restates the same scene in double
  * precision from those sources, with the ray-casting model the GPU renderer
  * documents (exact or sphere-traced shapes instead of meshes, a shadow ray
- * instead of the shadow map, per-sample shading of the 4x multisample
- * pattern, ray-differential derivatives), written independently of the
+ * instead of the shadow map, the 4x multisample pattern shaded once per
+ * pixel and surface, ray-differential derivatives), written independently of the
  * CUDA code and by brute force:
  *   - every terrain column is a box from the void's bottom to its top,
  *     tested against every ray (the GPU walks a 2D DDA over the cells);
@@ -640,6 +640,10 @@ int oracle_render(const arc_world *w, const double *markers, int n_markers, int 
                 (hash_f(fmaf(S.time_frac, 61.0f, (float)px + 0.5f), fmaf(S.time_frac, 61.0f, (float)wyp + 0.5f)) -
                  0.5) / 255.0;
             int acc[3] = {0, 0, 0};
+            /* shaded once per pixel and surface (a visual, or one face of a
+             * column): later samples on the same surface reuse the colour */
+            long gid[4] = {-1, -1, -1, -1};
+            int gcol[4][3], ngroups = 0;
             for (int si = 0; si < samples; ++si) {
                 double wx = samples == 1 ? px + 0.5 : px + SP[si][0];
                 double wy = samples == 1 ? wyp + 0.5 : wyp + SP[si][1];
@@ -665,7 +669,20 @@ int oracle_render(const arc_world *w, const double *markers, int n_markers, int 
                     }
                 }
                 int s8[3] = {0, 0, 0};
-                if (kind >= 0) {
+                long sid = -1;
+                if (kind == 0)
+                    sid = 1000000L + (long)(cy * 64 + cx) * 8 +
+                          (n.z > 0.5 ? 0 : (n.x < -0.5 ? 1 : (n.x > 0.5 ? 2 : (n.y < -0.5 ? 3 : 4))));
+                else if (kind == 1)
+                    sid = hit;
+                int reuse = -1;
+                for (int q = 0; q < ngroups; ++q)
+                    if (gid[q] == sid)
+                        reuse = q;
+                if (reuse >= 0) {
+                    for (int k = 0; k < 3; ++k)
+                        s8[k] = gcol[reuse][k];
+                } else if (kind >= 0) {
                     v3 p = add(eye, mul(d, best));
                     v3 alb;
                     double spec, gloss, emis, rim = 0.0, w_t = 0.0, wl = 0.0, wn = 0.0;
@@ -814,6 +831,12 @@ int oracle_render(const arc_world *w, const double *markers, int n_markers, int 
                         double x = cc[k];
                         x = x * (2.51 * x + 0.03) / (x * (2.43 * x + 0.59) + 0.14);
                         s8[k] = to8(pow(clampd(x, 0, 1), 1.0 / 2.2) + dither);
+                    }
+                    if (ngroups < 4) {
+                        gid[ngroups] = sid;
+                        for (int k = 0; k < 3; ++k)
+                            gcol[ngroups][k] = s8[k];
+                        ngroups++;
                     }
                 }
                 /* glow, depth tested against the scene */
