@@ -7,7 +7,7 @@
 // glow billboards, a vignette and 4x multisampling. Here the same scene is
 // ray cast, any number of worlds per launch:
 //
-//   k_frame_setup  one thread per rendered world: the camera (the
+//   k_frame_setup  one warp per rendered world: the camera (the
 //                  reference's smoothed orbit behind the robot, one state
 //                  per world), the lights, the world pose of every body,
 //                  the markers and glow billboards, the terrain's lowest
@@ -154,12 +154,14 @@ __device__ __forceinline__ F3 rot_tmul(const float* m, F3 v)
 
 // The shader's value noise (csrc/arc_render.c:151-158). The hash of a
 // lattice point is evaluated with one rounding order (an explicit fma), so
-// that CPU restatements can reproduce it.
+// that CPU restatements can reproduce it. noise2, hit_visual and
+// trace_terrain stay out of line: the kernel's code is far larger than the
+// instruction cache, and one copy of each is faster than inlined copies.
 __device__ __forceinline__ float hash2(float x, float y)
 {
     return fractf(__fmul_rn(sinf(fmaf(x, 127.1f, y * 311.7f)), 43758.5453f));
 }
-__device__ float noise2(float x, float y)
+__device__ __noinline__ float noise2(float x, float y)
 {
     float ix = floorf(x), iy = floorf(y);
     float fx = x - ix, fy = y - iy;
@@ -198,7 +200,7 @@ enum Face { kFaceTop = 0, kFaceX = 1, kFaceY = 2 };
 // neighbour is lower, down to the void's bottom). A 2D DDA over the cells
 // the ray crosses inside the grid's box. Returns t or -1.
 template <class R>
-__device__ float trace_terrain(const TerrainF<R>& T, F3 o, F3 D, float tmax, int& face, int& cx, int& cy, int& sgn)
+__device__ __noinline__ float trace_terrain(const TerrainF<R>& T, F3 o, F3 D, float tmax, int& face, int& cx, int& cy, int& sgn)
 {
     if (T.nx <= 0 || T.ny <= 0)
         return -1.0f;
@@ -321,7 +323,7 @@ __device__ __forceinline__ float sdf_ring(F3 w, F3 d, float major, float tube)
 constexpr int kMarch = 48;
 constexpr float kMarchEps = 2e-5f;
 
-__device__ bool hit_visual(const VisK& v, F3 o, F3 D, float tmax, float& t, F3& n)
+__device__ __noinline__ bool hit_visual(const VisK& v, F3 o, F3 D, float tmax, float& t, F3& n)
 {
     const F3 c = ld3(v.o), d = ld3(v.d);
     switch (v.type) {
@@ -1014,17 +1016,64 @@ __device__ __forceinline__ void put3(float* d, double x, double y, double z)
     d[2] = (float)z;
 }
 
-// One thread per rendered world: camera, lights, poses, markers, glow.
-template <class R>
-__global__ void k_frame_setup(Worlds<R> W, const VisK* __restrict__ vis, int nv, int eye_vis, const int* __restrict__ ids,
-                              int n, const float* __restrict__ markers, int mpw, const int* __restrict__ active,
-                              CamState* __restrict__ cams, int cam_slot, CamParams cp, FrameK* __restrict__ frames)
+__device__ __forceinline__ double warp_min(double v)
 {
-    const int item = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int o = 16; o > 0; o >>= 1)
+        v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+constexpr int kSetupWarps = 2;  // rendered worlds per CTA of k_frame_setup
+
+// One warp per rendered world: the terrain's lowest and highest column and
+// the lamps' heights spread over the lanes, then lane 0 sets up the camera,
+// lights, poses, markers and glow.
+template <class R>
+__global__ void __launch_bounds__(32 * kSetupWarps)
+    k_frame_setup(Worlds<R> W, const VisK* __restrict__ vis, int nv, int eye_vis, const int* __restrict__ ids,
+                  int n, const float* __restrict__ markers, int mpw, const int* __restrict__ active,
+                  CamState* __restrict__ cams, int cam_slot, CamParams cp, FrameK* __restrict__ frames)
+{
+    const int lane = threadIdx.x & 31;
+    const int item = blockIdx.x * kSetupWarps + threadIdx.x / 32;
     if (item >= n)
-        return;
+        return;  // the whole warp
     const int world = ids ? ids[item] : item;
     FrameK& f = frames[item];
+    // terrain: lowest and highest column, lamps (csrc/arc_render.c:523-549)
+    const TerrainView<R> tv = terrain_of(W, world);
+    double lo = 1e30, hi = -1e30;
+    for (int k = lane; k < tv.nx * tv.ny; k += 32) {
+        double h = (double)tv.h[k];
+        lo = fmin(lo, h);
+        hi = fmax(hi, h);
+    }
+    lo = warp_min(lo);
+    hi = warp_max(hi);
+    if (tv.nx * tv.ny == 0)
+        lo = hi = 0.0;
+    // the lamp's sample offsets accumulate as in the reference; lane k % 32
+    // looks up sample k of each lamp
+    for (int k = 0; k < kLamps; ++k) {
+        double x = (double)tv.ox + tv.nx * (double)tv.cell * (k % kLampGrid + 0.5) / kLampGrid;
+        double y = (double)tv.oy + tv.ny * (double)tv.cell * (k / kLampGrid + 0.5) / kLampGrid, top = lo;
+        int idx = 0;
+        for (double dx = -1.0; dx <= 1.0; dx += 0.5 * (double)tv.cell)
+            for (double dy = -1.0; dy <= 1.0; dy += 0.5 * (double)tv.cell, ++idx)
+                if ((idx & 31) == lane)
+                    top = fmax(top, height_at(tv, x + dx, y + dy));
+        top = warp_max(top);
+        if (lane == 0)
+            put3(f.lamps[k], x, y, top + kLampHeight);
+    }
+    if (lane != 0)
+        return;
     const R* rec = W.rec + (size_t)world * W.stride;
     const int nb = W.off_sphere / kBodyRec;
     // body poses (csrc/arc_render.c:453-469)
@@ -1054,16 +1103,6 @@ __global__ void k_frame_setup(Worlds<R> W, const VisK* __restrict__ vis, int nv,
         for (int k = 0; k < 9; ++k)
             f.rot[b][k] = (float)m[k];
     }
-    // terrain: lowest and highest column, lamps (csrc/arc_render.c:523-549)
-    const TerrainView<R> tv = terrain_of(W, world);
-    double lo = 1e30, hi = -1e30;
-    for (int k = 0; k < tv.nx * tv.ny; ++k) {
-        double h = (double)tv.h[k];
-        lo = fmin(lo, h);
-        hi = fmax(hi, h);
-    }
-    if (tv.nx * tv.ny == 0)
-        lo = hi = 0.0;
     f.nx = tv.nx;
     f.ny = tv.ny;
     f.cell = (float)tv.cell;
@@ -1073,14 +1112,6 @@ __global__ void k_frame_setup(Worlds<R> W, const VisK* __restrict__ vis, int nv,
     f.floor_z = (float)lo;
     f.bottom = (float)(lo - kVoidDepth);
     f.hmax = (float)hi;
-    for (int k = 0; k < kLamps; ++k) {
-        double x = (double)tv.ox + tv.nx * (double)tv.cell * (k % kLampGrid + 0.5) / kLampGrid;
-        double y = (double)tv.oy + tv.ny * (double)tv.cell * (k / kLampGrid + 0.5) / kLampGrid, top = lo;
-        for (double dx = -1.0; dx <= 1.0; dx += 0.5 * (double)tv.cell)
-            for (double dy = -1.0; dy <= 1.0; dy += 0.5 * (double)tv.cell)
-                top = fmax(top, height_at(tv, x + dx, y + dy));
-        put3(f.lamps[k], x, y, top + kLampHeight);
-    }
     // camera (csrc/arc_render.c:700-716, 1040-1062)
     CamState& cs = cams[cam_slot >= 0 ? cam_slot : world];
     const V3<double> fwd_body = qrotate(bq[0], V3<double>{1, 0, 0});
@@ -1484,7 +1515,7 @@ int launch(arc_renderer* r, const SimView& sv, const Worlds<R>& W, const int* d_
            int mpw, const int* d_active, int cam_slot, unsigned char* d_rgb, cudaStream_t st)
 {
     rd::CamParams cp{r->yaw, r->pitch, r->dist, r->w, r->h};
-    rd::k_frame_setup<R><<<(n + 63) / 64, 64, 0, st>>>(W, r->d_vis, r->nv, r->eye_vis, d_ids, n, d_markers, mpw,
+    rd::k_frame_setup<R><<<(n + rd::kSetupWarps - 1) / rd::kSetupWarps, 32 * rd::kSetupWarps, 0, st>>>(W, r->d_vis, r->nv, r->eye_vis, d_ids, n, d_markers, mpw,
                                                        d_active, r->d_cams, cam_slot, cp, r->d_frames);
     if (report(cudaGetLastError(), "frame setup"))
         return ARC_ERR_CUDA;
