@@ -38,6 +38,7 @@
 #include <vector>
 
 #include "arc_model.h"
+#include "arc_task.cuh"
 #include "../../include/arc_render.h"
 
 // CTAs of k_render resident per SM: 2 keeps its registers within 128
@@ -1001,12 +1002,14 @@ __device__ __forceinline__ double wrap_angle(double a)
     return a;
 }
 
-template <class R> __device__ double height_at(const TerrainView<R>& t, double x, double y)
+// Height of the column containing (x, y) (csrc/arc_terrain.h:42-50), with
+// the terrain's FP64 geometry, as the reference computes it.
+template <class R> __device__ double height_at(const TerrainGeomD& g, const R* h, double x, double y)
 {
-    double fx = floor((x - (double)t.ox) / (double)t.cell), fy = floor((y - (double)t.oy) / (double)t.cell);
-    if (!(fx >= 0.0 && fy >= 0.0 && fx < t.nx && fy < t.ny))
-        return (double)t.outside;
-    return (double)t.h[(int)fx + (int)fy * t.nx];
+    double fx = floor((x - g.ox) / g.cell), fy = floor((y - g.oy) / g.cell);
+    if (!(fx >= 0.0 && fy >= 0.0 && fx < g.nx && fy < g.ny))
+        return g.outside;
+    return (double)h[(int)fx + (int)fy * g.nx];
 }
 
 __device__ __forceinline__ void put3(float* d, double x, double y, double z)
@@ -1031,21 +1034,33 @@ __device__ __forceinline__ double warp_max(double v)
 
 constexpr int kSetupWarps = 2;  // rendered worlds per CTA of k_frame_setup
 
-// One warp per rendered world: the terrain's lowest and highest column and
-// the lamps' heights spread over the lanes, then lane 0 sets up the camera,
-// lights, poses, markers and glow.
+// One warp per rendered world: the lanes split the terrain's lowest and
+// highest column, the lamps' heights, the body poses, the visuals' bounding
+// spheres and glow billboards; lane 0 then writes the camera, lights and
+// markers.
 template <class R>
 __global__ void __launch_bounds__(32 * kSetupWarps)
     k_frame_setup(Worlds<R> W, const VisK* __restrict__ vis, int nv, int eye_vis, const int* __restrict__ ids,
                   int n, const float* __restrict__ markers, int mpw, const int* __restrict__ active,
                   CamState* __restrict__ cams, int cam_slot, CamParams cp, FrameK* __restrict__ frames)
 {
-    const int lane = threadIdx.x & 31;
-    const int item = blockIdx.x * kSetupWarps + threadIdx.x / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x / 32;
+    const int item = blockIdx.x * kSetupWarps + warp;
+    __shared__ float s_body_r[kSetupWarps][kPoses];
     if (item >= n)
         return;  // the whole warp
     const int world = ids ? ids[item] : item;
     FrameK& f = frames[item];
+    const R* rec = W.rec + (size_t)world * W.stride;
+    const int nb = W.off_sphere / kBodyRec;
+    auto body_x = [&](int b) {
+        const R* p = rec + b * kBodyRec;
+        return V3<double>{(double)p[0], (double)p[1], (double)p[2]};
+    };
+    auto body_q = [&](int b) {
+        const R* p = rec + b * kBodyRec;
+        return Q4<double>{(double)p[3], (double)p[4], (double)p[5], (double)p[6]};
+    };
     // terrain: lowest and highest column, lamps (csrc/arc_render.c:523-549)
     const TerrainView<R> tv = terrain_of(W, world);
     double lo = 1e30, hi = -1e30;
@@ -1058,51 +1073,155 @@ __global__ void __launch_bounds__(32 * kSetupWarps)
     hi = warp_max(hi);
     if (tv.nx * tv.ny == 0)
         lo = hi = 0.0;
-    // the lamp's sample offsets accumulate as in the reference; lane k % 32
-    // looks up sample k of each lamp
-    for (int k = 0; k < kLamps; ++k) {
-        double x = (double)tv.ox + tv.nx * (double)tv.cell * (k % kLampGrid + 0.5) / kLampGrid;
-        double y = (double)tv.oy + tv.ny * (double)tv.cell * (k / kLampGrid + 0.5) / kLampGrid, top = lo;
-        int idx = 0;
-        for (double dx = -1.0; dx <= 1.0; dx += 0.5 * (double)tv.cell)
-            for (double dy = -1.0; dy <= 1.0; dy += 0.5 * (double)tv.cell, ++idx)
-                if ((idx & 31) == lane)
-                    top = fmax(top, height_at(tv, x + dx, y + dy));
-        top = warp_max(top);
-        if (lane == 0)
-            put3(f.lamps[k], x, y, top + kLampHeight);
+    // Each lamp takes the highest column among samples at offsets that
+    // accumulate in steps of half a cell from -1 m to 1 m, as the reference's
+    // loops do. The lanes split the (lamp, x offset) pairs; a lane rebuilds
+    // its x offset by the same accumulation.
+    const TerrainGeomD gd = W.tgd[world];
+    const double step = 0.5 * gd.cell;
+    int count = 0;
+    for (double d = -1.0; d <= 1.0 && count < (1 << 16); d += step)
+        ++count;
+    auto lamp_x = [&](int k) { return gd.ox + gd.nx * gd.cell * (k % kLampGrid + 0.5) / kLampGrid; };
+    auto lamp_y = [&](int k) { return gd.oy + gd.ny * gd.cell * (k / kLampGrid + 0.5) / kLampGrid; };
+    double tops[kLamps];
+#pragma unroll
+    for (int k = 0; k < kLamps; ++k)
+        tops[k] = lo;
+    for (int q = lane; q < kLamps * count; q += 32) {
+        const int k = q / count, i = q % count;
+        double dx = -1.0;
+        for (int a = 0; a < i; ++a)
+            dx += step;
+        const double x = lamp_x(k) + dx, y = lamp_y(k);
+        double top = lo;
+        int guard = 0;
+        for (double dy = -1.0; dy <= 1.0 && guard < (1 << 16); dy += step, ++guard)
+            top = fmax(top, height_at(gd, tv.h, x, y + dy));
+#pragma unroll
+        for (int kk = 0; kk < kLamps; ++kk)
+            if (kk == k)
+                tops[kk] = fmax(tops[kk], top);
     }
-    if (lane != 0)
-        return;
-    const R* rec = W.rec + (size_t)world * W.stride;
-    const int nb = W.off_sphere / kBodyRec;
-    // body poses (csrc/arc_render.c:453-469)
-    V3<double> bx[kMaxBodies];
-    Q4<double> bq[kMaxBodies];
-    for (int b = 0; b < kPoses; ++b) {
+#pragma unroll
+    for (int k = 0; k < kLamps; ++k) {
+        const double top = warp_max(tops[k]);
+        if (lane == 0)
+            put3(f.lamps[k], lamp_x(k), lamp_y(k), top + kLampHeight);
+    }
+    // body poses (csrc/arc_render.c:453-469), one lane per body
+    if (lane < kPoses) {
+        const int b = lane;
         double x[3] = {0, 0, 0}, m[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
         if (b < nb && b < kMaxBodies) {
-            const R* p = rec + b * kBodyRec;
-            double qw = p[3], qx = p[4], qy = p[5], qz = p[6];
-            x[0] = p[0];
-            x[1] = p[1];
-            x[2] = p[2];
-            bx[b] = V3<double>{x[0], x[1], x[2]};
-            bq[b] = Q4<double>{qw, qx, qy, qz};
-            m[0] = 1 - 2 * (qy * qy + qz * qz);
-            m[1] = 2 * (qx * qy - qw * qz);
-            m[2] = 2 * (qx * qz + qw * qy);
-            m[3] = 2 * (qx * qy + qw * qz);
-            m[4] = 1 - 2 * (qx * qx + qz * qz);
-            m[5] = 2 * (qy * qz - qw * qx);
-            m[6] = 2 * (qx * qz - qw * qy);
-            m[7] = 2 * (qy * qz + qw * qx);
-            m[8] = 1 - 2 * (qx * qx + qy * qy);
+            const V3<double> bxx = body_x(b);
+            const Q4<double> q = body_q(b);
+            x[0] = bxx.x;
+            x[1] = bxx.y;
+            x[2] = bxx.z;
+            m[0] = 1 - 2 * (q.y * q.y + q.z * q.z);
+            m[1] = 2 * (q.x * q.y - q.w * q.z);
+            m[2] = 2 * (q.x * q.z + q.w * q.y);
+            m[3] = 2 * (q.x * q.y + q.w * q.z);
+            m[4] = 1 - 2 * (q.x * q.x + q.z * q.z);
+            m[5] = 2 * (q.y * q.z - q.w * q.x);
+            m[6] = 2 * (q.x * q.z - q.w * q.y);
+            m[7] = 2 * (q.y * q.z + q.w * q.x);
+            m[8] = 1 - 2 * (q.x * q.x + q.y * q.y);
         }
         put3(f.pos[b], x[0], x[1], x[2]);
         for (int k = 0; k < 9; ++k)
             f.rot[b][k] = (float)m[k];
+        s_body_r[warp][b] = 0.0f;
     }
+    // camera (csrc/arc_render.c:700-716, 1040-1062): every lane computes it,
+    // lane 0 stores the smoothing state
+    CamState& cs = cams[cam_slot >= 0 ? cam_slot : world];
+    const V3<double> x0 = body_x(0);
+    const Q4<double> q0 = body_q(0);
+    const V3<double> fwd_body = qrotate(q0, V3<double>{1, 0, 0});
+    const double heading = atan2(fwd_body.y, fwd_body.x);
+    const V3<double> target = x0 + V3<double>{0, 0, 0.1};
+    V3<double> ct{cs.target[0], cs.target[1], cs.target[2]};
+    double cam_heading = cs.heading;
+    __syncwarp();
+    if (!cs.init || len(target - ct) > 3.0) {
+        ct = target;
+        cam_heading = heading;
+    }
+    ct = ct + scale(target - ct, 0.15);
+    cam_heading += 0.03 * wrap_angle(heading - cam_heading);
+    __syncwarp();
+    if (lane == 0) {
+        cs.init = 1;
+        cs.heading = cam_heading;
+        cs.target[0] = ct.x;
+        cs.target[1] = ct.y;
+        cs.target[2] = ct.z;
+    }
+    const double yaw = cam_heading + kPi + cp.yaw;
+    V3<double> eye = ct + V3<double>{cp.dist * cos(cp.pitch) * cos(yaw), cp.dist * cos(cp.pitch) * sin(yaw),
+                                     cp.dist * sin(cp.pitch)};
+    eye.z = fmax(eye.z, height_at(gd, tv.h, eye.x, eye.y) + 0.2);
+    // bounding spheres of the shadow casters (the robot's, and each body's,
+    // centred on the body) and the robot's glow billboards, in visual order
+    // (csrc/arc_render.c:636-646), the lanes splitting the visuals
+    double rr = 0.0;
+    int ng = 0;
+    for (int base = 0; base < nv; base += 32) {
+        const int i = base + lane;
+        bool glow = false;
+        V3<double> c{0, 0, 0};
+        double sz = 0.0;
+        if (i < nv && vis[i].type >= 0) {
+            const VisK& v = vis[i];
+            const V3<double> bxx = body_x(v.body);
+            const Q4<double> bqq = body_q(v.body);
+            if (!v.glow) {
+                const V3<double> cw = bxx + qrotate(bqq, V3<double>{v.bc[0], v.bc[1], v.bc[2]});
+                rr = fmax(rr, len(cw - x0) + v.br);
+                atomicMax(reinterpret_cast<int*>(&s_body_r[warp][v.body]),
+                          __float_as_int((float)(len(cw - bxx) + v.br)));
+            } else {
+                V3<double> local = v.type == kVisCylinder
+                                       ? V3<double>{v.o[0] + 0.5 * v.b * v.d[0], v.o[1] + 0.5 * v.b * v.d[1],
+                                                    v.o[2] + 0.5 * v.b * v.d[2]}
+                                       : V3<double>{v.o[0], v.o[1], v.o[2]};
+                if (v.type == kVisTaper)
+                    local = V3<double>{v.bc[0], v.bc[1], v.bc[2]};
+                c = bxx + qrotate(bqq, local);
+                sz = v.type == kVisRing ? 1.7 * (v.a + v.b) : 3.5 * v.a;
+                glow = true;
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, glow);
+        const int pos = ng + __popc(m & ((1u << lane) - 1u));
+        if (glow && pos < kMaxGlow) {
+            const VisK& v = vis[i];
+            const V3<double> bc = c + scale(normalize(eye - c), 0.6 * sz);
+            GlowK& g = f.glow[pos];
+            put3(g.c, bc.x, bc.y, bc.z);
+            g.s = (float)sz;
+            put3(g.col, v.col[0], v.col[1], v.col[2]);
+            g.alpha = v.type == kVisRing ? 0.4f : 0.3f;
+            g.beam = 0;
+        }
+        ng = min(ng + __popc(m), kMaxGlow);
+    }
+    rr = warp_max(rr);
+    __syncwarp();
+    if (lane < kPoses) {
+        const int b = lane;
+        const float r = s_body_r[warp][b];
+        const bool has = b < nb && b < kMaxBodies && r > 0.0f;
+        const V3<double> bxx = has ? body_x(b) : V3<double>{0, 0, 0};
+        put3(f.body_c[b], bxx.x, bxx.y, bxx.z);
+        f.body_r[b] = has ? r + 1e-3f : 0.0f;
+    }
+    if (lane != 0)
+        return;
+    const V3<double> bx0 = x0;
+    const Q4<double> bq0 = q0;
     f.nx = tv.nx;
     f.ny = tv.ny;
     f.cell = (float)tv.cell;
@@ -1112,26 +1231,6 @@ __global__ void __launch_bounds__(32 * kSetupWarps)
     f.floor_z = (float)lo;
     f.bottom = (float)(lo - kVoidDepth);
     f.hmax = (float)hi;
-    // camera (csrc/arc_render.c:700-716, 1040-1062)
-    CamState& cs = cams[cam_slot >= 0 ? cam_slot : world];
-    const V3<double> fwd_body = qrotate(bq[0], V3<double>{1, 0, 0});
-    const double heading = atan2(fwd_body.y, fwd_body.x);
-    const V3<double> target = bx[0] + V3<double>{0, 0, 0.1};
-    V3<double> ct{cs.target[0], cs.target[1], cs.target[2]};
-    if (!cs.init || len(target - ct) > 3.0) {
-        ct = target;
-        cs.heading = heading;
-        cs.init = 1;
-    }
-    ct = ct + scale(target - ct, 0.15);
-    cs.heading += 0.03 * wrap_angle(heading - cs.heading);
-    cs.target[0] = ct.x;
-    cs.target[1] = ct.y;
-    cs.target[2] = ct.z;
-    const double yaw = cs.heading + kPi + cp.yaw;
-    V3<double> eye = ct + V3<double>{cp.dist * cos(cp.pitch) * cos(yaw), cp.dist * cos(cp.pitch) * sin(yaw),
-                                     cp.dist * sin(cp.pitch)};
-    eye.z = fmax(eye.z, height_at(tv, eye.x, eye.y) + 0.2);
     const V3<double> fz = normalize(ct - eye);
     const V3<double> sx = normalize(cross(fz, V3<double>{0, 0, 1}));
     const V3<double> uy = cross(sx, fz);
@@ -1167,8 +1266,8 @@ __global__ void __launch_bounds__(32 * kSetupWarps)
     if (eye_vis >= 0) {  // csrc/arc_render.c:1010-1023
         const VisK& v = vis[eye_vis];
         const float* ax = v.d;
-        const V3<double> axis = qrotate(bq[0], normalize(V3<double>{ax[0], ax[1], ax[2]}));
-        const V3<double> c = bx[0] + qrotate(bq[0], V3<double>{v.o[0], v.o[1], v.o[2]});
+        const V3<double> axis = qrotate(bq0, normalize(V3<double>{ax[0], ax[1], ax[2]}));
+        const V3<double> c = bx0 + qrotate(bq0, V3<double>{v.o[0], v.o[1], v.o[2]});
         const V3<double> ep = c + scale(axis, 0.05);
         const V3<double> ed = normalize(axis + V3<double>{0, 0, -0.35});
         put3(f.eye_pos, ep.x, ep.y, ep.z);
@@ -1187,49 +1286,9 @@ __global__ void __launch_bounds__(32 * kSetupWarps)
         put3(f.beacon_pos, mk[0], mk[1], (double)mk[2] + kBeaconHeight);
         put3(f.beacon_col, k * c[0], k * c[1], k * c[2]);
     }
-    // bounding spheres of the shadow casters: the robot's, and each body's
-    // (centred on the body), then the robot's glow billboards
-    double rr = 0.0, br[kPoses] = {};
-    int ng = 0;
-    for (int i = 0; i < nv; ++i) {
-        const VisK& v = vis[i];
-        if (v.type < 0)
-            continue;
-        const V3<double> cw =
-            bx[v.body] + qrotate(bq[v.body], V3<double>{v.bc[0], v.bc[1], v.bc[2]});
-        if (!v.glow) {
-            rr = fmax(rr, len(cw - bx[0]) + v.br);
-            br[v.body] = fmax(br[v.body], len(cw - bx[v.body]) + v.br);
-            continue;
-        }
-        if (ng >= kMaxGlow)
-            continue;
-        // halo (csrc/arc_render.c:636-646): centre of the visual, pulled toward the eye
-        V3<double> local = v.type == kVisCylinder || v.type == kVisTaper
-                               ? V3<double>{v.o[0] + 0.5 * v.b * v.d[0], v.o[1] + 0.5 * v.b * v.d[1],
-                                            v.o[2] + 0.5 * v.b * v.d[2]}
-                               : V3<double>{v.o[0], v.o[1], v.o[2]};
-        if (v.type == kVisTaper)
-            local = V3<double>{v.bc[0], v.bc[1], v.bc[2]};
-        const V3<double> c = bx[v.body] + qrotate(bq[v.body], local);
-        const double s = v.type == kVisRing ? 1.7 * (v.a + v.b) : 3.5 * v.a;
-        const V3<double> toward = normalize(eye - c);
-        const V3<double> bc = c + scale(toward, 0.6 * s);
-        GlowK& g = f.glow[ng++];
-        put3(g.c, bc.x, bc.y, bc.z);
-        g.s = (float)s;
-        put3(g.col, v.col[0], v.col[1], v.col[2]);
-        g.alpha = v.type == kVisRing ? 0.4f : 0.3f;
-        g.beam = 0;
-    }
-    for (int b = 0; b < kPoses; ++b) {
-        const bool has = b < nb && b < kMaxBodies && br[b] > 0.0;
-        put3(f.body_c[b], has ? bx[b].x : 0.0, has ? bx[b].y : 0.0, has ? bx[b].z : 0.0);
-        f.body_r[b] = has ? (float)br[b] + 1e-3f : 0.0f;
-    }
-    f.robot_c[0] = (float)bx[0].x;
-    f.robot_c[1] = (float)bx[0].y;
-    f.robot_c[2] = (float)bx[0].z;
+    f.robot_c[0] = (float)bx0.x;
+    f.robot_c[1] = (float)bx0.y;
+    f.robot_c[2] = (float)bx0.z;
     f.robot_r = (float)rr + 1e-3f;
     // markers: beacon spheres and rings (emissive), halos and beams (csrc/arc_render.c:566-599, 647-671)
     int ne = 0;
@@ -1281,6 +1340,23 @@ __global__ void __launch_bounds__(32 * kSetupWarps)
     }
     f.n_items = ne;
     f.n_glow = ng;
+}
+
+// The checkpoint of each world of a device env as its marker, highlighted
+// while the robot sees it (ArcTask.markers and Viewer.render,
+// arc/task.py:261-264, arc/env.py:45-47).
+__global__ void k_env_markers(TaskState S, double radius, const int* __restrict__ ids, int n,
+                              float* __restrict__ markers, int* __restrict__ active)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    const int w = ids ? ids[k] : k;
+    markers[4 * k + 0] = (float)S.target[2 * w];
+    markers[4 * k + 1] = (float)S.target[2 * w + 1];
+    markers[4 * k + 2] = (float)S.target_z[w];
+    markers[4 * k + 3] = (float)radius;
+    active[k] = S.in_view[w] ? 0 : -1;
 }
 
 }  // namespace rd
@@ -1438,6 +1514,10 @@ struct arc_renderer {
     int* d_active = nullptr;
     int markers_cap = 0;
     unsigned char* h_scratch = nullptr;
+    // markers of arc_env_render
+    float* d_env_markers = nullptr;
+    int* d_env_active = nullptr;
+    int env_cap = 0;
 };
 
 namespace {
@@ -1575,6 +1655,8 @@ void arc_render_destroy(arc_renderer* r)
     cudaFree(r->d_rgb);
     cudaFree(r->d_markers);
     cudaFree(r->d_ids);
+    cudaFree(r->d_env_markers);
+    cudaFree(r->d_env_active);
     cudaFreeHost(r->h_scratch);
     delete r;
 }
@@ -1668,6 +1750,36 @@ int arc_render_frames(arc_renderer* r, const arc_sim* s, const int* d_ids, int n
         return ARC_ERR_ARG;
     cudaStream_t st = stream ? (cudaStream_t)stream : (cudaStream_t)arc_sim_stream(s);
     return render_any(r, s, d_ids, n, d_markers, d_markers ? markers_per_world : 0, d_active, -1, d_rgb, st);
+}
+
+int arc_env_render(arc_renderer* r, const arc_sim* s, const int* d_ids, int n, unsigned char* d_rgb, void* stream)
+{
+    if (!r || !s || !d_rgb || n < 0)
+        return ARC_ERR_ARG;
+    TaskState ts;
+    double radius = 0.0;
+    if (!sim_task_view(s, &ts, &radius))
+        return ARC_ERR_ARG;
+    if (n == 0)
+        return ARC_OK;
+    if (!d_ids && n > arc_sim_num_worlds(s))
+        return ARC_ERR_ARG;
+    if (n > r->env_cap) {
+        cudaFree(r->d_env_markers);
+        cudaFree(r->d_env_active);
+        r->d_env_markers = nullptr;
+        r->d_env_active = nullptr;
+        r->env_cap = 0;
+        if (report(cudaMalloc((void**)&r->d_env_markers, sizeof(float) * 4 * n), "cudaMalloc(markers)") ||
+            report(cudaMalloc((void**)&r->d_env_active, sizeof(int) * n), "cudaMalloc(markers)"))
+            return ARC_ERR_CUDA;
+        r->env_cap = n;
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : (cudaStream_t)arc_sim_stream(s);
+    rd::k_env_markers<<<(n + 127) / 128, 128, 0, st>>>(ts, radius, d_ids, n, r->d_env_markers, r->d_env_active);
+    if (report(cudaGetLastError(), "env markers"))
+        return ARC_ERR_CUDA;
+    return render_any(r, s, d_ids, n, r->d_env_markers, 1, r->d_env_active, -1, d_rgb, st);
 }
 
 }  // extern "C"

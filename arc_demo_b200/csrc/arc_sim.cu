@@ -1573,3 +1573,12 @@ SimView arc::sim_view(const arc_sim* s)
 {
     return SimView{&s->model, view<float>(s), view<double>(s), s->fp64, s->n, s->stream};
 }
+
+bool arc::sim_task_view(const arc_sim* s, TaskState* state, double* checkpoint_radius)
+{
+    if (!s || !s->env)
+        return false;
+    *state = s->ts;
+    *checkpoint_radius = s->tp.checkpoint_radius;
+    return true;
+}

@@ -5,6 +5,8 @@
 
 #include "arc_kernels.cuh"
 
+struct arc_sim;
+
 namespace arc {
 
 constexpr int kNumOffsets = 143;                 // arc/task.py:74-76: 13 forward x 11 left
@@ -89,5 +91,9 @@ template <class R>
 cudaError_t launch_reset_warp(const ResetModel& RM, const Worlds<R>& W, TerrainGeom<R>* tg, TerrainGeomD* tgd,
                               const int* ids, int n_ids, const unsigned* seeds, const double* difficulty,
                               const int* grid_of, double cell, cudaStream_t stream);
+
+// The device task state of an arc_sim whose task layer is initialised
+// (false otherwise), and its checkpoint radius; arc_sim.cu owns the struct.
+bool sim_task_view(const arc_sim* s, TaskState* state, double* checkpoint_radius);
 
 }  // namespace arc

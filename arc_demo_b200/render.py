@@ -43,6 +43,7 @@ def render_lib() -> ctypes.CDLL:
     d("arc_render_set_samples", _int, _vp, _int)
     d("arc_render_reset_cameras", _int, _vp)
     d("arc_render_frames", _int, _vp, _vp, _vp, _int, _vp, _int, _vp, _vp, _vp)
+    d("arc_env_render", _int, _vp, _vp, _vp, _int, _vp, _vp)
     return lib
 
 
@@ -114,6 +115,28 @@ class Renderer:
                                          stream)
         if rc != 0:
             raise ArcSimError(f"arc_render_frames failed ({rc})")
+        return out
+
+    def env_frames(self, env, ids=None, out=None, stream: int | None = None):
+        """Frames of a `DeviceVecEnv`'s worlds with their checkpoints, as the
+        reference's Viewer draws them: a (n, H, W, 3) uint8 CUDA tensor."""
+        import torch
+
+        if not stream:
+            stream = torch.cuda.current_stream().cuda_stream or CUDA_STREAM_LEGACY
+        sim = env.sim
+        n = sim.num_worlds if ids is None else int(ids.numel())
+        w, h = self.size()
+        if out is None:
+            out = torch.empty((n, h, w, 3), dtype=torch.uint8, device="cuda")
+        assert out.is_cuda and out.dtype == torch.uint8 and out.is_contiguous() and out.numel() == n * h * w * 3
+        ids_ptr = None
+        if ids is not None:
+            assert ids.is_cuda and ids.dtype == torch.int32 and ids.is_contiguous()
+            ids_ptr = ids.data_ptr()
+        rc = self._lib.arc_env_render(self._ptr, sim.ptr, ids_ptr, n, out.data_ptr(), stream)
+        if rc != 0:
+            raise ArcSimError(f"arc_env_render failed ({rc})")
         return out
 
     def set_samples(self, samples: int) -> None:

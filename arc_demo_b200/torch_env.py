@@ -93,5 +93,20 @@ class DeviceVecEnv:
         self.sim._check(rc)
         return self.obs, self.reward, self.terminated, self.truncated
 
+    def render(self, ids: torch.Tensor | None = None, width: int = 640, height: int = 360) -> torch.Tensor:
+        """Frames of the worlds (all, or the int32 CUDA tensor ids) with their
+        checkpoints, as the reference's rgb_array mode draws one world
+        (arc/env.py:38-50): a (n, height, width, 3) uint8 CUDA tensor. Each
+        world keeps its own following camera across calls."""
+        from .render import Renderer
+        r = getattr(self, "_renderer", None)
+        if r is None or r.size() != (width, height):
+            r = self._renderer = Renderer(width, height, visible=False)
+        return r.env_frames(self, ids)
+
     def close(self) -> None:
+        r = getattr(self, "_renderer", None)
+        if r is not None:
+            r.close()
+            self._renderer = None
         self.sim.close()

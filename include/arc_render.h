@@ -78,6 +78,14 @@ int arc_render_reset_cameras(arc_renderer *r);
 int arc_render_frames(arc_renderer *r, const arc_sim *s, const int *d_ids, int n, const float *d_markers,
                       int markers_per_world, const int *d_active, unsigned char *d_rgb, void *stream);
 
+/*
+ * The worlds of a sim whose device task layer is initialised (arc_env_init)
+ * rendered like arc_render_frames, each with its current checkpoint as the
+ * marker, highlighted while the robot sees it (arc/env.py:45-47,
+ * arc/task.py:261-264). ARC_ERR_ARG without a task layer.
+ */
+int arc_env_render(arc_renderer *r, const arc_sim *s, const int *d_ids, int n, unsigned char *d_rgb, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -153,3 +153,33 @@ def test_errors_are_reported_not_faults():
     assert r.keys() == []
     # and it still renders
     assert r.frame(sim, 1, None, -1, rgb=True).mean() > 20.0
+
+
+def test_device_env_frames_show_each_world_checkpoint():
+    """arc_env_render takes each world's checkpoint and in-view flag from the
+    device task layer: the bytes equal arc_render_frames given the same
+    markers from the task state (target x, y, z, radius; active 0 while in
+    view, arc/env.py:45-47)."""
+    import torch
+    from arc_demo_b200.task import TaskConfig
+    from arc_demo_b200.torch_env import DeviceVecEnv
+
+    n = 6
+    env = DeviceVecEnv(n, TaskConfig(curriculum=False), seed=3)
+    env.reset()
+    for _ in range(3):
+        env.step(torch.zeros((n, 12), dtype=torch.float32, device="cuda"))
+    torch.cuda.synchronize()
+    ids = torch.tensor([5, 1, 3], dtype=torch.int32, device="cuda")
+    a = Renderer(W, H, visible=False)
+    got = a.env_frames(env, ids).cpu().numpy()
+    st = env.gpu.get_state()[ids.cpu().numpy()]
+    markers = np.stack([st[:, 0], st[:, 1], st[:, 2], np.full(3, env.cfg.checkpoint_radius)], axis=1)
+    markers = torch.tensor(markers[:, None, :].astype(np.float32), device="cuda")
+    active = torch.tensor(np.where(st[:, 22] != 0, 0, -1).astype(np.int32), device="cuda")
+    b = Renderer(W, H, visible=False)
+    want = b.frames(env.sim, ids, markers, active).cpu().numpy()
+    assert np.array_equal(got, want)
+    frames = env.render(width=W, height=H)
+    assert frames.shape == (n, H, W, 3) and frames.is_cuda
+    env.close()
