@@ -31,7 +31,9 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxe
 # per-file flags: the warp-per-leg FP32 step divides and takes square roots
 # with the full-range approximate instructions (at most 2 ulp), whose errors
 # are far below the FP32 parity bounds its tests hold it to
-FILE_FLAGS = {"arc_step_warps.cu": ["-prec-div=false", "-prec-sqrt=false"]}
+FILE_FLAGS = {"arc_step_warps.cu": ["-prec-div=false", "-prec-sqrt=false"],
+              # the renderer: the same, for code size (its output is 8-bit colour)
+              "arc_render.cu": ["-prec-div=false", "-prec-sqrt=false"]}
 
 
 def nvcc() -> str:

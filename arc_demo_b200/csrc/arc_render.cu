@@ -155,10 +155,13 @@ __device__ __forceinline__ F3 rot_tmul(const float* m, F3 v)
 
 // The shader's value noise (csrc/arc_render.c:151-158). The hash of a
 // lattice point is evaluated with one rounding order (an explicit fma), so
-// that CPU restatements can reproduce it. noise2, hit_visual and
-// trace_terrain stay out of line: the kernel's code is far larger than the
-// instruction cache, and one copy of each is faster than inlined copies.
-__device__ __forceinline__ float hash2(float x, float y)
+// that CPU restatements can reproduce it. noise2, hit_visual,
+// trace_terrain and shade_light stay out of line and the taper's plane loop
+// stays rolled: the kernel's code is larger than the instruction cache, and
+// one copy of each is faster than inlined copies. For the same reason this
+// file is compiled with the approximate (at most 2 ulp) division and square
+// root, whose code is a fraction of the IEEE versions'.
+__device__ __noinline__ float hash2(float x, float y)
 {
     return fractf(__fmul_rn(sinf(fmaf(x, 127.1f, y * 311.7f)), 43758.5453f));
 }
@@ -372,6 +375,7 @@ __device__ __noinline__ bool hit_visual(const VisK& v, F3 o, F3 D, float tmax, f
     case kVisTaper: {
         float tn = 1e-4f, tf = tmax;
         int enter = -1;
+#pragma unroll 1
         for (int k = 0; k < 10; ++k) {
             const F3 pn{v.pl[k][0], v.pl[k][1], v.pl[k][2]};
             float den = dot(pn, D), dist = v.pl[k][3] - dot(pn, o);
@@ -442,7 +446,7 @@ __device__ __noinline__ bool hit_visual(const VisK& v, F3 o, F3 D, float tmax, f
             float z = dot(p, d);
             F3 radial = normalize(p - scale(d, z));
             // ribbed sleeve: the corrugation's slope (csrc/arc_mesh.c:84-90)
-            float slope = rib > 0.0f ? rib * 0.5f * v.e * sinf(v.e * z) : 0.0f;
+            float slope = rib > 0.0f ? rib * 0.5f * (3.14159265f * v.e) * sinpif(v.e * z) : 0.0f;
             n = normalize(radial + scale(d, slope));
         } else {
             n = kind == 1 ? -d : d;
@@ -542,11 +546,16 @@ struct Surface {
     F3 g;             // terrain: grid coordinates (g.x, g.y); panels: unit-sphere point
 };
 
-__device__ __forceinline__ F3 shade_light(F3 a, float spec, float gloss, F3 n, F3 v, F3 l, F3 col)
+// x^y for x in [0, 1], y > 0, by the hardware base-2 exponential and
+// logarithm (relative error ~1e-6: far below one level of 8-bit colour);
+// 0^y = 0.
+__device__ __forceinline__ float pow_approx(float x, float y) { return x > 0.0f ? exp2f(y * __log2f(x)) : 0.0f; }
+
+__device__ __noinline__ F3 shade_light(F3 a, float spec, float gloss, F3 n, F3 v, F3 l, F3 col)
 {
     float d = fmaxf(dot(n, l), 0.0f);
     F3 hv = normalize(l + v);
-    float s = powf(fmaxf(dot(n, hv), 0.0f), gloss) * (gloss + 8.0f) / 25.0f;
+    float s = pow_approx(fmaxf(dot(n, hv), 0.0f), gloss) * (gloss + 8.0f) / 25.0f;
     return F3{(a.x + spec * s) * d * col.x, (a.y + spec * s) * d * col.y, (a.z + spec * s) * d * col.z};
 }
 
@@ -590,7 +599,7 @@ __device__ F3 shade_scene(const FrameK& fr, const Surface& s, float lit_k)
     const float hemi = 0.5f + 0.5f * n.z;
     F3 c = vmul(a, F3{mixf(gnd.x, sky.x, hemi), mixf(gnd.y, sky.y, hemi), mixf(gnd.z, sky.z, hemi)});
     float qx = (s.p.x - fr.focus[0]) / 6.0f, qy = (s.p.y - fr.focus[1]) / 6.0f;
-    float pool = 0.65f + 0.35f * expf(-(qx * qx + qy * qy));
+    float pool = 0.65f + 0.35f * __expf(-(qx * qx + qy * qy));
     c = c + scale(shade_light(a, spec, gloss, n, v, ld3(fr.sun), ld3(c_sun_col)), lit_k * pool);
     c = c + shade_light(a, spec, gloss, n, v, ld3(fr.fill), ld3(c_fill_col));
     for (int i = 0; i < kLamps; ++i) {
@@ -625,14 +634,14 @@ __device__ F3 shade_scene(const FrameK& fr, const Surface& s, float lit_k)
     c = c + scale(sky, rim * nv4 * 0.6f);
     if (s.emis >= 0.5f)
         c = scale(a, s.emis);
-    c = scale(c, expf(-kFogDensity * fmaxf(len(ld3(fr.eye) - s.p) - fr.fog_start, 0.0f)));
+    c = scale(c, __expf(-kFogDensity * fmaxf(len(ld3(fr.eye) - s.p) - fr.fog_start, 0.0f)));
     c = scale(c, smooth(fr.floor_z - 3.0f, fr.floor_z + 0.2f, s.p.z));
     // ACES fit, then gamma
     float cc[3] = {c.x, c.y, c.z};
     for (int k = 0; k < 3; ++k) {
         float x = cc[k];
         x = x * (2.51f * x + 0.03f) / (x * (2.43f * x + 0.59f) + 0.14f);
-        cc[k] = powf(clampf(x, 0.0f, 1.0f), 1.0f / 2.2f);
+        cc[k] = pow_approx(clampf(x, 0.0f, 1.0f), 1.0f / 2.2f);
     }
     return F3{cc[0], cc[1], cc[2]};
 }
@@ -663,7 +672,7 @@ __device__ F3 glow_along(const FrameK& fr, unsigned mask, F3 O, F3 D, float tdep
             if (fabsf(u) > 1.0f || fabsf(vv) > 1.0f)
                 continue;
             float r2 = u * u + vv * vv;
-            float halo = expf(-6.0f * r2) * 0.8f + expf(-30.0f * r2);
+            float halo = __expf(-6.0f * r2) * 0.8f + __expf(-30.0f * r2);
             w = halo * (1.0f - smooth(0.7f, 1.0f, r2));
         } else {
             const F3 side = ld3(k.side);
@@ -679,10 +688,10 @@ __device__ F3 glow_along(const FrameK& fr, unsigned mask, F3 O, F3 D, float tdep
             vv = P.z / 3.5f;
             if (fabsf(u) > 1.0f || vv < 0.0f || vv > 1.0f)
                 continue;
-            w = expf(-12.0f * u * u) * (1.0f - vv) * (1.0f - vv);
+            w = __expf(-12.0f * u * u) * (1.0f - vv) * (1.0f - vv);
         }
         F3 P = O + scale(D, t);
-        w *= k.alpha * expf(-kFogDensity * fmaxf(len(eye - P) - fr.fog_start, 0.0f));
+        w *= k.alpha * __expf(-kFogDensity * fmaxf(len(eye - P) - fr.fog_start, 0.0f));
         g = g + scale(ld3(k.col), w);
     }
     return g;
@@ -1470,7 +1479,7 @@ VisK make_vis(const ModelHost::Visual& s)
         v.b = (float)L;
         if (s.material == kMatRibs) {  // csrc/arc_mesh.c:71-72
             v.c = (float)(0.12 * s.radius);
-            v.e = (float)(2.0 * kPi / 0.010);
+            v.e = (float)(2.0 / 0.010);  // sin(2 pi z / pitch) = sinpi(e z)
         }
         put(v.bc, s.p0 + scale(d, 0.5 * L));
         v.br = (float)sqrt(0.25 * L * L + s.radius * s.radius) + 1e-4f;
