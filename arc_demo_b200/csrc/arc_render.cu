@@ -12,7 +12,7 @@
 //                  per world), the lights, the world pose of every body,
 //                  the markers and glow billboards, the terrain's lowest
 //                  and highest column and the lamp heights above it.
-//   k_render       one CTA per 32 x 8 pixel tile of one world: the tile's
+//   k_render       one CTA per 16 x 16 pixel tile of one world: the tile's
 //                  frustum culls the visuals' bounding spheres into a list
 //                  in shared memory; each thread traces its pixel's samples
 //                  (the terrain by a 2D DDA over the columns, the visuals
@@ -41,10 +41,12 @@
 #include "arc_task.cuh"
 #include "../../include/arc_render.h"
 
-// CTAs of k_render resident per SM: 2 keeps its registers within 128
-// without spills
+// CTAs of k_render resident per SM. 4 caps its registers at 64 at the cost
+// of ~250 bytes of spills to L1; the extra warps hide more latency than the
+// spills cost (ms per 256 frames of 640 x 360 x 4 rays: 2 CTAs 24.7, 3 20.6,
+// 4 20.0).
 #ifndef ARC_RENDER_MIN_BLOCKS
-#define ARC_RENDER_MIN_BLOCKS 2
+#define ARC_RENDER_MIN_BLOCKS 4
 #endif
 
 namespace arc {
@@ -52,7 +54,7 @@ namespace rd {
 
 using F3 = V3<float>;
 
-constexpr int kTileW = 32, kTileH = 8, kThreads = kTileW * kTileH;
+constexpr int kTileW = 16, kTileH = 16, kThreads = kTileW * kTileH;
 constexpr int kMaxMarkers = 4;
 constexpr int kLampGrid = 3, kLamps = kLampGrid * kLampGrid;  // csrc/arc_render.c:36-38
 constexpr int kPoses = kMaxBodies + 1;                          // + the identity pose of world-frame items
@@ -697,7 +699,7 @@ __device__ F3 glow_along(const FrameK& fr, unsigned mask, F3 O, F3 D, float tdep
     return g;
 }
 
-// One CTA per 32 x 8 tile of one world's frame (blockIdx.y: the world).
+// One CTA per 16 x 16 tile of one world's frame (blockIdx.y: the world).
 template <class R>
 __global__ void __launch_bounds__(kThreads, ARC_RENDER_MIN_BLOCKS)
     k_render(const VisK* __restrict__ vis, int nv, const FrameK* __restrict__ frames, Worlds<R> W,
@@ -794,7 +796,10 @@ __global__ void __launch_bounds__(kThreads, ARC_RENDER_MIN_BLOCKS)
     T.hmax = fr.hmax;
     T.bottom = fr.bottom;
 
-    const int px = x0 + (tid % kTileW), row = r0 + tid / kTileW;
+    // each warp takes an 8 x 4 block of the tile: nearby pixels tend to hit
+    // the same surfaces, so fewer lanes diverge than along a 32-pixel row
+    static_assert(kTileW == 16 && kTileH == 16, "warp blocks laid out for 16 x 16 tiles");
+    const int px = x0 + ((tid >> 5) & 1) * 8 + (tid & 7), row = r0 + (tid >> 6) * 4 + ((tid >> 3) & 3);
     if (px >= width || row >= height)
         return;
     const float wy_pix = (float)(height - 1 - row);
