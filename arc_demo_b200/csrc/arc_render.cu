@@ -1532,6 +1532,8 @@ struct arc_renderer {
     float* d_env_markers = nullptr;
     int* d_env_active = nullptr;
     int env_cap = 0;
+    cudaEvent_t done = nullptr;  // the last call's kernels
+    bool used = false;
 };
 
 namespace {
@@ -1573,8 +1575,10 @@ int sync_visuals(arc_renderer* r, const SimView& sv)
     return ARC_OK;
 }
 
-// Cameras for every world of s plus one for arc_render_frame (slot n).
-int sync_cameras(arc_renderer* r, const arc_sim* s, int n)
+// Cameras for every world of s plus one for arc_render_frame (slot n),
+// zeroed on the stream of the launch that first reads them (the sim's
+// stream does not synchronise with the legacy default stream).
+int sync_cameras(arc_renderer* r, const arc_sim* s, int n, cudaStream_t st)
 {
     if (r->cam_sim == s && r->cam_n == n && r->d_cams)
         return ARC_OK;
@@ -1583,7 +1587,7 @@ int sync_cameras(arc_renderer* r, const arc_sim* s, int n)
     r->d_cams = nullptr;
     if (report(cudaMalloc((void**)&r->d_cams, sizeof(rd::CamState) * (n + 1)), "cudaMalloc(cameras)"))
         return ARC_ERR_CUDA;
-    if (report(cudaMemset(r->d_cams, 0, sizeof(rd::CamState) * (n + 1)), "cameras"))
+    if (report(cudaMemsetAsync(r->d_cams, 0, sizeof(rd::CamState) * (n + 1), st), "cameras"))
         return ARC_ERR_CUDA;
     r->cam_sim = s;
     r->cam_n = n;
@@ -1625,12 +1629,22 @@ int render_any(arc_renderer* r, const arc_sim* s, const int* d_ids, int n, const
 {
     const SimView sv = sim_view(s);
     int rc;
-    if ((rc = sync_visuals(r, sv)) || (rc = sync_cameras(r, s, sv.n)) || (rc = grow_frames(r, n)))
+    // calls share the frame records and cameras: a call on another stream
+    // waits for the previous call's kernels
+    if (r->used && report(cudaStreamWaitEvent(st, r->done, 0), "stream wait"))
+        return ARC_ERR_CUDA;
+    if ((rc = sync_visuals(r, sv)) || (rc = sync_cameras(r, s, sv.n, st)) || (rc = grow_frames(r, n)))
         return rc;
     if (r->nv > kMaxVisuals)
         return ARC_ERR_ARG;
-    return sv.fp64 ? launch<double>(r, sv, sv.wd, d_ids, n, d_markers, mpw, d_active, cam_slot, d_rgb, st)
-                   : launch<float>(r, sv, sv.wf, d_ids, n, d_markers, mpw, d_active, cam_slot, d_rgb, st);
+    rc = sv.fp64 ? launch<double>(r, sv, sv.wd, d_ids, n, d_markers, mpw, d_active, cam_slot, d_rgb, st)
+                 : launch<float>(r, sv, sv.wf, d_ids, n, d_markers, mpw, d_active, cam_slot, d_rgb, st);
+    if (rc == ARC_OK) {
+        if (report(cudaEventRecord(r->done, st), "event"))
+            return ARC_ERR_CUDA;
+        r->used = true;
+    }
+    return rc;
 }
 
 }  // namespace
@@ -1651,7 +1665,8 @@ arc_renderer* arc_render_create(int width, int height, int visible)
     if (cudaMalloc((void**)&r->d_rgb, bytes) != cudaSuccess ||
         cudaMalloc((void**)&r->d_markers, sizeof(float) * 4 * rd::kMaxMarkers) != cudaSuccess ||
         cudaMalloc((void**)&r->d_ids, sizeof(int) * 2) != cudaSuccess ||
-        cudaMallocHost((void**)&r->h_scratch, bytes) != cudaSuccess) {
+        cudaMallocHost((void**)&r->h_scratch, bytes) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming) != cudaSuccess) {
         arc_render_destroy(r);
         return nullptr;
     }
@@ -1672,6 +1687,8 @@ void arc_render_destroy(arc_renderer* r)
     cudaFree(r->d_env_markers);
     cudaFree(r->d_env_active);
     cudaFreeHost(r->h_scratch);
+    if (r->done)
+        cudaEventDestroy(r->done);
     delete r;
 }
 
@@ -1748,8 +1765,14 @@ int arc_render_reset_cameras(arc_renderer* r)
 {
     if (!r)
         return ARC_ERR_ARG;
-    if (r->d_cams)
-        return report(cudaMemset(r->d_cams, 0, sizeof(rd::CamState) * (r->cam_n + 1)), "cameras");
+    if (!r->d_cams)
+        return ARC_OK;
+    // after every call in flight, before any later one
+    if (r->used && report(cudaEventSynchronize(r->done), "cameras"))
+        return ARC_ERR_CUDA;
+    if (report(cudaMemset(r->d_cams, 0, sizeof(rd::CamState) * (r->cam_n + 1)), "cameras") ||
+        report(cudaDeviceSynchronize(), "cameras"))
+        return ARC_ERR_CUDA;
     return ARC_OK;
 }
 

@@ -66,14 +66,15 @@ int arc_render_set_samples(arc_renderer *r, int samples);
 int arc_render_reset_cameras(arc_renderer *r);
 
 /*
- * Renders the n worlds d_ids[0..n) of s (d_ids NULL: worlds 0..n-1) into
+ * Renders the n distinct worlds d_ids[0..n) of s (d_ids NULL: worlds 0..n-1) into
  * d_rgb, n x height x width x 3 bytes on the device, top rows first.
  * d_markers: NULL, or n x markers_per_world x 4 floats (x, y, z, radius)
  * on the device; d_active: NULL (none highlighted) or n ints, the
  * highlighted marker of each world or -1. markers_per_world <= 4. Each
  * world has its own camera, which follows its robot from frame to frame
  * like the reference's single camera. Asynchronous on `stream` (NULL: the
- * sim's stream); returns ARC_OK or an ARC_ERR_* code.
+ * sim's stream); a call on another stream than the previous call's waits
+ * for it. Returns ARC_OK or an ARC_ERR_* code.
  */
 int arc_render_frames(arc_renderer *r, const arc_sim *s, const int *d_ids, int n, const float *d_markers,
                       int markers_per_world, const int *d_active, unsigned char *d_rgb, void *stream);

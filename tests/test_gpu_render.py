@@ -244,3 +244,27 @@ def test_larger_frame_on_the_full_grid_and_determinism():
     fa = a.frames(sim).cpu().numpy()
     fb = b.frames(sim).cpu().numpy()
     assert np.array_equal(fa, fb)
+
+
+def test_calls_on_different_streams_are_ordered():
+    """Consecutive calls of one renderer on different streams share its
+    frame records and cameras; each waits for the previous one, so the
+    frames equal those of the same calls on one stream."""
+    import torch
+
+    sim = make_sim(4)
+    a = Renderer(W, H, visible=False)
+    b = Renderer(W, H, visible=False)
+    side = torch.cuda.Stream()
+    ids1 = torch.tensor([0, 2], dtype=torch.int32, device="cuda")
+    ids2 = torch.tensor([1, 3, 0], dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    with torch.cuda.stream(side):
+        f1 = a.frames(sim, ids1)
+    f2 = a.frames(sim, ids2)
+    side.synchronize()
+    torch.cuda.synchronize()
+    g1 = b.frames(sim, ids1)
+    g2 = b.frames(sim, ids2)
+    torch.cuda.synchronize()
+    assert torch.equal(f1, g1) and torch.equal(f2, g2)
