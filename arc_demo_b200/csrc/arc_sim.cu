@@ -77,6 +77,13 @@ struct arc_sim {
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t graph_stream = nullptr;
     int graph_kernel = -1, graph_wpc = -1, graph_queue = -1;  // the step form the graph captured
+    // arc_env_step_host: world indices 0..n-1, per-chunk ended-world lists and
+    // counts, the two copy streams and their events
+    int* iota = nullptr;
+    int* chunk_done = nullptr;
+    int* chunk_count = nullptr;
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    cudaEvent_t ev[2 * 16 + 2] = {};
     mutable int err = 0;
     mutable std::string msg;
     mutable bool reported = false;
@@ -251,10 +258,16 @@ void free_all(arc_sim* s)
     for (void* p : s->env_allocs)
         cudaFree(p);
     void* ps[] = {s->rec, s->sph, s->unstable, s->time, s->th, s->toff, s->tg, s->tgd, s->grid_of, s->spill, s->queue,
-                  s->st_in.p, s->st_in2.p, s->st_in3.p, s->st_out.p};
+                  s->st_in.p, s->st_in2.p, s->st_in3.p, s->st_out.p, s->iota, s->chunk_done, s->chunk_count};
     for (void* p : ps)
         if (p)
             cudaFree(p);
+    for (cudaEvent_t e : s->ev)
+        if (e)
+            cudaEventDestroy(e);
+    for (cudaStream_t c : {s->copy_in, s->copy_out, s->graph_stream})
+        if (c)
+            cudaStreamDestroy(c);
     if (s->stream)
         cudaStreamDestroy(s->stream);
     delete s->hworld;
@@ -1133,9 +1146,170 @@ int env_step_launches(arc_sim* s, const float* actions, cudaStream_t st)
     return s->fp64 ? env_reset_done<double>(s, st) : env_reset_done<float>(s, st);
 }
 
+constexpr int kMaxChunks = 16;
+
+// World ranges of arc_env_step_host: range c is first[c] .. first[c + 1] - 1.
+struct Ranges {
+    int first[kMaxChunks + 1];
+};
+
+// Ranges that halve from one to the next (rounded to 32 worlds): the copies
+// of each range are shorter than the step of the next (a world's step takes
+// ~3x its copies), and the last range's copies, which nothing hides, are a
+// small share of all.
+Ranges host_ranges(int n, int chunks)
+{
+    Ranges r{};
+    const double total = 1.0 - std::ldexp(1.0, -chunks);
+    r.first[0] = 0;
+    for (int c = 1; c < chunks; ++c) {
+        const double frac = (1.0 - std::ldexp(1.0, -c)) / total;
+        int f = (int)std::lround(n * frac / 32.0) * 32;
+        f = std::max(f, r.first[c - 1] + 1);
+        r.first[c] = std::min(f, n - (chunks - c));
+    }
+    r.first[chunks] = n;
+    return r;
+}
+
+// The ended worlds of every range, range c's at chunk_done[first[c] ..],
+// gathered into done_list in range order, and their total into done_count.
+__global__ void k_merge_done(const int* __restrict__ chunk_done, const int* __restrict__ chunk_count,
+                             const __grid_constant__ Ranges R, int chunks, int* __restrict__ done_list,
+                             int* __restrict__ done_count)
+{
+    __shared__ int base[kMaxChunks + 1];
+    if (threadIdx.x == 0) {
+        base[0] = 0;
+        for (int c = 0; c < chunks; ++c)
+            base[c + 1] = base[c] + chunk_count[c];
+        *done_count = base[chunks];
+    }
+    __syncthreads();
+    for (int c = 0; c < chunks; ++c) {
+        const int first = R.first[c];
+        for (int k = threadIdx.x; k < chunk_count[c]; k += blockDim.x)
+            done_list[base[c] + k] = chunk_done[first + k];
+    }
+}
+
+__global__ void k_iota(int* __restrict__ out, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        out[i] = i;
+}
+
+int ensure_step_host(arc_sim* s)
+{
+    if (s->iota)
+        return ARC_OK;
+    int* iota = nullptr;
+    if (check(s, cudaMalloc((void**)&s->chunk_done, sizeof(int) * s->n), "cudaMalloc(chunk lists)") ||
+        check(s, cudaMalloc((void**)&s->chunk_count, sizeof(int) * kMaxChunks), "cudaMalloc(chunk counts)") ||
+        check(s, cudaMalloc((void**)&iota, sizeof(int) * s->n), "cudaMalloc(world indices)"))
+        return ARC_ERR_CUDA;
+    k_iota<<<(s->n + 255) / 256, 256, 0, s->stream>>>(iota, s->n);
+    if (check(s, cudaGetLastError(), "world indices") ||
+        check(s, cudaStreamCreateWithFlags(&s->copy_in, cudaStreamNonBlocking), "copy stream") ||
+        check(s, cudaStreamCreateWithFlags(&s->copy_out, cudaStreamNonBlocking), "copy stream")) {
+        cudaFree(iota);
+        return ARC_ERR_CUDA;
+    }
+    for (cudaEvent_t& e : s->ev)
+        if (check(s, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event")) {
+            cudaFree(iota);
+            return ARC_ERR_CUDA;
+        }
+    s->iota = iota;
+    return ARC_OK;
+}
+
+template <class R> int env_step_chunk(arc_sim* s, int first, int count, int c, cudaStream_t st)
+{
+    Actuation A{nullptr, s->actions};
+    if (int rc = step_any(s, A, st, s->iota + first, count))
+        return rc;
+    TaskOut O = s->to;
+    O.done_list = s->chunk_done + first;
+    O.done_count = s->chunk_count + c;
+    if (check(s, launch_task_step<R>(dev_model<R>(s), view<R>(s), s->tp, s->ts, O, s->actions, 1, st, first, count),
+              "task step kernel"))
+        return ARC_ERR_CUDA;
+    return check(s,
+                 launch_task_reset<R>(dev_model<R>(s), s->rm, view<R>(s), (TerrainGeom<R>*)s->tg, s->tgd, s->grid_of,
+                                      s->cell, s->tp, s->ts, s->to.obs, s->chunk_done + first, s->chunk_count + c,
+                                      count, st),
+                 "task reset kernel");
+}
+
 }  // namespace
 
 extern "C" {
+
+int arc_env_step_host(arc_sim* s, const float* h_actions, float* h_obs, float* h_reward, unsigned char* h_terminated,
+                      unsigned char* h_truncated, int chunks)
+{
+    if (int rc = env_check(s))
+        return rc;
+    if (!h_actions || !h_obs)
+        return fail(s, ARC_ERR_ARG, "arc_env_step_host: actions and observations are required");
+    chunks = std::max(1, std::min(chunks, std::min(kMaxChunks, s->n)));
+    if (int rc = ensure_step_host(s))
+        return rc;
+    cudaStream_t st = s->stream;
+    cudaEvent_t* ev_in = s->ev;
+    cudaEvent_t* ev_out = s->ev + kMaxChunks;
+    cudaEvent_t ev_start = s->ev[2 * kMaxChunks], ev_end = s->ev[2 * kMaxChunks + 1];
+    const Ranges R = host_ranges(s->n, chunks);
+    auto range = [&](int c, int& first, int& count) {
+        first = R.first[c];
+        count = R.first[c + 1] - first;
+    };
+    // the copies start after the work already queued on the sim's stream
+    if (check(s, cudaEventRecord(ev_start, st), "event") ||
+        check(s, cudaStreamWaitEvent(s->copy_in, ev_start, 0), "wait") ||
+        check(s, cudaStreamWaitEvent(s->copy_out, ev_start, 0), "wait") ||
+        check(s, cudaMemsetAsync(s->chunk_count, 0, sizeof(int) * chunks, st), "memset counts"))
+        return ARC_ERR_CUDA;
+    for (int c = 0; c < chunks; ++c) {
+        int first, count;
+        range(c, first, count);
+        if (check(s, cudaMemcpyAsync(s->actions + (size_t)first * kNumJoints, h_actions + (size_t)first * kNumJoints,
+                                     sizeof(float) * kNumJoints * count, cudaMemcpyHostToDevice, s->copy_in),
+                  "actions in") ||
+            check(s, cudaEventRecord(ev_in[c], s->copy_in), "event"))
+            return ARC_ERR_CUDA;
+    }
+    for (int c = 0; c < chunks; ++c) {
+        int first, count;
+        range(c, first, count);
+        if (check(s, cudaStreamWaitEvent(st, ev_in[c], 0), "wait"))
+            return ARC_ERR_CUDA;
+        if (int rc = s->fp64 ? env_step_chunk<double>(s, first, count, c, st) : env_step_chunk<float>(s, first, count, c, st))
+            return rc;
+        if (check(s, cudaEventRecord(ev_out[c], st), "event") ||
+            check(s, cudaStreamWaitEvent(s->copy_out, ev_out[c], 0), "wait") ||
+            check(s, cudaMemcpyAsync(h_obs + (size_t)first * kObsSize, s->to.obs + (size_t)first * kObsSize,
+                                     sizeof(float) * kObsSize * count, cudaMemcpyDeviceToHost, s->copy_out),
+                  "observations out") ||
+            (h_reward && check(s, cudaMemcpyAsync(h_reward + first, s->to.reward + first, sizeof(float) * count,
+                                                  cudaMemcpyDeviceToHost, s->copy_out),
+                               "rewards out")) ||
+            (h_terminated && check(s, cudaMemcpyAsync(h_terminated + first, s->to.terminated + first, count,
+                                                      cudaMemcpyDeviceToHost, s->copy_out),
+                                   "terminations out")) ||
+            (h_truncated && check(s, cudaMemcpyAsync(h_truncated + first, s->to.truncated + first, count,
+                                                     cudaMemcpyDeviceToHost, s->copy_out),
+                                  "truncations out")))
+            return ARC_ERR_CUDA;
+    }
+    k_merge_done<<<1, 256, 0, st>>>(s->chunk_done, s->chunk_count, R, chunks, s->to.done_list, s->to.done_count);
+    if (check(s, cudaGetLastError(), "merge ended worlds") || check(s, cudaEventRecord(ev_end, s->copy_out), "event") ||
+        check(s, cudaStreamWaitEvent(st, ev_end, 0), "wait"))
+        return ARC_ERR_CUDA;
+    return sync(s, "arc_env_step_host");
+}
 
 int arc_env_init(arc_sim* s, const arc_task_config* cfg, unsigned long long seed)
 {

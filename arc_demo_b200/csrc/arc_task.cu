@@ -276,11 +276,13 @@ __device__ void place_target(const TaskParams& P, const Worlds<R>& W, const Task
 
 template <class R>
 __global__ void k_task_step(const __grid_constant__ DevModel<R> M, Worlds<R> W, const __grid_constant__ TaskParams P,
-                            TaskState S, TaskOut O, const float* __restrict__ actions, int write_obs_rows)
+                            TaskState S, TaskOut O, const float* __restrict__ actions, int write_obs_rows, int first,
+                            int count)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= W.n)
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count)
         return;
+    const int i = first + k;
     Obs64 o;
     read_world(M, W, i, o);
     const int steps = S.steps[i] + 1;
@@ -689,11 +691,14 @@ int reset_grid(int n)
 
 template <class R>
 cudaError_t launch_task_step(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskState& S,
-                             const TaskOut& O, const float* actions, int write_obs_rows, cudaStream_t stream)
+                             const TaskOut& O, const float* actions, int write_obs_rows, cudaStream_t stream, int first,
+                             int count)
 {
-    if (W.n <= 0)
-        return cudaSuccess;
-    k_task_step<R><<<(W.n + 127) / 128, 128, 0, stream>>>(M, W, P, S, O, actions, write_obs_rows);
+    if (count < 0)
+        count = W.n - first;
+    if (count <= 0 || first < 0 || first + count > W.n)
+        return count == 0 ? cudaSuccess : cudaErrorInvalidValue;
+    k_task_step<R><<<(count + 127) / 128, 128, 0, stream>>>(M, W, P, S, O, actions, write_obs_rows, first, count);
     return cudaGetLastError();
 }
 
@@ -763,7 +768,8 @@ cudaError_t launch_reset_warp(const ResetModel& RM, const Worlds<R>& W, TerrainG
 
 #define ARC_INSTANTIATE_TASK(R)                                                                                    \
     template cudaError_t launch_task_step<R>(const DevModel<R>&, const Worlds<R>&, const TaskParams&,            \
-                                             const TaskState&, const TaskOut&, const float*, int, cudaStream_t); \
+                                             const TaskState&, const TaskOut&, const float*, int, cudaStream_t,  \
+                                             int, int);                                                          \
     template cudaError_t launch_task_observe<R>(const DevModel<R>&, const Worlds<R>&, const TaskParams&,         \
                                                 const TaskState&, float*, const int*, int, cudaStream_t);        \
     template cudaError_t launch_task_reset<R>(const DevModel<R>&, const ResetModel&, const Worlds<R>&,           \

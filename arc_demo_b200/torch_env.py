@@ -93,6 +93,25 @@ class DeviceVecEnv:
         self.sim._check(rc)
         return self.obs, self.reward, self.terminated, self.truncated
 
+    def step_host(self, actions: torch.Tensor, chunks: int = 3):
+        """One control step with host tensors: actions (N x 12 float32, on
+        the host, ideally pinned) in; (obs, reward, terminated, truncated)
+        out as pinned host tensors, reused by the next call. The worlds go
+        in `chunks` ranges whose copies overlap the next range's step
+        (arc_env_step_host); the results equal step() followed by copies."""
+        n = self.num_envs
+        if getattr(self, "_host_out", None) is None:
+            self._host_out = (torch.empty((n, 195), dtype=torch.float32, pin_memory=True),
+                              torch.empty(n, dtype=torch.float32, pin_memory=True),
+                              torch.empty(n, dtype=torch.uint8, pin_memory=True),
+                              torch.empty(n, dtype=torch.uint8, pin_memory=True))
+        a = actions.contiguous()
+        assert a.device.type == "cpu" and a.dtype == torch.float32 and a.shape == (n, 12)
+        obs, rew, term, trunc = self._host_out
+        self.sim._check(self.gpu.lib.arc_env_step_host(self.sim.ptr, a.data_ptr(), obs.data_ptr(), rew.data_ptr(),
+                                                      term.data_ptr(), trunc.data_ptr(), chunks))
+        return self._host_out
+
     def render(self, ids: torch.Tensor | None = None, width: int = 640, height: int = 360) -> torch.Tensor:
         """Frames of the worlds (all, or the int32 CUDA tensor ids) with their
         checkpoints, as the reference's rgb_array mode draws one world

@@ -296,6 +296,22 @@ int arc_env_reset(arc_sim *s, const int *ids, int n_ids, void *stream);
  * through a CUDA graph of the whole step captured on first use. */
 int arc_env_step(arc_sim *s, const float *d_actions, void *stream);
 
+/*
+ * The same control step with host buffers, as ArcVecEnv.step_wait's caller
+ * sees it (arc/env.py:99-117): h_actions (N x 12 float32) in; observations
+ * (N x 195 float32), rewards (N float32), terminated and truncated (N
+ * bytes) out; any output but the observations may be NULL. The worlds are
+ * stepped in `chunks` contiguous ranges (1..16), each about half the size
+ * of the one before, so that the copies of one range overlap the step of
+ * the next: with page-locked host buffers only the last, smallest range's
+ * copies add to the step's time. Results equal
+ * arc_env_step's followed by copies, world for world; the ended-world list
+ * (ARC_ENV_DONE_LIST / DONE_COUNT) is filled in range order. Synchronous:
+ * returns when the host buffers hold the results.
+ */
+int arc_env_step_host(arc_sim *s, const float *h_actions, float *h_obs, float *h_reward, unsigned char *h_terminated,
+                      unsigned char *h_truncated, int chunks);
+
 /* ArcTask.step alone (arc/task.py:155-220): no observation, no reset. */
 int arc_env_task_step(arc_sim *s, const float *d_actions, void *stream);
 /* ArcTask.observe (arc/task.py:231-259) of every world into ARC_ENV_OBS. */

@@ -85,3 +85,39 @@ def test_vec_normalize_over_the_device_env():
         assert info["terminal_observation"].abs().max() <= 10.0
     assert env.obs_rms.count == pytest.approx(count0 + 20 * n)
     assert ended  # max_steps 15: every world has ended once
+
+
+@pytest.mark.parametrize("chunks", [1, 3, 4])
+def test_host_step_in_chunks_equals_the_device_step(chunks):
+    """arc_env_step_host (actions in, observations, rewards and done flags
+    out through host buffers, the worlds stepped in ranges whose copies
+    overlap) gives, world for world and bit for bit, what arc_env_step's
+    graph gives on a twin env, through episode ends and auto-resets."""
+    import torch
+    from arc_demo_b200.torch_env import DeviceVecEnv
+
+    n, steps = 1000, 30
+    cfg = TaskConfig(curriculum=False, max_steps=12)
+    a = DeviceVecEnv(n, cfg, seed=9)
+    b = DeviceVecEnv(n, cfg, seed=9)
+    for env in (a, b):
+        env.set_levels(np.random.default_rng(2).uniform(0.0, 1.0, n))
+        env.reset()
+    torch.cuda.synchronize()
+    ended_total = 0
+    for act in ou_actions(n, steps, seed=4):
+        ho = torch.from_numpy(act).pin_memory()
+        obs, rew, term, trunc = a.step(ho.cuda(), graph=True)
+        torch.cuda.synchronize()
+        hobs, hrew, hterm, htrunc = b.step_host(ho, chunks=chunks)
+        assert torch.equal(obs.cpu(), hobs)
+        assert torch.equal(rew.cpu(), hrew)
+        assert torch.equal(term.cpu(), hterm) and torch.equal(trunc.cpu(), htrunc)
+        ca, cb = int(a.done_count.item()), int(b.done_count.item())
+        assert ca == cb
+        assert np.array_equal(np.sort(a.done_list[:ca].cpu().numpy()), np.sort(b.done_list[:cb].cpu().numpy()))
+        assert torch.equal(a.terminal_obs[term.bool() | trunc.bool()], b.terminal_obs[term.bool() | trunc.bool()])
+        ended_total += ca
+    assert ended_total >= n  # max_steps 12: every world ended at least twice
+    a.close()
+    b.close()
