@@ -380,24 +380,31 @@ def run_ours(args) -> dict | None:
 
 def run_e2e(torch, env, params, stream, K) -> dict:
     """The same loop through host buffers, with the library's host-buffer
-    step (arc_env_step_host): every step copies the actions in from pinned
-    host memory and the observations, rewards and done flags out to pinned
-    host memory, the worlds in ranges whose copies overlap the next range's
-    step; the number of ranges is the fastest of 1, 2, 3, 4 on a few steps."""
+    step (arc_env_step_host). Every step: the policy reads the last
+    observations and its actions are copied to pinned host memory (as the
+    reference's loop, whose policy runs on the host, is also timed with its
+    policy), then the step copies those actions in and the observations,
+    rewards and done flags out to pinned host memory, the worlds in ranges
+    whose copies overlap the next range's step; the number of ranges is the
+    fastest of 1, 2, 3, 4 on a few steps."""
     n = env.num_envs
     host_act = torch.empty((n, 12), dtype=torch.float32, pin_memory=True)
-    # the host-side policy's actions: the device policy's output, staged on the host
-    policy_forward(torch, params, env.obs, env.actions)
-    host_act.copy_(env.actions)
     stream.synchronize()
     torch.cuda.synchronize()
+
+    def one(chunks):
+        with torch.cuda.stream(stream):
+            policy_forward(torch, params, env.obs, env.actions)
+            host_act.copy_(env.actions, non_blocking=True)
+        stream.synchronize()
+        env.step_host(host_act, chunks)
 
     def run(chunks, k):
         t = time.perf_counter()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(k):
-            env.step_host(host_act, chunks)
+            one(chunks)
         e1.record(stream)
         e1.synchronize()
         return e0.elapsed_time(e1) / k, (time.perf_counter() - t) / k * 1e3
@@ -409,12 +416,13 @@ def run_e2e(torch, env, params, stream, K) -> dict:
     best = min(tried, key=tried.get)
     ms, wall = run(best, K)
     h2d = n * 12 * 4
-    d2h = n * 195 * 4 + n * 4 + 2 * n
+    d2h = n * 12 * 4 + n * 195 * 4 + n * 4 + 2 * n
     return {"value": round(n / (ms * 1e-3), 1), "unit": "env-steps/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": round(ms, 4), "wall_ms_per_step": round(wall, 4),
             "chunks": best, "ms_per_chunks": tried,
-            "path": "DeviceVecEnv.step_host (arc_env_step_host): pinned host actions in, observations, rewards "
-                    "and done flags out every step, synchronised every step"}
+            "path": "policy on the device, its actions to pinned host memory, then DeviceVecEnv.step_host "
+                    "(arc_env_step_host): the actions in, observations, rewards and done flags out to pinned "
+                    "host memory, synchronised every step"}
 
 
 # ---------------------------------------------------------------------------
