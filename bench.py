@@ -53,6 +53,12 @@ WARPS_DRAM_BYTES_PER_WORLD = (42.240e6 + 0.175e6) / 16384
 RENDER_METRIC = "frames/s at 640x360, 4 samples per pixel"
 RENDER_WORLDS = 256
 RENDER_W, RENDER_H, RENDER_SAMPLES = 640, 360, 4
+# Work and DRAM traffic of k_render per frame of this workload, from one ncu
+# capture of a 16-frame launch (profiles/render_640x360.md): 864.7 M warp
+# instructions, 1.56 MB read + 79.12 MB written, over 16 frames. The kernel is
+# bound by instruction issue (4 warp instructions per SM per cycle).
+RENDER_WARP_INST_PER_FRAME = 864.684e6 / 16
+RENDER_DRAM_BYTES_PER_FRAME = (1.5616e6 + 79.1224e6) / 16
 
 
 def parse():
@@ -554,6 +560,23 @@ def render_cpu_baseline(sim, markers, active) -> dict:
                       "(oracle/render_oracle.c: every column and visual tested against every ray)"}
 
 
+def render_roofline(torch, frames_per_s: float, clock: dict, frames_per_launch: int) -> dict:
+    """Issue roofline of k_render: warp instructions per second (the frames
+    rendered per second of one GPU times the instructions of a frame, from
+    ncu) against 4 per SM per cycle at the SM clock sampled during the run."""
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = clock.get("sm_mhz") or clock.get("sm_max_mhz") or 1965.0
+    peak = sms * 4 * mhz * 1e6
+    achieved = frames_per_s * RENDER_WARP_INST_PER_FRAME
+    return {"bound": "issue", "kernel": "k_render", "achieved": round(achieved / 1e12, 4),
+            "peak": round(peak / 1e12, 4), "unit": "T warp-instructions/s", "frac": round(achieved / peak, 4),
+            "traffic": round(RENDER_DRAM_BYTES_PER_FRAME * frames_per_launch),
+            "traffic_unit": f"bytes per launch of {frames_per_launch} frames (ncu, scaled from 16 frames)",
+            "peak_source": f"{sms} SMs x 4 issue slots x {mhz:.0f} MHz (median SM clock under load)",
+            "note": "no dense contraction and under 1% of HBM bandwidth: ray casting and shading are bound by "
+                    "instruction issue"}
+
+
 def run_render(args) -> dict | None:
     """Frames/s of the batched renderer: `value` device-resident (one launch
     renders every world's frame into HBM); `e2e` through the reference's
@@ -608,9 +631,6 @@ def run_render(args) -> dict | None:
         one._lib.arc_render_frame(one._ptr, sim.ptr, i, markers[i].astype(np.float64).ctypes.data, 1,
                                   int(active[i]), img.ctypes.data)
     e2e_s = max_over_ranks(torch, dist, time.perf_counter() - t)
-    peak = ctypes.c_double(0.0)
-    from arc_demo_b200.native import sim_lib
-    sim_lib().arc_probe_fp32_peak(ctypes.byref(peak), None)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -628,10 +648,7 @@ def run_render(args) -> dict | None:
                    "frames_per_launch": n, "l2": f"output {n * rays // RENDER_SAMPLES * 3 / 1e6:.0f} MB per step, "
                                                   "larger than L2"},
         "primary_rays_per_s": round(value * rays, 1),
-        "roofline": {"bound": "fp32 issue", "kernel": "k_render",
-                     "note": "no dense contraction and little memory traffic: the ray casting and shading are "
-                             "issue bound; the issue fraction comes from ncu (profiles/render_640x360.md)",
-                     "peak_fp32_tflops": round(peak.value / 1e12, 3)},
+        "roofline": render_roofline(torch, value / world, clock, n),
         "gpu_launches": 2 * K,
         "clocks": clock,
         "e2e": {"value": round(m / e2e_s, 1), "unit": "frames/s", "h2d_bytes_per_step": 4 * 4 + 8,
