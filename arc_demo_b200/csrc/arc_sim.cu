@@ -246,6 +246,9 @@ template <class R> int init_worlds(arc_sim* s)
     rc |= check(s, cudaMemset(s->sph, 0, sizeof(uint32_t) * (size_t)n * std::max(s->model.ns, 1)), "init spheres");
     rc |= check(s, cudaMemset(s->unstable, 0, sizeof(int) * n), "init flags");
     rc |= check(s, cudaMemset(s->time, 0, sizeof(double) * n), "init time");
+    // the zeroing runs on the legacy default stream, which the sim's
+    // non-blocking stream does not wait for: finish it before any kernel
+    rc |= check(s, cudaDeviceSynchronize(), "init");
     return rc ? ARC_ERR_CUDA : ARC_OK;
 }
 
@@ -1405,7 +1408,9 @@ int arc_env_init(arc_sim* s, const arc_task_config* cfg, unsigned long long seed
     // initial level / difficulty (arc/task.py:107-108)
     std::vector<double> lvl(n, c.curriculum ? 0.0 : c.difficulty);
     if (check(s, cudaMemcpy(S.level, lvl.data(), n * sizeof(double), cudaMemcpyHostToDevice), "level") ||
-        check(s, cudaMemcpy(S.difficulty, lvl.data(), n * sizeof(double), cudaMemcpyHostToDevice), "difficulty"))
+        check(s, cudaMemcpy(S.difficulty, lvl.data(), n * sizeof(double), cudaMemcpyHostToDevice), "difficulty") ||
+        // the buffers' zeroing (legacy default stream) before any kernel on the sim's stream
+        check(s, cudaDeviceSynchronize(), "env init"))
         return ARC_ERR_CUDA;
     s->env = true;
     return ARC_OK;
