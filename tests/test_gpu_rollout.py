@@ -121,3 +121,34 @@ def test_host_step_in_chunks_equals_the_device_step(chunks):
     assert ended_total >= n  # max_steps 12: every world ended at least twice
     a.close()
     b.close()
+
+
+def test_large_configuration_2048_step_rollout():
+    """The large configuration at full size: 65,536 worlds, difficulty in
+    {0, 0.1, ..., 1.0} per world, 2,048 control steps of uniform random
+    actions through the CUDA-graph step with auto-reset. Observations and
+    rewards stay finite on every step (checked on the device), and every
+    world ends an episode at least twice (max_steps 1,000)."""
+    import torch
+    from arc_demo_b200.torch_env import DeviceVecEnv
+
+    n, steps = 65536, 2048
+    env = DeviceVecEnv(n, TaskConfig(curriculum=False), seed=7)
+    env.set_levels(np.random.default_rng(7).integers(0, 11, n) / 10.0)
+    env.reset()
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(7)
+    bad = torch.zeros((), dtype=torch.bool, device="cuda")
+    ended = torch.zeros((), dtype=torch.int64, device="cuda")
+    for _ in range(steps):
+        a = torch.rand((n, 12), device="cuda", generator=gen) * 2.0 - 1.0
+        obs, rew, term, trunc = env.step(a)
+        bad |= ~(torch.isfinite(obs).all() & torch.isfinite(rew).all())
+        ended += env.done_count[0]
+    torch.cuda.synchronize()
+    assert not bool(bad.item())
+    assert int(ended.item()) >= 2 * n
+    st = env.gpu.get_state()
+    assert (st[:, 18] < 1000).all()          # no episode outlives max_steps
+    assert ((st[:, 20] >= 0.0) & (st[:, 20] <= 1.0)).all()
+    env.close()
