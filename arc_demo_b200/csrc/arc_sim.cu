@@ -7,12 +7,15 @@
 // (csrc/arc_sim.c:112-215). Errors never cross the ABI as exceptions: the
 // void calls record them (arc_sim_last_error) and print them once to stderr.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "arc_model.h"
@@ -64,6 +67,10 @@ struct arc_sim {
     double spill_cell = 0.0;
     // staging
     DevBuffer st_in, st_in2, st_in3, st_out;
+    // page-locked staging of large device-to-host copies (copy_out)
+    void* pin[2] = {nullptr, nullptr};
+    cudaEvent_t pin_ev[2] = {nullptr, nullptr};
+    std::vector<char> skip;  // observe's outputs the caller did not ask for
     std::vector<double> host_tmp;
     arc_world* hworld = nullptr;
     // task layer (arc_env_*)
@@ -268,6 +275,12 @@ void free_all(arc_sim* s)
     for (cudaEvent_t e : s->ev)
         if (e)
             cudaEventDestroy(e);
+    for (int k = 0; k < 2; ++k) {
+        if (s->pin[k])
+            cudaFreeHost(s->pin[k]);
+        if (s->pin_ev[k])
+            cudaEventDestroy(s->pin_ev[k]);
+    }
     for (cudaStream_t c : {s->copy_in, s->copy_out, s->graph_stream})
         if (c)
             cudaStreamDestroy(c);
@@ -371,6 +384,184 @@ bool ids_ok(const arc_sim* s, const int* ids, int n_ids)
 }
 
 int sync(const arc_sim* s, const char* where) { return check(s, cudaStreamSynchronize(s->stream), where); }
+
+// Host memcpy split over a few persistent threads and the caller: copying
+// from page-locked staging into the caller's (pageable) arrays is the slow
+// half of a large device-to-host transfer. One job at a time; each part
+// index carries its job's generation, so a thread still finishing one job
+// can never take a part of the next.
+class CopyPool {
+public:
+    static CopyPool& get()
+    {
+        static CopyPool pool;
+        return pool;
+    }
+    void copy(void* dst, const void* src, size_t bytes)
+    {
+        std::lock_guard<std::mutex> one_job(job_mu_);
+        if (workers_.empty() || bytes < (size_t(1) << 20)) {
+            std::memcpy(dst, src, bytes);
+            return;
+        }
+        const int parts = 4 * ((int)workers_.size() + 1);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            job_ = Job{(char*)dst, (const char*)src, bytes, parts};
+            ++gen_;
+            pending_ = parts;
+            next_.store(gen_ << 32);
+        }
+        cv_.notify_all();
+        work(gen_, job_);
+        std::unique_lock<std::mutex> lk(mu_);
+        done_cv_.wait(lk, [&] { return pending_ == 0; });
+    }
+    ~CopyPool()
+    {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (std::thread& t : workers_)
+            t.join();
+    }
+
+private:
+    struct Job {
+        char* dst;
+        const char* src;
+        size_t bytes;
+        int parts;
+    };
+    CopyPool()
+    {
+        const unsigned hc = std::thread::hardware_concurrency();
+        // besides the caller: half the host's threads, at most 7
+        const int n = std::max(0, std::min(7, (int)hc / 2 - 1));
+        for (int i = 0; i < n; ++i)
+            workers_.emplace_back([this] { loop(); });
+    }
+    void work(unsigned long long gen, Job job)
+    {
+        for (;;) {
+            unsigned long long v = next_.load();
+            if ((v >> 32) != gen || (long long)(v & 0xffffffffu) >= job.parts)
+                return;
+            if (!next_.compare_exchange_weak(v, v + 1))
+                continue;
+            const size_t p = v & 0xffffffffu;
+            const size_t a = job.bytes * p / job.parts, b = job.bytes * (p + 1) / job.parts;
+            std::memcpy(job.dst + a, job.src + a, b - a);
+            std::lock_guard<std::mutex> lk(mu_);
+            if (--pending_ == 0)
+                done_cv_.notify_all();
+        }
+    }
+    void loop()
+    {
+        unsigned long long seen = 0;
+        for (;;) {
+            Job job;
+            unsigned long long gen;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                if (stop_)
+                    return;
+                seen = gen = gen_;
+                job = job_;
+            }
+            work(gen, job);
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex job_mu_, mu_;
+    std::condition_variable cv_, done_cv_;
+    Job job_{};
+    unsigned long long gen_ = 0;
+    int pending_ = 0;
+    bool stop_ = false;
+    std::atomic<unsigned long long> next_{0};
+};
+
+constexpr size_t kPinChunk = size_t(8) << 20;  // bytes per staging buffer
+
+int ensure_staging(arc_sim* s)
+{
+    for (int k = 0; k < 2; ++k) {
+        if (!s->pin[k] && check(s, cudaMallocHost(&s->pin[k], kPinChunk), "cudaMallocHost(staging)"))
+            return ARC_ERR_CUDA;
+        if (!s->pin_ev[k] && check(s, cudaEventCreateWithFlags(&s->pin_ev[k], cudaEventDisableTiming), "event"))
+            return ARC_ERR_CUDA;
+    }
+    return ARC_OK;
+}
+
+// Device-to-host copy on the sim's stream of `n_seg` consecutive pieces of
+// the device range starting at `src` into the host arrays seg_dst[k] (which
+// may be pageable) of seg_bytes[k] bytes each, returning when they hold the
+// data. Large copies go through two page-locked buffers: the DMA of one chunk
+// overlaps the host copy of the one before, which is split over the copy
+// threads. Anything queued on the stream before runs first.
+int copy_out_pieces(const arc_sim* sc, const void* src, int n_seg, void* const* seg_dst, const size_t* seg_bytes,
+                    const char* where)
+{
+    arc_sim* s = const_cast<arc_sim*>(sc);
+    size_t bytes = 0;
+    for (int k = 0; k < n_seg; ++k)
+        bytes += seg_bytes[k];
+    if (bytes < (size_t(2) << 20)) {
+        size_t off = 0;
+        for (int k = 0; k < n_seg; ++k) {
+            if (seg_bytes[k] && check(s, cudaMemcpyAsync(seg_dst[k], (const char*)src + off, seg_bytes[k],
+                                                         cudaMemcpyDeviceToHost, s->stream),
+                                      where))
+                return ARC_ERR_CUDA;
+            off += seg_bytes[k];
+        }
+        return sync(s, where);
+    }
+    if (ensure_staging(s))
+        return ARC_ERR_CUDA;
+    const size_t chunks = (bytes + kPinChunk - 1) / kPinChunk;
+    auto issue = [&](size_t c) {
+        const size_t off = c * kPinChunk, len = std::min(kPinChunk, bytes - off);
+        return check(s, cudaMemcpyAsync(s->pin[c & 1], (const char*)src + off, len, cudaMemcpyDeviceToHost, s->stream),
+                     where) ||
+               check(s, cudaEventRecord(s->pin_ev[c & 1], s->stream), where);
+    };
+    if (issue(0))
+        return ARC_ERR_CUDA;
+    int seg = 0;
+    size_t seg_start = 0;  // offset of piece `seg` in the device range
+    for (size_t c = 0; c < chunks; ++c) {
+        // chunk c + 1 goes into the buffer whose host copy finished last round
+        if (c + 1 < chunks && issue(c + 1))
+            return ARC_ERR_CUDA;
+        if (check(s, cudaEventSynchronize(s->pin_ev[c & 1]), where))
+            return ARC_ERR_CUDA;
+        const size_t off = c * kPinChunk, end = off + std::min(kPinChunk, bytes - off);
+        // scatter [off, end) into the pieces it overlaps
+        while (seg < n_seg && seg_start + seg_bytes[seg] <= off) {
+            seg_start += seg_bytes[seg];
+            ++seg;
+        }
+        size_t ks = seg_start;  // offset of piece k
+        for (int k = seg; k < n_seg && ks < end; ks += seg_bytes[k], ++k) {
+            const size_t a = std::max(ks, off), b = std::min(ks + seg_bytes[k], end);
+            if (b > a)
+                CopyPool::get().copy((char*)seg_dst[k] + (a - ks), (const char*)s->pin[c & 1] + (a - off), b - a);
+        }
+    }
+    return ARC_OK;
+}
+
+int copy_out(const arc_sim* s, void* dst, const void* src, size_t bytes, const char* where)
+{
+    return copy_out_pieces(s, src, 1, &dst, &bytes, where);
+}
 
 template <class R> const DevModel<R>& dev_model(const arc_sim* s);
 template <> const DevModel<float>& dev_model<float>(const arc_sim* s) { return s->mf; }
@@ -539,15 +730,23 @@ void arc_sim_observe(const arc_sim* s, double* root, double* rot, double* joints
                                   joints ? dj : nullptr, contacts ? dc : nullptr, flags ? df : nullptr, s->stream);
     if (check(s, e, "observe kernel"))
         return;
-    double* devs[4] = {dr, drot, dj, dc};
-    for (int k = 0; k < 4; ++k)
-        if (outs[k] &&
-            check(s, cudaMemcpyAsync(outs[k], devs[k], sizes[k] * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
-                  "observe copy"))
-            return;
-    if (flags && check(s, cudaMemcpyAsync(flags, df, n * sizeof(int), cudaMemcpyDeviceToHost, s->stream), "flags"))
-        return;
-    sync(s, "arc_sim_observe");
+    // the five outputs lie back to back on the device: one staged copy; a
+    // NULL output's bytes go to a scratch array
+    std::vector<char>& skip = const_cast<arc_sim*>(s)->skip;
+    size_t skip_bytes = 0;
+    for (int k = 0; k < 5; ++k)
+        if (!(k < 4 ? (void*)outs[k] : (void*)flags))
+            skip_bytes = std::max(skip_bytes, sizes[k] * (k < 4 ? sizeof(double) : sizeof(int)));
+    if (skip.size() < skip_bytes)
+        skip.resize(skip_bytes);
+    void* dsts[5];
+    size_t lens[5];
+    for (int k = 0; k < 5; ++k) {
+        void* o = k < 4 ? (void*)outs[k] : (void*)flags;
+        dsts[k] = o ? o : (void*)skip.data();
+        lens[k] = sizes[k] * (k < 4 ? sizeof(double) : sizeof(int));
+    }
+    copy_out_pieces(s, d, 5, dsts, lens, "arc_sim_observe");
 }
 
 void arc_sim_heights(const arc_sim* s, const double* offsets, int k, double* out)
@@ -565,10 +764,7 @@ void arc_sim_heights(const arc_sim* s, const double* offsets, int k, double* out
                             : launch_heights<float>(view<float>(s), doff, k, dout, s->stream);
     if (check(s, e, "heights kernel"))
         return;
-    if (check(s, cudaMemcpyAsync(out, dout, sizeof(double) * (size_t)s->n * k, cudaMemcpyDeviceToHost, s->stream),
-              "heights copy"))
-        return;
-    sync(s, "arc_sim_heights");
+    copy_out(s, out, dout, sizeof(double) * (size_t)s->n * k, "heights copy");
 }
 
 void arc_sim_terrain_at(const arc_sim* s, const int* ids, const double* xy, int m, double* out)
@@ -782,10 +978,9 @@ int arc_sim_get_state(const arc_sim* s, const int* ids, int n_ids, double* out)
         return ARC_ERR_CUDA;
     cudaError_t e = s->fp64 ? launch_get_state<double>(s->md, view<double>(s), dids, n_ids, dout, s->stream)
                             : launch_get_state<float>(s->mf, view<float>(s), dids, n_ids, dout, s->stream);
-    if (check(s, e, "get_state kernel") ||
-        check(s, cudaMemcpyAsync(out, dout, sizeof(double) * ss * n_ids, cudaMemcpyDeviceToHost, s->stream), "copy"))
+    if (check(s, e, "get_state kernel"))
         return ARC_ERR_CUDA;
-    return sync(s, "arc_sim_get_state");
+    return copy_out(s, out, dout, sizeof(double) * ss * n_ids, "arc_sim_get_state");
 }
 
 int arc_sim_set_state(arc_sim* s, const int* ids, int n_ids, const double* in)

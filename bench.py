@@ -336,6 +336,9 @@ def run_ours(args) -> dict | None:
             e2e = run_e2e(torch, env, params, stream, max(3, min(K, 50)))
             e2e["ms_per_step"] = round(max_over_ranks(torch, dist, e2e["ms_per_step"]), 4)
             e2e["value"] = round(whole_job_rate(world, n, 1, e2e["ms_per_step"]), 1)
+            e2e_abi = run_e2e_reference_abi(env.sim, max(3, min(K, 20)))
+            e2e_abi["ms_per_step"] = round(max_over_ranks(torch, dist, e2e_abi["ms_per_step"]), 4)
+            e2e_abi["value"] = round(whole_job_rate(world, n, 1, e2e_abi["ms_per_step"]), 1)
 
     peak = ctypes.c_double(0.0)
     sim_lib().arc_probe_fp32_peak(ctypes.byref(peak), None)
@@ -379,6 +382,7 @@ def run_ours(args) -> dict | None:
     }
     if e2e:
         out["e2e"] = e2e
+        out["e2e_reference_abi"] = e2e_abi
     if world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(args.cpu_seconds, n)
     return out
@@ -429,6 +433,40 @@ def run_e2e(torch, env, params, stream, K) -> dict:
             "path": "policy on the device, its actions to pinned host memory, then DeviceVecEnv.step_host "
                     "(arc_env_step_host): the actions in, observations, rewards and done flags out to pinned "
                     "host memory, synchronised every step"}
+
+
+def run_e2e_reference_abi(sim, K) -> dict:
+    """The drop-in figure: the calls the reference's task layer makes on its
+    simulation every control step (arc/task.py:155-170, 231-259), through the
+    reference's C ABI with host float64 buffers: arc_sim_step with the
+    targets, arc_sim_observe and arc_sim_heights at the 143 observation
+    offsets, each synchronous like the reference's. Physics and its I/O
+    only: the task arithmetic, which the reference does in numpy, is not in
+    it."""
+    from arc_demo_b200.task import HEIGHT_OFFSETS
+    n = sim.num_worlds
+    rng = np.random.default_rng(5)
+    targets = np.ascontiguousarray(np.tile(sim.default_angles, (n, 1)) + 0.6 * rng.uniform(-1, 1, (n, 12)))
+    offsets = np.ascontiguousarray(HEIGHT_OFFSETS, dtype=np.float64)
+    heights = np.empty((n, len(offsets)))
+
+    def one():
+        sim.step(targets)
+        sim.observe()
+        sim.heights(offsets, heights)
+
+    for _ in range(2):
+        one()
+    t = time.perf_counter()
+    for _ in range(K):
+        one()
+    ms = (time.perf_counter() - t) / K * 1e3
+    h2d = n * 12 * 8 + offsets.nbytes
+    d2h = n * (13 + 9 + 36 + 6) * 8 + n * 4 + heights.nbytes
+    return {"value": round(n / (ms * 1e-3), 1), "unit": "env-steps/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": round(ms, 4),
+            "path": "arc_sim_step + arc_sim_observe + arc_sim_heights with host float64 buffers (the reference's "
+                    "C ABI, as arc/task.py calls it), wall clock, physics and its I/O only"}
 
 
 # ---------------------------------------------------------------------------

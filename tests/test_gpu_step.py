@@ -440,3 +440,25 @@ def test_small_flat_configuration_every_step(fp64):
         assert np.percentile(dq, 95) <= max(1e-5, 1.25 * np.percentile(oq, 95))
         assert np.percentile(dq, 99) <= max(5e-5, 1.25 * np.percentile(oq, 99))
         assert mism <= 0.01 * len(dx)
+
+
+def test_large_copies_through_staging_equal_small_ones():
+    """Outputs larger than 2 MB reach the caller's arrays through page-locked
+    staging and a host copy split over threads; they equal the same data
+    fetched in pieces small enough to be copied directly."""
+    n = 65536
+    g = Sim(n)
+    rng = np.random.default_rng(8)
+    g.reset(np.arange(n), rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32), rng.uniform(0, 1, n))
+    for _ in range(3):
+        g.step(np.tile(g.default_angles, (n, 1)) + 0.6 * rng.uniform(-1, 1, (n, 12)))
+    full = g.get_state()                                       # ~200 MB
+    parts = np.concatenate([g.get_state(np.arange(a, min(a + 512, n))) for a in range(0, n, 512)])
+    assert np.array_equal(full, parts)
+    root, joints, contacts, flags = g.observe()                 # 3-19 MB each, staged as one range
+    assert np.array_equal(root, full[:, :13])
+    assert np.array_equal(joints[:, :12], full[:, 13 * g.num_bodies + 8 * g.num_spheres + 1::4][:, :12])
+    # outputs the caller leaves out (NULL) are skipped, the others still filled
+    only = np.zeros_like(joints)
+    g._lib.arc_sim_observe(g.ptr, None, None, only.ctypes.data, None, None)
+    assert np.array_equal(only, joints)
