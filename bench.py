@@ -54,11 +54,11 @@ RENDER_METRIC = "frames/s at 640x360, 4 samples per pixel"
 RENDER_WORLDS = 256
 RENDER_W, RENDER_H, RENDER_SAMPLES = 640, 360, 4
 # Work and DRAM traffic of k_render per frame of this workload, from one ncu
-# capture of a 16-frame launch (profiles/render_640x360.md): 864.7 M warp
-# instructions, 1.56 MB read + 79.12 MB written, over 16 frames. The kernel is
+# capture of a 16-frame launch (profiles/render_640x360.md): 786.8 M warp
+# instructions, 1.58 MB read + 76.73 MB written, over 16 frames. The kernel is
 # bound by instruction issue (4 warp instructions per SM per cycle).
-RENDER_WARP_INST_PER_FRAME = 864.684e6 / 16
-RENDER_DRAM_BYTES_PER_FRAME = (1.5616e6 + 79.1224e6) / 16
+RENDER_WARP_INST_PER_FRAME = 786.831e6 / 16
+RENDER_DRAM_BYTES_PER_FRAME = (1.5777e6 + 76.7283e6) / 16
 
 
 def parse():
