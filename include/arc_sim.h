@@ -306,8 +306,10 @@ int arc_env_step(arc_sim *s, const float *d_actions, void *stream);
  * the next: with page-locked host buffers only the last, smallest range's
  * copies add to the step's time. Results equal
  * arc_env_step's followed by copies, world for world; the ended-world list
- * (ARC_ENV_DONE_LIST / DONE_COUNT) is filled in range order. Synchronous:
- * returns when the host buffers hold the results.
+ * (ARC_ENV_DONE_LIST / DONE_COUNT) is filled in range order. Runs after the
+ * work queued on the sim's own stream; work the caller queued on other
+ * streams (e.g. arc_env_step on its own stream) must have finished.
+ * Synchronous: returns when the host buffers hold the results.
  */
 int arc_env_step_host(arc_sim *s, const float *h_actions, float *h_obs, float *h_reward, unsigned char *h_terminated,
                       unsigned char *h_truncated, int chunks);
