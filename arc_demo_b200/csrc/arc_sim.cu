@@ -1319,8 +1319,11 @@ template <class R> int env_task_step(arc_sim* s, const float* actions, bool writ
     const Worlds<R> W = view<R>(s);
     if (check(s, cudaMemsetAsync(s->to.done_count, 0, sizeof(int), st), "memset done_count"))
         return ARC_ERR_CUDA;
-    return check(s, launch_task_step<R>(dev_model<R>(s), W, s->tp, s->ts, s->to, actions, write_obs ? 1 : 0, st),
-                  "task step kernel");
+    if (check(s, launch_task_step<R>(dev_model<R>(s), W, s->tp, s->ts, s->to, actions, write_obs ? 2 : 0, st),
+              "task step kernel"))
+        return ARC_ERR_CUDA;
+    return write_obs ? check(s, launch_task_heights<R>(dev_model<R>(s), W, s->tp, s->to, st), "task heights kernel")
+                     : ARC_OK;
 }
 
 template <class R> int env_reset_done(arc_sim* s, cudaStream_t st)
@@ -1431,8 +1434,9 @@ template <class R> int env_step_chunk(arc_sim* s, int first, int count, int c, c
     TaskOut O = s->to;
     O.done_list = s->chunk_done + first;
     O.done_count = s->chunk_count + c;
-    if (check(s, launch_task_step<R>(dev_model<R>(s), view<R>(s), s->tp, s->ts, O, s->actions, 1, st, first, count),
-              "task step kernel"))
+    if (check(s, launch_task_step<R>(dev_model<R>(s), view<R>(s), s->tp, s->ts, O, s->actions, 2, st, first, count),
+              "task step kernel") ||
+        check(s, launch_task_heights<R>(dev_model<R>(s), view<R>(s), s->tp, O, st, first, count), "task heights kernel"))
         return ARC_ERR_CUDA;
     return check(s,
                  launch_task_reset<R>(dev_model<R>(s), s->rm, view<R>(s), (TerrainGeom<R>*)s->tg, s->tgd, s->grid_of,

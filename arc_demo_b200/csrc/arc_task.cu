@@ -177,9 +177,47 @@ __device__ __forceinline__ float obs_value(double v)
 }
 
 // arc/task.py:231-259: writes the 195 observation values of world i
+// Observation entries m_begin .. m_end - 1 of the 143 terrain heights in the
+// heading frame (csrc/arc_sim.c:185-203), written to dst[m - m_begin], kChunk
+// samples at a time: their terrain loads are all issued before any is used.
+template <class R>
+__device__ void write_heights(const TaskParams& P, const Worlds<R>& W, int i, V3<double> x, Q4<double> q, float* dst,
+                              int m_begin, int m_end)
+{
+    V3<double> f = qrotate(q, V3<double>{1.0, 0.0, 0.0});
+    const double yaw = atan2(f.y, f.x), cy = cos(yaw), sy = sin(yaw);
+    const TerrainGeomD g = W.tgd[i];
+    const R* th = W.th + W.toff[i];
+    constexpr int kChunk = 8;
+    int k = 0;
+    for (int m0 = m_begin; m0 < m_end; m0 += kChunk) {
+        double h[kChunk];
+#pragma unroll
+        for (int u = 0; u < kChunk; ++u) {
+            const int m = m0 + u < m_end ? m0 + u : m_end - 1;
+            const double fo = P.offsets[m][0], lo = P.offsets[m][1];
+            const double px = x.x + cy * fo - sy * lo, py = x.y + sy * fo + cy * lo;
+            // csrc/arc_terrain.h:42-50
+            const double fx = floor((px - g.ox) / g.cell), fy = floor((py - g.oy) / g.cell);
+            const bool in = fx >= 0.0 && fy >= 0.0 && fx < g.nx && fy < g.ny;
+            const int idx = in ? (int)fx + (int)fy * g.nx : 0;
+            const double top = (double)__ldg(th + idx);
+            h[u] = in ? top : g.outside;
+        }
+#pragma unroll
+        for (int u = 0; u < kChunk; ++u) {
+            if (m0 + u >= m_end)
+                break;
+            double rel = x.z - P.stand_height - h[u];
+            rel = rel < -1.0 ? -1.0 : (rel > 1.0 ? 1.0 : rel);
+            dst[k++] = obs_value(rel);
+        }
+    }
+}
+
 template <class R>
 __device__ void write_obs(const TaskParams& P, const Worlds<R>& W, const TaskState& S, int i, const Obs64& o,
-                          float* dst)
+                          float* dst, bool heights = true)
 {
     const M3<double>& r = o.rot;
     int k = 0;
@@ -208,36 +246,9 @@ __device__ void write_obs(const TaskParams& P, const Worlds<R>& W, const TaskSta
     dst[k++] = obs_value(fwd / dist);
     dst[k++] = obs_value(left / dist);
     dst[k++] = obs_value((dist < 6.0 ? dist : 6.0) / 6.0);
-    // heights in the heading frame (csrc/arc_sim.c:185-203), kChunk samples
-    // at a time: their terrain loads are all issued before any is used
-    V3<double> f = qrotate(o.q, V3<double>{1.0, 0.0, 0.0});
-    const double yaw = atan2(f.y, f.x), cy = cos(yaw), sy = sin(yaw);
-    const TerrainGeomD g = W.tgd[i];
-    const R* th = W.th + W.toff[i];
-    constexpr int kChunk = 8;
-    for (int m0 = 0; m0 < kNumOffsets; m0 += kChunk) {
-        double h[kChunk];
-#pragma unroll
-        for (int u = 0; u < kChunk; ++u) {
-            const int m = m0 + u < kNumOffsets ? m0 + u : kNumOffsets - 1;
-            const double fo = P.offsets[m][0], lo = P.offsets[m][1];
-            const double x = o.x.x + cy * fo - sy * lo, y = o.x.y + sy * fo + cy * lo;
-            // csrc/arc_terrain.h:42-50
-            const double fx = floor((x - g.ox) / g.cell), fy = floor((y - g.oy) / g.cell);
-            const bool in = fx >= 0.0 && fy >= 0.0 && fx < g.nx && fy < g.ny;
-            const int idx = in ? (int)fx + (int)fy * g.nx : 0;
-            const double top = (double)__ldg(th + idx);
-            h[u] = in ? top : g.outside;
-        }
-#pragma unroll
-        for (int u = 0; u < kChunk; ++u) {
-            if (m0 + u >= kNumOffsets)
-                break;
-            double rel = o.x.z - P.stand_height - h[u];
-            rel = rel < -1.0 ? -1.0 : (rel > 1.0 ? 1.0 : rel);
-            dst[k++] = obs_value(rel);
-        }
-    }
+    if (heights)
+        write_heights(P, W, i, o.x, o.q, dst + k, 0, kNumOffsets);
+    k += kNumOffsets;
     for (int l = 0; l < kNumLegs; ++l)
         dst[k++] = obs_value(o.contact[l]);
 }
@@ -365,12 +376,42 @@ __global__ void k_task_step(const __grid_constant__ DevModel<R> M, Worlds<R> W, 
     }
     if (write_obs_rows && O.obs) {
         float* row = O.obs + (size_t)i * kObsSize;
-        write_obs(P, W, S, i, o, row);
+        write_obs(P, W, S, i, o, row, write_obs_rows == 1);
         if (done && O.terminal_obs) {
             float* t = O.terminal_obs + (size_t)i * kObsSize;
             for (int k = 0; k < kObsSize; ++k)
                 t[k] = row[k];
         }
+    }
+}
+
+// The observations' terrain heights of worlds first .. first + count - 1,
+// kHeightsPer samples per thread (k_task_step, with write_obs_rows == 2,
+// writes the rest of each row): the 143 samples of a world spread over nine
+// threads instead of one. Rows of worlds that ended this step get them in
+// their terminal observation too.
+constexpr int kHeightsPer = 16;
+constexpr int kHeightParts = (kNumOffsets + kHeightsPer - 1) / kHeightsPer;
+constexpr int kHeightsAt = 9 + 3 * kNumJoints + 3;  // offset of the heights in a row
+
+template <class R>
+__global__ void k_task_heights(const __grid_constant__ DevModel<R> M, Worlds<R> W, const __grid_constant__ TaskParams P,
+                               TaskOut O, int first, int count)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)count * kHeightParts)
+        return;
+    const int i = first + (int)(t / kHeightParts), part = (int)(t % kHeightParts);
+    const int m0 = part * kHeightsPer, m1 = m0 + kHeightsPer < kNumOffsets ? m0 + kHeightsPer : kNumOffsets;
+    const R* b0 = W.rec + (size_t)i * W.stride;  // the torso's pose, as read_world reads it
+    const V3<double> x{(double)b0[0], (double)b0[1], (double)b0[2]};
+    const Q4<double> q{(double)b0[3], (double)b0[4], (double)b0[5], (double)b0[6]};
+    float* row = O.obs + (size_t)i * kObsSize + kHeightsAt;
+    write_heights(P, W, i, x, q, row + m0, m0, m1);
+    if (O.terminal_obs && (O.terminated[i] | O.truncated[i])) {
+        float* t_row = O.terminal_obs + (size_t)i * kObsSize + kHeightsAt;
+        for (int m = m0; m < m1; ++m)
+            t_row[m] = row[m];
     }
 }
 
@@ -703,6 +744,19 @@ cudaError_t launch_task_step(const DevModel<R>& M, const Worlds<R>& W, const Tas
 }
 
 template <class R>
+cudaError_t launch_task_heights(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskOut& O,
+                                cudaStream_t stream, int first, int count)
+{
+    if (count < 0)
+        count = W.n - first;
+    if (count <= 0 || first < 0 || first + count > W.n)
+        return count == 0 ? cudaSuccess : cudaErrorInvalidValue;
+    const long long threads = (long long)count * kHeightParts;
+    k_task_heights<R><<<(unsigned)((threads + 127) / 128), 128, 0, stream>>>(M, W, P, O, first, count);
+    return cudaGetLastError();
+}
+
+template <class R>
 cudaError_t launch_task_observe(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskState& S,
                                 float* obs, const int* ids, int n_ids, cudaStream_t stream)
 {
@@ -770,6 +824,8 @@ cudaError_t launch_reset_warp(const ResetModel& RM, const Worlds<R>& W, TerrainG
     template cudaError_t launch_task_step<R>(const DevModel<R>&, const Worlds<R>&, const TaskParams&,            \
                                              const TaskState&, const TaskOut&, const float*, int, cudaStream_t,  \
                                              int, int);                                                          \
+    template cudaError_t launch_task_heights<R>(const DevModel<R>&, const Worlds<R>&, const TaskParams&,         \
+                                                const TaskOut&, cudaStream_t, int, int);                         \
     template cudaError_t launch_task_observe<R>(const DevModel<R>&, const Worlds<R>&, const TaskParams&,         \
                                                 const TaskState&, float*, const int*, int, cudaStream_t);        \
     template cudaError_t launch_task_reset<R>(const DevModel<R>&, const ResetModel&, const Worlds<R>&,           \

@@ -65,9 +65,15 @@ struct TaskOut {
 
 template <class R>
 // Worlds first .. first + count - 1 (count < 0: to the last world).
+// write_obs: 0 no observation rows, 1 whole rows, 2 rows without the terrain
+// heights, which launch_task_heights then writes with more threads.
 cudaError_t launch_task_step(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskState& S,
                              const TaskOut& O, const float* actions, int write_obs, cudaStream_t stream, int first = 0,
                              int count = -1);
+
+template <class R>
+cudaError_t launch_task_heights(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskOut& O,
+                                cudaStream_t stream, int first = 0, int count = -1);
 
 template <class R>
 cudaError_t launch_task_observe(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskState& S,

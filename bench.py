@@ -376,7 +376,7 @@ def run_ours(args) -> dict | None:
                      "flop_per_env_step": FLOP_PER_ENV_STEP,
                      "peak_source": "measured FP32 FMA probe (arc_probe_fp32_peak) on this GPU",
                      "hbm_gbs_algorithmic": round(n * HBM_BYTES_PER_ENV_STEP / (step_kernel_ms * 1e-3) / 1e9, 1)},
-        "gpu_launches": 3 * K,
+        "gpu_launches": 4 * K,  # step, task, terrain heights, reset of ended worlds
         "ended_in_last_step": ended,
         "clocks": clock,
     }
