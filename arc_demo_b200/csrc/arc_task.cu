@@ -180,7 +180,7 @@ __device__ __forceinline__ float obs_value(double v)
 // Observation entries m_begin .. m_end - 1 of the 143 terrain heights in the
 // heading frame (csrc/arc_sim.c:185-203), written to dst[m - m_begin], kChunk
 // samples at a time: their terrain loads are all issued before any is used.
-template <class R>
+template <int kChunk, class R>
 __device__ void write_heights(const TaskParams& P, const Worlds<R>& W, int i, V3<double> x, Q4<double> q, float* dst,
                               int m_begin, int m_end)
 {
@@ -188,7 +188,6 @@ __device__ void write_heights(const TaskParams& P, const Worlds<R>& W, int i, V3
     const double yaw = atan2(f.y, f.x), cy = cos(yaw), sy = sin(yaw);
     const TerrainGeomD g = W.tgd[i];
     const R* th = W.th + W.toff[i];
-    constexpr int kChunk = 8;
     int k = 0;
     for (int m0 = m_begin; m0 < m_end; m0 += kChunk) {
         double h[kChunk];
@@ -247,7 +246,7 @@ __device__ void write_obs(const TaskParams& P, const Worlds<R>& W, const TaskSta
     dst[k++] = obs_value(left / dist);
     dst[k++] = obs_value((dist < 6.0 ? dist : 6.0) / 6.0);
     if (heights)
-        write_heights(P, W, i, o.x, o.q, dst + k, 0, kNumOffsets);
+        write_heights<8>(P, W, i, o.x, o.q, dst + k, 0, kNumOffsets);
     k += kNumOffsets;
     for (int l = 0; l < kNumLegs; ++l)
         dst[k++] = obs_value(o.contact[l]);
@@ -388,15 +387,21 @@ __global__ void k_task_step(const __grid_constant__ DevModel<R> M, Worlds<R> W, 
 // The observations' terrain heights of worlds first .. first + count - 1,
 // kHeightsPer samples per thread (k_task_step, with write_obs_rows == 2,
 // writes the rest of each row): the 143 samples of a world spread over nine
-// threads instead of one. Rows of worlds that ended this step get them in
+// threads instead of one, four loads in flight per thread and registers sized
+// for eight blocks per SM (the kernel waits on latency: occupancy pays more
+// than loads in flight). Rows of worlds that ended this step get them in
 // their terminal observation too.
 constexpr int kHeightsPer = 16;
 constexpr int kHeightParts = (kNumOffsets + kHeightsPer - 1) / kHeightsPer;
 constexpr int kHeightsAt = 9 + 3 * kNumJoints + 3;  // offset of the heights in a row
 
+constexpr int kHeightThreads = 128;
+constexpr int kHeightBlocks = 8;
+
 template <class R>
-__global__ void k_task_heights(const __grid_constant__ DevModel<R> M, Worlds<R> W, const __grid_constant__ TaskParams P,
-                               TaskOut O, int first, int count)
+__global__ void __launch_bounds__(kHeightThreads, kHeightBlocks)
+    k_task_heights(const __grid_constant__ DevModel<R> M, Worlds<R> W, const __grid_constant__ TaskParams P, TaskOut O,
+                   int first, int count)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)count * kHeightParts)
@@ -407,7 +412,7 @@ __global__ void k_task_heights(const __grid_constant__ DevModel<R> M, Worlds<R> 
     const V3<double> x{(double)b0[0], (double)b0[1], (double)b0[2]};
     const Q4<double> q{(double)b0[3], (double)b0[4], (double)b0[5], (double)b0[6]};
     float* row = O.obs + (size_t)i * kObsSize + kHeightsAt;
-    write_heights(P, W, i, x, q, row + m0, m0, m1);
+    write_heights<4>(P, W, i, x, q, row + m0, m0, m1);
     if (O.terminal_obs && (O.terminated[i] | O.truncated[i])) {
         float* t_row = O.terminal_obs + (size_t)i * kObsSize + kHeightsAt;
         for (int m = m0; m < m1; ++m)
@@ -752,7 +757,8 @@ cudaError_t launch_task_heights(const DevModel<R>& M, const Worlds<R>& W, const 
     if (count <= 0 || first < 0 || first + count > W.n)
         return count == 0 ? cudaSuccess : cudaErrorInvalidValue;
     const long long threads = (long long)count * kHeightParts;
-    k_task_heights<R><<<(unsigned)((threads + 127) / 128), 128, 0, stream>>>(M, W, P, O, first, count);
+    k_task_heights<R><<<(unsigned)((threads + kHeightThreads - 1) / kHeightThreads), kHeightThreads, 0, stream>>>(
+        M, W, P, O, first, count);
     return cudaGetLastError();
 }
 
