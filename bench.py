@@ -143,22 +143,29 @@ class ClockSampler:
 # our arm
 
 def make_policy(torch, seed: int):
+    """Random-init MLP 195-256-256-12 (torch.nn.Linear's uniform init): the
+    weights are kept transposed (in x out) and the hidden activations in
+    buffers reused every step."""
     g = torch.Generator(device="cpu").manual_seed(seed)
 
     def lin(i, o):
         bound = 1.0 / np.sqrt(i)
         w = (torch.rand(o, i, generator=g) * 2 - 1) * bound
         b = (torch.rand(o, generator=g) * 2 - 1) * bound
-        return w.cuda().contiguous(), b.cuda().contiguous()
-    return [lin(195, 256), lin(256, 256), lin(256, 12)]
+        return w.t().contiguous().cuda(), b.cuda().contiguous()
+    return {"layers": [lin(195, 256), lin(256, 256), lin(256, 12)], "hidden": {}}
 
 
 def policy_forward(torch, params, obs, out):
     """MLP 195-256-256-12 with tanh, FP32; writes the actions into `out`."""
-    (w1, b1), (w2, b2), (w3, b3) = params
-    h = torch.tanh(torch.addmm(b1, obs, w1.t()))
-    h = torch.tanh(torch.addmm(b2, h, w2.t()))
-    torch.addmm(b3, h, w3.t(), out=out)
+    (w1, b1), (w2, b2), (w3, b3) = params["layers"]
+    n = obs.shape[0]
+    h = params["hidden"].get(n)
+    if h is None:
+        h = params["hidden"][n] = (torch.empty(n, 256, device=obs.device), torch.empty(n, 256, device=obs.device))
+    torch.addmm(b1, obs, w1, out=h[0]).tanh_()
+    torch.addmm(b2, h[0], w2, out=h[1]).tanh_()
+    torch.addmm(b3, h[1], w3, out=out)
 
 
 def autotune(env, torch, stream, candidates=("warps", "warps+queue", 8, 16), steps=4):
