@@ -89,6 +89,7 @@ struct arc_sim {
     int* iota = nullptr;
     int* chunk_done = nullptr;
     int* chunk_count = nullptr;
+    int* part_queue = nullptr;  // arc_env_step_part: a work queue (two ints) per part
     cudaStream_t copy_in = nullptr, copy_out = nullptr;
     cudaEvent_t ev[2 * 16 + 2] = {};
     mutable int err = 0;
@@ -268,7 +269,8 @@ void free_all(arc_sim* s)
     for (void* p : s->env_allocs)
         cudaFree(p);
     void* ps[] = {s->rec, s->sph, s->unstable, s->time, s->th, s->toff, s->tg, s->tgd, s->grid_of, s->spill, s->queue,
-                  s->st_in.p, s->st_in2.p, s->st_in3.p, s->st_out.p, s->iota, s->chunk_done, s->chunk_count};
+                  s->st_in.p, s->st_in2.p, s->st_in3.p, s->st_out.p, s->iota, s->chunk_done, s->chunk_count,
+                  s->part_queue};
     for (void* p : ps)
         if (p)
             cudaFree(p);
@@ -568,29 +570,33 @@ template <> const DevModel<float>& dev_model<float>(const arc_sim* s) { return s
 template <> const DevModel<double>& dev_model<double>(const arc_sim* s) { return s->md; }
 
 template <class R> cudaError_t launch_warps_if_fp32(arc_sim*, const DevModel<R>&, const Worlds<R>&, const Actuation&,
-                                                   const int*, int, cudaStream_t)
+                                                   const int*, int, int*, cudaStream_t)
 {
     return cudaErrorNotSupported;
 }
 template <> cudaError_t launch_warps_if_fp32<float>(arc_sim* s, const DevModel<float>& M, const Worlds<float>& W,
-                                                    const Actuation& A, const int* ids, int n_items, cudaStream_t st)
+                                                    const Actuation& A, const int* ids, int n_items, int* queue,
+                                                    cudaStream_t st)
 {
     return launch_step_warps(M, W, A, static_cast<float*>(s->spill), s->spill_per_lane, s->lane_cap, ids, n_items,
-                             s->use_queue ? s->queue : nullptr, st);
+                             queue, st);
 }
 
 // ids: device list of n_ids distinct worlds to step (NULL: all worlds).
 // A subset is stepped by the warp-per-leg kernel (FP32 quadruped) or the
-// plain kernel; the leg-parallel kernel steps whole batches only.
-template <class R> int step_impl(arc_sim* s, const Actuation& A, cudaStream_t st, const int* ids, int n_ids)
+// plain kernel; the leg-parallel kernel steps whole batches only. part >= 0:
+// the worlds of that part of arc_env_step_part, whose launches may run
+// beside other parts' and so take their own work queue.
+template <class R> int step_impl(arc_sim* s, const Actuation& A, cudaStream_t st, const int* ids, int n_ids, int part)
 {
+    int* queue = !s->use_queue ? nullptr : (part >= 0 ? s->part_queue + 2 * part : s->queue);
     const Worlds<R> W = view<R>(s);
     const DevModel<R>& M = dev_model<R>(s);
     const int n_items = ids ? n_ids : s->n;
     const bool warps_ok = !s->fp64 && M.leaper && s->substeps <= kFastMaxSubsteps;
     cudaError_t e;
     if (warps_ok && (s->kernel == ARC_KERNEL_WARPS || (ids && s->kernel == ARC_KERNEL_LEGS)))
-        e = launch_warps_if_fp32<R>(s, M, W, A, ids, n_items, st);
+        e = launch_warps_if_fp32<R>(s, M, W, A, ids, n_items, queue, st);
     else if (!ids && s->kernel == ARC_KERNEL_LEGS && M.leaper && s->substeps <= kFastMaxSubsteps)
         e = launch_step_fast<R>(M, W, A, static_cast<R*>(s->spill), s->spill_per_lane, s->lane_cap, s->wpc, st);
     else
@@ -598,9 +604,9 @@ template <class R> int step_impl(arc_sim* s, const Actuation& A, cudaStream_t st
     return check(s, e, "step kernel");
 }
 
-int step_any(arc_sim* s, const Actuation& A, cudaStream_t st, const int* ids = nullptr, int n_ids = 0)
+int step_any(arc_sim* s, const Actuation& A, cudaStream_t st, const int* ids = nullptr, int n_ids = 0, int part = -1)
 {
-    return s->fp64 ? step_impl<double>(s, A, st, ids, n_ids) : step_impl<float>(s, A, st, ids, n_ids);
+    return s->fp64 ? step_impl<double>(s, A, st, ids, n_ids, part) : step_impl<float>(s, A, st, ids, n_ids, part);
 }
 
 cudaStream_t stream_of(const arc_sim* s, void* stream) { return stream ? (cudaStream_t)stream : s->stream; }
@@ -1373,6 +1379,21 @@ Ranges host_ranges(int n, int chunks)
     return r;
 }
 
+// Ranges of near-equal size (whole 32-world groups where n allows): the
+// parts of arc_env_step_part.
+Ranges part_ranges(int n, int parts)
+{
+    Ranges r{};
+    r.first[0] = 0;
+    for (int c = 1; c < parts; ++c) {
+        int f = (int)std::lround((double)n * c / parts / 32.0) * 32;
+        f = std::max(f, r.first[c - 1] + 1);
+        r.first[c] = std::min(f, n - (parts - c));
+    }
+    r.first[parts] = n;
+    return r;
+}
+
 // The ended worlds of every range, range c's at chunk_done[first[c] ..],
 // gathered into done_list in range order, and their total into done_count.
 __global__ void k_merge_done(const int* __restrict__ chunk_done, const int* __restrict__ chunk_count,
@@ -1408,10 +1429,14 @@ int ensure_step_host(arc_sim* s)
     int* iota = nullptr;
     if (check(s, cudaMalloc((void**)&s->chunk_done, sizeof(int) * s->n), "cudaMalloc(chunk lists)") ||
         check(s, cudaMalloc((void**)&s->chunk_count, sizeof(int) * kMaxChunks), "cudaMalloc(chunk counts)") ||
+        check(s, cudaMalloc((void**)&s->part_queue, sizeof(int) * 2 * kMaxChunks), "cudaMalloc(part queues)") ||
         check(s, cudaMalloc((void**)&iota, sizeof(int) * s->n), "cudaMalloc(world indices)"))
         return ARC_ERR_CUDA;
     k_iota<<<(s->n + 255) / 256, 256, 0, s->stream>>>(iota, s->n);
+    // ready before any stream uses them (arc_env_step_part runs on the caller's)
     if (check(s, cudaGetLastError(), "world indices") ||
+        check(s, cudaMemsetAsync(s->part_queue, 0, sizeof(int) * 2 * kMaxChunks, s->stream), "zero part queues") ||
+        check(s, cudaStreamSynchronize(s->stream), "world indices") ||
         check(s, cudaStreamCreateWithFlags(&s->copy_in, cudaStreamNonBlocking), "copy stream") ||
         check(s, cudaStreamCreateWithFlags(&s->copy_out, cudaStreamNonBlocking), "copy stream")) {
         cudaFree(iota);
@@ -1426,10 +1451,13 @@ int ensure_step_host(arc_sim* s)
     return ARC_OK;
 }
 
-template <class R> int env_step_chunk(arc_sim* s, int first, int count, int c, cudaStream_t st)
+// One control step of worlds first .. first + count - 1 into `st`, their
+// ended worlds listed at chunk_done[first ..] with chunk_count[c] of them.
+// part >= 0: a part of arc_env_step_part (its own work queue).
+template <class R> int env_step_chunk(arc_sim* s, int first, int count, int c, cudaStream_t st, int part = -1)
 {
     Actuation A{nullptr, s->actions};
-    if (int rc = step_any(s, A, st, s->iota + first, count))
+    if (int rc = step_any(s, A, st, s->iota + first, count, part))
         return rc;
     TaskOut O = s->to;
     O.done_list = s->chunk_done + first;
@@ -1511,6 +1539,46 @@ int arc_env_step_host(arc_sim* s, const float* h_actions, float* h_obs, float* h
         check(s, cudaStreamWaitEvent(st, ev_end, 0), "wait"))
         return ARC_ERR_CUDA;
     return sync(s, "arc_env_step_host");
+}
+
+int arc_env_part_range(const arc_sim* s, int part, int parts, int* first, int* count)
+{
+    if (int rc = env_check(s))
+        return rc;
+    if (parts < 1 || parts > std::min(kMaxChunks, s->n) || part < 0 || part >= parts)
+        return fail(s, ARC_ERR_ARG, "arc_env_part_range: need 0 <= part < parts <= min(16, worlds)");
+    const Ranges R = part_ranges(s->n, parts);
+    if (first)
+        *first = R.first[part];
+    if (count)
+        *count = R.first[part + 1] - R.first[part];
+    return ARC_OK;
+}
+
+int arc_env_step_part(arc_sim* s, int part, int parts, void* stream)
+{
+    int first = 0, count = 0;
+    if (int rc = arc_env_part_range(s, part, parts, &first, &count))
+        return rc;
+    if (int rc = ensure_step_host(s))
+        return rc;
+    cudaStream_t st = stream_of(s, stream);
+    if (check(s, cudaMemsetAsync(s->chunk_count + part, 0, sizeof(int), st), "memset part count"))
+        return ARC_ERR_CUDA;
+    return s->fp64 ? env_step_chunk<double>(s, first, count, part, st, part)
+                   : env_step_chunk<float>(s, first, count, part, st, part);
+}
+
+int arc_env_merge_parts(arc_sim* s, int parts, void* stream)
+{
+    if (int rc = arc_env_part_range(s, 0, parts, nullptr, nullptr))
+        return rc;
+    if (!s->iota)
+        return fail(s, ARC_ERR_ARG, "arc_env_merge_parts: no part was stepped");
+    cudaStream_t st = stream_of(s, stream);
+    k_merge_done<<<1, 256, 0, st>>>(s->chunk_done, s->chunk_count, part_ranges(s->n, parts), parts, s->to.done_list,
+                                    s->to.done_count);
+    return check(s, cudaGetLastError(), "merge ended worlds");
 }
 
 int arc_env_init(arc_sim* s, const arc_task_config* cfg, unsigned long long seed)

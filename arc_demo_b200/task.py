@@ -109,6 +109,9 @@ def env_lib() -> ctypes.CDLL:
     d("arc_env_reset", _int, _vp, _vp, _int, _vp)
     d("arc_env_step", _int, _vp, _vp, _vp)
     d("arc_env_step_host", _int, _vp, _vp, _vp, _vp, _vp, _vp, _int)
+    d("arc_env_part_range", _int, _vp, _int, _int, ctypes.POINTER(_int), ctypes.POINTER(_int))
+    d("arc_env_step_part", _int, _vp, _int, _int, _vp)
+    d("arc_env_merge_parts", _int, _vp, _int, _vp)
     d("arc_env_task_step", _int, _vp, _vp, _vp)
     d("arc_env_observe", _int, _vp, _vp)
     d("arc_env_buffer", _int, _vp, _int, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_longlong * 2),

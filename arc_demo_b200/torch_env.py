@@ -93,6 +93,46 @@ class DeviceVecEnv:
         self.sim._check(rc)
         return self.obs, self.reward, self.terminated, self.truncated
 
+    def part_range(self, part: int, parts: int) -> tuple[int, int]:
+        """(first, count): the worlds of part `part` of `parts` (arc_env_part_range)."""
+        first, count = ctypes.c_int(), ctypes.c_int()
+        self.sim._check(self.gpu.lib.arc_env_part_range(self.sim.ptr, part, parts, ctypes.byref(first),
+                                                        ctypes.byref(count)))
+        return first.value, count.value
+
+    def step_parts(self, policy, parts: int = 4):
+        """One control step of every world in `parts` ranges, each on a stream
+        of its own: policy(part, obs, actions) writes the part's actions (obs
+        and actions are that part's rows of self.obs and self.actions), then
+        the part steps (arc_env_step_part). A part's policy so runs beside the
+        step of the parts queued before it, and its step fills the last wave
+        of theirs. The part streams start after the work queued on the current
+        stream, which waits for all of them; the ended-world list is merged
+        in part order. World for world the results equal step()'s. Returns
+        (obs, reward, terminated, truncated)."""
+        cached = getattr(self, "_parts", None)
+        if cached is None or cached[0] != parts:
+            ranges = [self.part_range(p, parts) for p in range(parts)]
+            cached = self._parts = (parts, ranges, [torch.cuda.Stream() for _ in range(parts)])
+        _, ranges, streams = cached
+        cur = torch.cuda.current_stream()
+        start = torch.cuda.Event()
+        start.record(cur)
+        ends = []
+        for p, ((first, count), st) in enumerate(zip(ranges, streams)):
+            st.wait_event(start)
+            with torch.cuda.stream(st):
+                policy(p, self.obs[first:first + count], self.actions[first:first + count])
+                self.sim._check(self.gpu.lib.arc_env_step_part(self.sim.ptr, p, parts,
+                                                               ctypes.c_void_p(stream_handle(st))))
+                end = torch.cuda.Event()
+                end.record(st)
+            ends.append(end)
+        for end in ends:
+            cur.wait_event(end)
+        self.sim._check(self.gpu.lib.arc_env_merge_parts(self.sim.ptr, parts, ctypes.c_void_p(stream_handle(cur))))
+        return self.obs, self.reward, self.terminated, self.truncated
+
     def step_host(self, actions: torch.Tensor, chunks: int = 3):
         """One control step with host tensors: actions (N x 12 float32, on
         the host, ideally pinned) in; (obs, reward, terminated, truncated)

@@ -13,9 +13,11 @@ observations, resets; plus the policy forward that produces its actions.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Prints one JSON line (rank 0). `value` is device-resident throughput (the
-step is a CUDA graph of the library's kernels on a stream shared with the
-policy); `e2e` is the same loop through the host-buffer API (actions copied
+Prints one JSON line (rank 0). `value` is device-resident throughput: either
+the policy, then the step as one CUDA graph of the library's kernels, or the
+worlds in 2 or 4 ranges on their own streams, each range's policy then its
+step (DeviceVecEnv.step_parts), whichever a short timing picks; `e2e` is the
+same loop through the host-buffer API (actions copied
 in, observations/rewards/dones copied out every step). `--impl reference`
 times the reference's own CPU path (its csrc/ built by oracle/Makefile, run
 with OpenMP on every host core) plus the task layer, on a bounded sample.
@@ -74,6 +76,8 @@ def parse():
     p.add_argument("--wpc", type=int, default=0, help="worlds per CTA (0: autotune)")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--kernel", choices=["auto", "warps"], default="auto")
+    p.add_argument("--parts", type=int, default=0,
+                   help="policy + step in this many world ranges on their own streams (0: autotune over 1, 2, 4)")
     p.add_argument("--workload", choices=["step", "render"], default="step",
                    help="step: the world step (the headline); render: frames of the headless renderer")
     p.add_argument("--render-worlds", type=int, default=RENDER_WORLDS)
@@ -213,6 +217,31 @@ def autotune(env, torch, stream, candidates=("warps", "warps+queue", 8, 16), ste
     return best, table
 
 
+def autotune_parts(env, torch, stream, one_step, candidates=(1, 2, 4), steps=6):
+    """How many world ranges the control step runs in (DeviceVecEnv.step_parts;
+    1: the policy, then the whole step as one CUDA graph), by timing whole
+    control steps, each candidate from the same world states."""
+    table = {}
+    stream.synchronize()
+    start = env.sim.get_state()
+    for parts in candidates:
+        env.sim.set_state(start)
+        torch.cuda.synchronize()
+        for _ in range(2):
+            one_step(parts)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            one_step(parts)
+        e1.record(stream)
+        e1.synchronize()
+        table[str(parts)] = round(e0.elapsed_time(e1) / steps, 4)
+    env.sim.set_state(start)
+    torch.cuda.synchronize()
+    best = min(candidates, key=lambda p: table[str(p)])
+    return best, table
+
+
 def max_over_ranks(torch, dist, x: float) -> float:
     """The largest x over all ranks, on every rank (x itself without a
     process group): multi-GPU times are the slowest rank's."""
@@ -264,14 +293,26 @@ def run_ours(args) -> dict | None:
             best_wpc, tune = "warps", None
         else:
             best_wpc, tune = autotune(env, torch, stream)
+        part_params = [{"layers": params["layers"], "hidden": {}} for _ in range(16)]  # one set per stream
+
+        def part_policy(p, obs, actions):
+            policy_forward(torch, part_params[p], obs, actions)
+
+        def one_step(parts=1):
+            if parts == 1:
+                policy_forward(torch, params, env.obs, env.actions)
+                env.step()
+            else:
+                env.step_parts(part_policy, parts)
+
+        if args.parts:
+            parts, parts_tune = args.parts, None
+        else:
+            parts, parts_tune = autotune_parts(env, torch, stream, one_step)
         env.reset()
 
-        def one_step():
-            policy_forward(torch, params, env.obs, env.actions)
-            env.step()
-
         for _ in range(max(args.warmup, 3)):
-            one_step()
+            one_step(parts)
         stream.synchronize()
         if dist:
             dist.barrier()
@@ -285,7 +326,7 @@ def run_ours(args) -> dict | None:
             t0.record(stream)
             for k in range(K):
                 starts[k].record(stream)
-                one_step()
+                one_step(parts)
                 ends[k].record(stream)
             t1.record(stream)
             t1.synchronize()
@@ -368,6 +409,11 @@ def run_ours(args) -> dict | None:
                        str(best_wpc), "leg-parallel"),
                    "worlds_per_cta": 32 if str(best_wpc).startswith("warps") else best_wpc,
                    "autotune_step_kernel_ms": tune,
+                   "parts": parts,
+                   "autotune_parts_ms_per_step": parts_tune,
+                   "loop": ("policy then env.step() (one CUDA graph) per control step" if parts == 1 else
+                            f"policy and step of {parts} world ranges, each on its own stream "
+                            "(DeviceVecEnv.step_parts), joined every control step"),
                    "l2": "inputs larger than L2 (world records + 64x64 terrains: ~1.2 GB per GPU)"},
         "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 4),
                        "p99": round(float(np.percentile(lat, 99)), 4), "max": round(float(lat.max()), 4)},
@@ -383,7 +429,9 @@ def run_ours(args) -> dict | None:
                      "flop_per_env_step": FLOP_PER_ENV_STEP,
                      "peak_source": "measured FP32 FMA probe (arc_probe_fp32_peak) on this GPU",
                      "hbm_gbs_algorithmic": round(n * HBM_BYTES_PER_ENV_STEP / (step_kernel_ms * 1e-3) / 1e9, 1)},
-        "gpu_launches": 4 * K,  # step, task, terrain heights, reset of ended worlds
+        # step, task, terrain heights, reset of ended worlds (per part), and the
+        # merge of the parts' ended-world lists
+        "gpu_launches": (4 * parts + (1 if parts > 1 else 0)) * K,
         "ended_in_last_step": ended,
         "clocks": clock,
     }

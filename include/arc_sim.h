@@ -314,6 +314,25 @@ int arc_env_step(arc_sim *s, const float *d_actions, void *stream);
 int arc_env_step_host(arc_sim *s, const float *h_actions, float *h_obs, float *h_reward, unsigned char *h_terminated,
                       unsigned char *h_truncated, int chunks);
 
+/*
+ * The control step of arc_env_step in `parts` contiguous ranges of
+ * near-equal size (1..16 parts, at most one per world), each stepped
+ * into the caller's stream: part `part` covers worlds first .. first +
+ * count - 1 (arc_env_part_range). Parts may run at the same time on
+ * different streams (each has its own work queue and ended-world list), so
+ * that a policy evaluated on one part's observations overlaps the step of
+ * another, which fills the step kernel's last, partly filled wave of
+ * blocks. Each part reads its rows of the ARC_ENV_ACTIONS buffer and writes
+ * its rows of every output; world for world the results equal
+ * arc_env_step's. Once every part of a step has been queued,
+ * arc_env_merge_parts (on a stream that waited for all parts) fills
+ * ARC_ENV_DONE_LIST / DONE_COUNT in part order. No arc_env_step_host or
+ * second set of parts may run while parts are in flight.
+ */
+int arc_env_part_range(const arc_sim *s, int part, int parts, int *first, int *count);
+int arc_env_step_part(arc_sim *s, int part, int parts, void *stream);
+int arc_env_merge_parts(arc_sim *s, int parts, void *stream);
+
 /* ArcTask.step alone (arc/task.py:155-220): no observation, no reset. */
 int arc_env_task_step(arc_sim *s, const float *d_actions, void *stream);
 /* ArcTask.observe (arc/task.py:231-259) of every world into ARC_ENV_OBS. */

@@ -123,6 +123,59 @@ def test_host_step_in_chunks_equals_the_device_step(chunks):
     b.close()
 
 
+@pytest.mark.parametrize("parts,queue", [(2, True), (4, False), (7, True)])
+def test_step_in_parts_equals_the_device_step(parts, queue):
+    """DeviceVecEnv.step_parts (each range of worlds' policy, then its step,
+    on a stream of its own, the ranges running side by side) gives, world
+    for world and bit for bit, what the policy followed by arc_env_step's
+    graph gives on a twin env, through episode ends and auto-resets. The
+    policy reads the observations, so a part whose rows were misplaced
+    would act differently from then on."""
+    import torch
+    from arc_demo_b200.native import ArcSimError
+    from arc_demo_b200.torch_env import DeviceVecEnv
+
+    n, steps = 1000, 30
+    cfg = TaskConfig(curriculum=False, max_steps=12)
+    a = DeviceVecEnv(n, cfg, seed=9)
+    b = DeviceVecEnv(n, cfg, seed=9)
+    for env in (a, b):
+        env.sim.set_work_queue(queue)
+        env.set_levels(np.random.default_rng(2).uniform(0.0, 1.0, n))
+        env.reset()
+    ranges = [b.part_range(p, parts) for p in range(parts)]
+    assert ranges[0][0] == 0 and sum(c for _, c in ranges) == n
+    assert all(f0 + c0 == f1 for (f0, c0), (f1, _) in zip(ranges, ranges[1:]))
+    torch.cuda.synchronize()
+    ended_total = 0
+    for act in ou_actions(n, steps, seed=4):
+        ou = torch.from_numpy(act).cuda()
+        torch.cuda.synchronize()
+
+        def policy(p, obs, actions):
+            first, count = ranges[p]
+            actions.copy_(torch.clamp(ou[first:first + count] + 0.3 * torch.tanh(obs[:, 9:21]), -1.0, 1.0))
+
+        a.actions.copy_(torch.clamp(ou + 0.3 * torch.tanh(a.obs[:, 9:21]), -1.0, 1.0))
+        a.step()
+        b.step_parts(policy, parts)
+        torch.cuda.synchronize()
+        assert torch.equal(a.actions, b.actions)
+        assert torch.equal(a.obs, b.obs) and torch.equal(a.reward, b.reward)
+        assert torch.equal(a.terminated, b.terminated) and torch.equal(a.truncated, b.truncated)
+        ca, cb = int(a.done_count.item()), int(b.done_count.item())
+        assert ca == cb
+        assert np.array_equal(np.sort(a.done_list[:ca].cpu().numpy()), np.sort(b.done_list[:cb].cpu().numpy()))
+        ended = a.terminated.bool() | a.truncated.bool()
+        assert torch.equal(a.terminal_obs[ended], b.terminal_obs[ended])
+        ended_total += ca
+    assert ended_total >= n  # max_steps 12: every world ended at least twice
+    with pytest.raises(ArcSimError):
+        b.part_range(0, 17)  # at most 16 parts
+    a.close()
+    b.close()
+
+
 def test_large_configuration_2048_step_rollout():
     """The large configuration at full size: 65,536 worlds, difficulty in
     {0, 0.1, ..., 1.0} per world, 2,048 control steps of uniform random
