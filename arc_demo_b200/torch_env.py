@@ -3,7 +3,8 @@
 `DeviceVecEnv` runs ArcVecEnv.step_wait's work (arc/env.py:99-117) on the GPU:
 actuation, physics, rewards, terminations, checkpoints, curriculum,
 observations and the auto-reset of ended worlds, in one CUDA graph per
-control step. Observations, rewards and done flags are torch tensors that
+control step (or, with step_parts, in ranges of worlds on side-by-side
+streams, each after its share of the policy). Observations, rewards and done flags are torch tensors that
 alias the library's device buffers through DLPack: no copies, no host
 round trip. Torch is only the consumer here; the step itself is the
 library's CUDA kernels.
@@ -104,9 +105,10 @@ class DeviceVecEnv:
         """One control step of every world in `parts` ranges, each on a stream
         of its own: policy(part, obs, actions) writes the part's actions (obs
         and actions are that part's rows of self.obs and self.actions), then
-        the part steps (arc_env_step_part). A part's policy so runs beside the
-        step of the parts queued before it, and its step fills the last wave
-        of theirs. The part streams start after the work queued on the current
+        the part steps (arc_env_step_part). A part's policy starts once the
+        policy of the part before it has finished, so it runs beside that
+        part's step, and its own step fills the last wave of the steps before
+        it. The part streams start after the work queued on the current
         stream, which waits for all of them; the ended-world list is merged
         in part order. World for world the results equal step()'s. Returns
         (obs, reward, terminated, truncated)."""
@@ -118,11 +120,15 @@ class DeviceVecEnv:
         cur = torch.cuda.current_stream()
         start = torch.cuda.Event()
         start.record(cur)
-        ends = []
+        ends, acted = [], None
         for p, ((first, count), st) in enumerate(zip(ranges, streams)):
             st.wait_event(start)
+            if acted is not None:
+                st.wait_event(acted)
             with torch.cuda.stream(st):
                 policy(p, self.obs[first:first + count], self.actions[first:first + count])
+                acted = torch.cuda.Event()
+                acted.record(st)
                 self.sim._check(self.gpu.lib.arc_env_step_part(self.sim.ptr, p, parts,
                                                                ctypes.c_void_p(stream_handle(st))))
                 end = torch.cuda.Event()

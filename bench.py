@@ -167,9 +167,11 @@ def policy_forward(torch, params, obs, out):
     h = params["hidden"].get(n)
     if h is None:
         h = params["hidden"][n] = (torch.empty(n, 256, device=obs.device), torch.empty(n, 256, device=obs.device))
-    torch.addmm(b1, obs, w1, out=h[0]).tanh_()
-    torch.addmm(b2, h[0], w2, out=h[1]).tanh_()
-    torch.addmm(b3, h[1], w3, out=out)
+    # x @ W, then + b in place: the same numbers as addmm, without the
+    # separate bias kernel cuBLAS adds to its FP32 (non-tensor) GEMMs
+    torch.mm(obs, w1, out=h[0]).add_(b1).tanh_()
+    torch.mm(h[0], w2, out=h[1]).add_(b2).tanh_()
+    torch.mm(h[1], w3, out=out).add_(b3)
 
 
 def autotune(env, torch, stream, candidates=("warps", "warps+queue", 8, 16), steps=4):
