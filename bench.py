@@ -581,13 +581,22 @@ def reference_loop(n: int, seconds: float | None, steps: int | None, warmup: int
 
 
 def cpu_baseline(seconds: float, full_n: int) -> dict:
+    import torch
     threads = os.cpu_count() or 1
+    torch_threads = torch.get_num_threads()
     sample_n = 4096
     r = reference_loop(sample_n, seconds, None, 2, threads)
+    # the same loop on one thread (OpenMP and torch), a shorter sample
+    one_n = 1024
+    r1 = reference_loop(one_n, seconds / 3, None, 1, 1)
+    torch.set_num_threads(torch_threads)
     return {"value": round(r["value"], 1), "unit": "env-steps/s", "cores": threads, "kind": "reference",
             "sample": f"{sample_n} of the {full_n} worlds (same difficulty mix), {r['steps']} control steps "
                       f"in {r['seconds']:.1f} s: reference csrc/ step+observe+heights with OpenMP x{threads}, "
-                      "numpy task layer with auto-reset, MLP policy in torch on the host"}
+                      "numpy task layer with auto-reset, MLP policy in torch on the host",
+            "single_thread": {"value": round(r1["value"], 1), "unit": "env-steps/s", "cores": 1,
+                              "sample": f"{one_n} worlds, {r1['steps']} control steps in {r1['seconds']:.1f} s, "
+                                        "OpenMP and torch on one thread"}}
 
 
 def run_reference(args) -> dict | None:
