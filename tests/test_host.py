@@ -1,5 +1,6 @@
 """Host-side logic that needs no GPU: the serving load generator's request
-shapes and the serving engine's per-slot byte count."""
+shapes, the serving engine's per-slot byte count, and the task weights'
+balance."""
 
 import math
 
@@ -24,3 +25,13 @@ def test_state_budget_holds_about_1_8_million_worlds():
     # 40 GB of FP32 worlds with 64 x 64 terrains: the serving configuration
     assert 20_000 < WORLD_BYTES < 23_000
     assert math.isclose(40e9 / WORLD_BYTES, 1.84e6, rel_tol=0.02)
+
+
+def test_no_reward_for_ending_episodes_on_purpose():
+    """tests/test_env.py:148-153 of the reference: under PPO's discount,
+    standing still forever costs less than falling once (the task weights
+    are the reference's, arc/task.py:17-66)."""
+    from arc_demo_b200.task import TaskConfig
+    cfg = TaskConfig()
+    gamma = 0.99
+    assert cfg.w_time / (1 - gamma) < cfg.w_fall
