@@ -3,8 +3,11 @@
 nvcc compiles every .cu under csrc/ for sm_100a only (no other targets, no
 PTX fallback) and links them with the static CUDA runtime into one shared
 library with a plain C ABI (include/arc_sim.h). Objects go to _build/.
+build(checked=True) makes the checked build, libarcsim_checked.so (objects
+in _build_checked/): the same sources with ARC_DEVICE_CHECKS, whose kernels
+test their data-dependent indexes (csrc/arc_checks.cuh).
 
-    python -m arc_demo_b200.build          # or: python arc_demo_b200/build.py
+    python -m arc_demo_b200.build          # or: python arc_demo_b200/build.py [-f] [--checked]
 """
 
 from __future__ import annotations
@@ -20,6 +23,8 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 LIB = HERE / "libarcsim.so"
+BUILD_CHECKED = HERE / "_build_checked"
+LIB_CHECKED = HERE / "libarcsim_checked.so"
 # the reference loads its renderer from a second library (arc/native.py:59-70);
 # this one only depends on libarcsim.so, which exports the arc_render_* calls
 RENDER_LIB = HERE / "libarcrender.so"
@@ -56,13 +61,14 @@ def _stale(obj: Path, src: Path) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False, extra: list[str] | None = None) -> Path:
-    BUILD.mkdir(exist_ok=True)
+def build(verbose: bool = False, force: bool = False, extra: list[str] | None = None, checked: bool = False) -> Path:
+    build_dir, lib = (BUILD_CHECKED, LIB_CHECKED) if checked else (BUILD, LIB)
+    build_dir.mkdir(exist_ok=True)
     cc = nvcc()
-    extra = extra or []
+    extra = (extra or []) + (["-DARC_DEVICE_CHECKS"] if checked else [])
     jobs = []
     for src in sources():
-        obj = BUILD / (src.stem + ".o")
+        obj = build_dir / (src.stem + ".o")
         if force or _stale(obj, src):
             jobs.append([cc, *ARCH, *FLAGS, *FILE_FLAGS.get(src.name, []), *extra, "-c", str(src), "-o", str(obj)])
 
@@ -76,9 +82,11 @@ def build(verbose: bool = False, force: bool = False, extra: list[str] | None = 
 
     with ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as ex:
         list(ex.map(run, jobs))
-    objs = [str(BUILD / (s.stem + ".o")) for s in sources()]
-    if jobs or not LIB.exists():
-        run([cc, *ARCH, "-shared", "-o", str(LIB), *objs, "-lcudart_static", "-lrt", "-ldl", "-lpthread"])
+    objs = [str(build_dir / (s.stem + ".o")) for s in sources()]
+    if jobs or not lib.exists():
+        run([cc, *ARCH, "-shared", "-o", str(lib), *objs, "-lcudart_static", "-lrt", "-ldl", "-lpthread"])
+    if checked:
+        return lib
     if jobs or not RENDER_LIB.exists():
         cxx = shutil.which("gcc") or "gcc"
         run([cxx, "-shared", "-fPIC", "-o", str(RENDER_LIB), "-x", "c", os.devnull, f"-L{HERE}",
@@ -87,5 +95,4 @@ def build(verbose: bool = False, force: bool = False, extra: list[str] | None = 
 
 
 if __name__ == "__main__":
-    build(verbose="-v" in sys.argv, force="-f" in sys.argv)
-    print(LIB)
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv, checked="--checked" in sys.argv))

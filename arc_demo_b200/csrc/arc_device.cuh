@@ -68,12 +68,43 @@ template <class R> struct Worlds {
     const TerrainGeom<R>* tg;
     const TerrainGeomD* tgd;
     int n;
+#ifdef ARC_DEVICE_CHECKS
+    const int* grid_of = nullptr;  // terrain capacity of each world: grid_of[i]^2 columns
+#endif
 };
+
+// Columns of world i's slice of the terrain pool (checked build; -1: unknown)
+template <class R> ARC_HD long long terrain_cap(const Worlds<R>& W, int i)
+{
+#ifdef ARC_DEVICE_CHECKS
+    return W.grid_of ? (long long)W.grid_of[i] * W.grid_of[i] : -1;
+#else
+    return -1;
+#endif
+}
+
+// Whether column c lies in world i's slice of the terrain pool: always in
+// the regular build, checked (and recorded under `site` when not) in the
+// checked build.
+template <class R> ARC_HD bool terrain_column_ok(const Worlds<R>& W, int i, long long c, int site)
+{
+#ifdef ARC_DEVICE_CHECKS
+    const long long cap = terrain_cap(W, i);
+    return cap < 0 || ARC_IN_BOUNDS(c, cap, site);
+#else
+    (void)W, (void)i, (void)c, (void)site;
+    return true;
+#endif
+}
 
 template <class R> ARC_HD TerrainView<R> terrain_of(const Worlds<R>& W, int i)
 {
     TerrainGeom<R> g = W.tg[i];
-    return TerrainView<R>{W.th + W.toff[i], g.nx, g.ny, g.cell, g.ox, g.oy, g.outside};
+    TerrainView<R> v{W.th + W.toff[i], g.nx, g.ny, g.cell, g.ox, g.oy, g.outside};
+#ifdef ARC_DEVICE_CHECKS
+    v.cap = terrain_cap(W, i);
+#endif
+    return v;
 }
 
 // How a step kernel gets its drive targets.

@@ -66,6 +66,8 @@ template <class R> __device__ __forceinline__ double terrain_height_d(const Worl
     double fx = floor((x - g.ox) / g.cell), fy = floor((y - g.oy) / g.cell);
     if (!(fx >= 0.0 && fy >= 0.0 && fx < g.nx && fy < g.ny))
         return g.outside;
+    if (!terrain_column_ok(W, i, (int)fx + (long long)(int)fy * g.nx, kCheckHeightsRead))
+        return g.outside;
     return (double)W.th[W.toff[i] + (int)fx + (int)fy * g.nx];
 }
 
@@ -253,6 +255,8 @@ __global__ void k_reset(const __grid_constant__ ResetModel RM, Worlds<R> W, Terr
     tgd[i] = g;
     tg[i] = TerrainGeom<R>{n, n, (R)g.cell, (R)g.ox, (R)g.oy, (R)g.outside};
     R* h = W.th + W.toff[i];
+    if (!terrain_column_ok(W, i, (long long)n * n - 1, kCheckTerrainWrite))
+        return;
 
     const double reach = RM.footprint + 0.1, step = 0.5 * cell;
     bool out_x = false, out_y = false;
@@ -370,7 +374,7 @@ __global__ void k_set_terrain(Worlds<R> W, TerrainGeom<R>* tg, TerrainGeomD* tgd
         tgd[id] = g;
         tg[id] = TerrainGeom<R>{nx, ny, (R)g.cell, (R)g.ox, (R)g.oy, (R)g.outside};
     }
-    if (t < nx * ny)
+    if (t < nx * ny && terrain_column_ok(W, id, t, kCheckTerrainWrite))
         W.th[W.toff[id] + t] = (R)heights[t];
 }
 

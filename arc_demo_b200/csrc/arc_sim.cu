@@ -135,6 +135,24 @@ void* grow(const arc_sim* sc, DevBuffer& b, size_t bytes)
     return b.p;
 }
 
+#ifdef ARC_DEVICE_CHECKS
+}  // namespace
+namespace arc {
+// the readers of every translation unit's check record (arc_checks.cuh)
+std::vector<int (*)(unsigned long long*, bool)>& device_check_readers()
+{
+    static std::vector<int (*)(unsigned long long*, bool)> readers;
+    return readers;
+}
+int register_device_checks(int (*read)(unsigned long long* record, bool clear))
+{
+    device_check_readers().push_back(read);
+    return 1;
+}
+}  // namespace arc
+namespace {
+#endif
+
 template <class R> Worlds<R> view(const arc_sim* s)
 {
     Worlds<R> w;
@@ -150,6 +168,9 @@ template <class R> Worlds<R> view(const arc_sim* s)
     w.tg = static_cast<const TerrainGeom<R>*>(s->tg);
     w.tgd = s->tgd;
     w.n = s->n;
+#ifdef ARC_DEVICE_CHECKS
+    w.grid_of = s->grid_of;
+#endif
     return w;
 }
 
@@ -1212,6 +1233,38 @@ int arc_sim_set_work_queue(arc_sim* s, int on)
 {
     s->use_queue = on != 0;
     return ARC_OK;
+}
+
+int arc_device_checks(unsigned long long* failures, int* first_site, long long* first_index, int clear)
+{
+    unsigned long long total = 0;
+    int site = 0;
+    long long index = 0;
+#ifdef ARC_DEVICE_CHECKS
+    for (auto read : arc::device_check_readers()) {
+        unsigned long long r[3];
+        if (read(r, clear != 0))
+            return ARC_ERR_CUDA;
+        total += r[0];
+        if (r[0] && !site) {
+            site = (int)r[1];
+            index = (long long)r[2];
+        }
+    }
+#else
+    (void)clear;
+#endif
+    if (failures)
+        *failures = total;
+    if (first_site)
+        *first_site = site;
+    if (first_index)
+        *first_index = index;
+#ifdef ARC_DEVICE_CHECKS
+    return 1;
+#else
+    return 0;
+#endif
 }
 
 arc_sim* arc_sim_create_sized(int n_worlds, const int* grids, double dt, int substeps, double cell, unsigned flags)

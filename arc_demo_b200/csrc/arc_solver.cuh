@@ -15,6 +15,8 @@
 #include <cstdint>
 #include <cmath>
 
+#include "arc_checks.cuh"
+
 #ifdef __CUDACC__
 #define ARC_HD __host__ __device__ __forceinline__
 #else
@@ -541,12 +543,19 @@ template <class R> struct TerrainView {
     const R* h;
     int nx, ny;
     R cell, ox, oy, outside;
+#ifdef ARC_DEVICE_CHECKS
+    long long cap = -1;  // columns of the world's slice of the pool (< 0: unchecked)
+#endif
 };
 
 template <class R> ARC_HD R terrain_cell(const TerrainView<R>& t, int ix, int iy)
 {
     if (ix < 0 || iy < 0 || ix >= t.nx || iy >= t.ny)
         return t.outside;
+#ifdef ARC_DEVICE_CHECKS
+    if (t.cap >= 0 && !ARC_IN_BOUNDS(ix + (long long)iy * t.nx, t.cap, kCheckTerrainRead))
+        return t.outside;
+#endif
 #ifdef __CUDA_ARCH__
     return __ldg(t.h + ix + iy * t.nx);
 #else

@@ -273,7 +273,9 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
                     SphereState<R> ss{V3<R>{a[0], a[1], a[2]}, V3<R>{a[3], a[4], a[5]}, (int)((anch >> it) & 1u)};
                     const int t = collide_sphere(P, sm.body[b], xp, qp, sk, ss, T, st, [&](V3<R> local, V3<R> n) {
                         R* dst = nc < kOnChip ? con + nc * kCRec
-                                              : (nc < lane_cap ? spl + (size_t)(nc - kOnChip) * kCRec : nullptr);
+                                 : (nc < lane_cap && ARC_IN_BOUNDS(nc - kOnChip, spill_per_lane, kCheckSpillWrite))
+                                     ? spl + (size_t)(nc - kOnChip) * kCRec
+                                     : nullptr;
                         if (dst) {
                             dst[0] = local.x; dst[1] = local.y; dst[2] = local.z;
                             dst[3] = n.x; dst[4] = n.y; dst[5] = n.z;
@@ -341,6 +343,8 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
         if (active) {
             const int ncl = nc < lane_cap ? nc : lane_cap;
             for (int c = 0; c < ncl && base + c < kMaxContacts; ++c) {
+                if (c >= kOnChip && !ARC_IN_BOUNDS(c - kOnChip, spill_per_lane, kCheckSpillRead))
+                    continue;
                 const R* src = c < kOnChip ? con + c * kCRec : spl + (size_t)(c - kOnChip) * kCRec;
                 ContactRec<R> cr{V3<R>{src[0], src[1], src[2]}, V3<R>{src[3], src[4], src[5]}};
                 const int b = (int)src[6];

@@ -456,7 +456,7 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
                     setv(d, 0, local);
                     setv(d, 3, n);
                     d[6] = (F)body;
-                } else if (nc < lane_cap) {
+                } else if (nc < lane_cap && ARC_IN_BOUNDS(nc - kOnChip, spill_per_lane, kCheckSpillWrite)) {
                     F* d = spill + (((size_t)wi * kWarps + leg) * (size_t)spill_per_lane + (nc - kOnChip)) * 8;
                     d[0] = local.x; d[1] = local.y; d[2] = local.z;
                     d[3] = n.x; d[4] = n.y; d[5] = n.z;
@@ -612,6 +612,8 @@ k_step_warps(const __grid_constant__ DevModel<F> M, Worlds<F> W, Actuation A, F*
                                 for (int f = 0; f < 7; ++f)
                                     rc[f] = sm.con[leg][c * 7 + f][j];
                             } else {
+                                if (!ARC_IN_BOUNDS(c - kOnChip, spill_per_lane, kCheckSpillRead))
+                                    continue;
                                 const F* src =
                                     spill + (((size_t)wi * kWarps + leg) * (size_t)spill_per_lane + (c - kOnChip)) * 8;
 #pragma unroll

@@ -151,6 +151,8 @@ template <class R> __device__ __forceinline__ double height_at(const Worlds<R>& 
     double fx = floor((x - g.ox) / g.cell), fy = floor((y - g.oy) / g.cell);
     if (!(fx >= 0.0 && fy >= 0.0 && fx < g.nx && fy < g.ny))
         return g.outside;
+    if (!terrain_column_ok(W, i, (int)fx + (long long)(int)fy * g.nx, kCheckHeightsRead))
+        return g.outside;
     return (double)W.th[W.toff[i] + (int)fx + (int)fy * g.nx];
 }
 
@@ -198,7 +200,8 @@ __device__ void write_heights(const TaskParams& P, const Worlds<R>& W, int i, V3
             const double px = x.x + cy * fo - sy * lo, py = x.y + sy * fo + cy * lo;
             // csrc/arc_terrain.h:42-50
             const double fx = floor((px - g.ox) / g.cell), fy = floor((py - g.oy) / g.cell);
-            const bool in = fx >= 0.0 && fy >= 0.0 && fx < g.nx && fy < g.ny;
+            const bool in = fx >= 0.0 && fy >= 0.0 && fx < g.nx && fy < g.ny &&
+                            terrain_column_ok(W, i, (int)fx + (long long)(int)fy * g.nx, kCheckHeightsRead);
             const int idx = in ? (int)fx + (int)fy * g.nx : 0;
             const double top = (double)__ldg(th + idx);
             h[u] = in ? top : g.outside;
@@ -519,6 +522,8 @@ __device__ void reset_world_warp(ResetSmem& sm, const ResetModel& RM, const Worl
     const int L = rough ? m1 * m1 + m2 * m2 : 0;
     const int J = rough ? n * n : 0;
     R* h = W.th + W.toff[i];
+    if (!terrain_column_ok(W, i, (long long)n * n - 1, kCheckTerrainWrite))
+        return;  // the whole warp: n and the slice are the world's
     // the raw jitter draw of column c sits in the low word of h[c] until the
     // column's height replaces it
     uint32_t* hdraw = reinterpret_cast<uint32_t*>(h);

@@ -14,13 +14,16 @@ from __future__ import annotations
 
 import ctypes
 import functools
+import os
 import re
 from pathlib import Path
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-LIB_PATH = HERE / "libarcsim.so"
+# ARC_SIM_LIB selects another build of the library, e.g. the checked build
+# libarcsim_checked.so (arc_demo_b200/build.py)
+LIB_PATH = Path(os.environ["ARC_SIM_LIB"]) if os.environ.get("ARC_SIM_LIB") else HERE / "libarcsim.so"
 HEADER = HERE.parent / "include" / "arc_sim.h"
 
 _f64 = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -100,7 +103,20 @@ def sim_lib() -> ctypes.CDLL:
     d("arc_sim_create_sized", _vp, _int, _i32, _dbl, _int, _dbl, _uint)
     d("arc_sim_step_ids", _int, _vp, _vp, _int, _vp, _vp, _vp)
     d("arc_sim_set_work_queue", _int, _vp, _int)
+    d("arc_device_checks", _int, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(_int),
+      ctypes.POINTER(ctypes.c_longlong), _int)
     return lib
+
+
+def device_checks(clear: bool = False) -> dict:
+    """The loaded library's record of failed index checks (arc_device_checks):
+    whether it is the checked build, how many checks failed since the last
+    clear, and the site and index of the first."""
+    failures, site, index = ctypes.c_ulonglong(), _int(), ctypes.c_longlong()
+    rc = sim_lib().arc_device_checks(ctypes.byref(failures), ctypes.byref(site), ctypes.byref(index), int(clear))
+    if rc < 0:
+        raise ArcSimError(f"arc_device_checks failed: {rc}")
+    return {"checked": rc == 1, "failures": failures.value, "site": site.value, "index": index.value}
 
 
 def header_symbols() -> list[str]:

@@ -195,6 +195,18 @@ int arc_sim_observe_ids(const arc_sim *s, const int *d_ids, int n_ids, double *r
  * groups of 32 worlds from a device work queue, instead of one CTA per group */
 int arc_sim_set_work_queue(arc_sim *s, int on);
 
+/* The checked build (libarcsim_checked.so, compiled with ARC_DEVICE_CHECKS)
+ * tests the kernels' data-dependent indexes - terrain columns against their
+ * world's slice of the terrain pool, contact records against their lane's
+ * slice of the spill buffer - and skips an access that fails, recording it.
+ * This call reads the record of every kernel of the library: the number of
+ * failed checks since the last clear, the site of the first (1 terrain read
+ * in a step, 2/3 contact spill write/read, 4 observation height or terrain
+ * lookup, 5 terrain write of a reset) and its index; clear != 0 zeroes the
+ * record. Returns 1 for the checked build, 0 for the regular build (which
+ * checks nothing and reports zeros), < 0 on a CUDA error. */
+int arc_device_checks(unsigned long long *failures, int *first_site, long long *first_index, int clear);
+
 /* Measured FP32 FMA throughput of the current device (FLOP/s, an FMA
  * counted as 2): the roofline denominator of the step kernels. */
 int arc_probe_fp32_peak(double *flops_per_s, double *seconds);

@@ -6,7 +6,7 @@ import subprocess
 import pytest
 
 from arc_demo_b200 import native
-from arc_demo_b200.build import LIB, build
+from arc_demo_b200.build import LIB, LIB_CHECKED, build
 
 # the reference's batched API (csrc/arc_sim.h:25-56), bound by arc/native.py:38-55
 REFERENCE_SYMBOLS = [
@@ -37,6 +37,26 @@ def test_library_exports_every_declared_symbol(lib):
     assert not missing, missing
     for s in native.header_symbols():
         getattr(lib, s)
+
+
+def test_checked_build_exports_the_same_abi():
+    """libarcsim_checked.so (the kernels testing their indexes) is a drop-in
+    for libarcsim.so: every declared symbol, and it says it is the checked
+    build only through arc_device_checks, which needs a device."""
+    if not LIB_CHECKED.exists():
+        build(checked=True)
+    out = subprocess.run(["nm", "-D", "--defined-only", str(LIB_CHECKED)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    missing = [s for s in native.header_symbols() if s not in exported]
+    assert not missing, missing
+
+
+def test_regular_build_checks_nothing():
+    """The regular build compiles the index checks away: arc_device_checks
+    reports 0 (not the checked build) and no failures, without a device."""
+    record = native.device_checks()
+    assert not record["checked"] and record["failures"] == 0
 
 
 def test_constants_without_a_device(lib):
