@@ -317,7 +317,9 @@ int arc_env_step(arc_sim *s, const float *d_actions, void *stream);
  * of the one before, so that the copies of one range overlap the step of
  * the next: with page-locked host buffers only the last, smallest range's
  * copies add to the step's time. Results equal
- * arc_env_step's followed by copies, world for world; the ended-world list
+ * arc_env_step's followed by copies, world for world (with the leg-parallel
+ * kernel selected, ranges step on the warp-per-leg kernel, which agrees with
+ * it to FP32 rounding rather than bit for bit); the ended-world list
  * (ARC_ENV_DONE_LIST / DONE_COUNT) is filled in range order. Runs after the
  * work queued on the sim's own stream; work the caller queued on other
  * streams (e.g. arc_env_step on its own stream) must have finished.
@@ -336,7 +338,8 @@ int arc_env_step_host(arc_sim *s, const float *h_actions, float *h_obs, float *h
  * another, which fills the step kernel's last, partly filled wave of
  * blocks. Each part reads its rows of the ARC_ENV_ACTIONS buffer and writes
  * its rows of every output; world for world the results equal
- * arc_env_step's. Once every part of a step has been queued,
+ * arc_env_step's (the same caveat for the leg-parallel kernel as
+ * arc_env_step_host's). Once every part of a step has been queued,
  * arc_env_merge_parts (on a stream that waited for all parts) fills
  * ARC_ENV_DONE_LIST / DONE_COUNT in part order. No arc_env_step_host or
  * second set of parts may run while parts are in flight.
