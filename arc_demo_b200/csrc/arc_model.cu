@@ -1,4 +1,6 @@
 // arc_model.cu - host construction of the robot template (FP64).
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include "arc_model.h"
 
@@ -381,5 +383,27 @@ ResetModel make_reset_model(const ModelHost& m)
 
 template DevModel<float> make_dev_model<float>(const ModelHost&, double, int, double);
 template DevModel<double> make_dev_model<double>(const ModelHost&, double, int, double);
+
+// Upper bound of the contacts one lane of the leg-parallel kernel records in
+// a substep: a sphere of radius r touches at most (floor(2r/cell)+2)^2
+// columns, one contact each.
+int lane_contact_bound(const ModelHost& m, double cell)
+{
+    if (!m.leaper)
+        return 0;
+    int worst = 0;
+    for (int leg = 0; leg < kNumLegs; ++leg) {
+        long long sum = 0;
+        for (int it = 0; it < 6; ++it) {
+            int s = it == 0 ? (leg == 0 ? 0 : -1) : 5 * leg + it;
+            if (s < 0)
+                continue;
+            long long per = (long long)std::floor(2.0 * m.s[s].radius / cell) + 2;
+            sum += per * per;
+        }
+        worst = (int)std::max<long long>(worst, std::min<long long>(sum, kMaxContacts));
+    }
+    return worst;
+}
 
 }  // namespace arc

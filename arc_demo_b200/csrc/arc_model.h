@@ -76,6 +76,11 @@ void build_leaper(ModelHost& m);
 // femurs and tibias only.
 bool is_leaper_topology(const ModelHost& m);
 
+// Upper bound of the contact records one lane of the leg-parallel kernel
+// (one leg: its five spheres, and the torso's for leg 0) can make in one
+// substep on columns of the given cell size (0 for other topologies).
+int lane_contact_bound(const ModelHost& m, double cell);
+
 // What the renderer reads of an arc_sim (arc_sim.cu owns the struct).
 struct SimView {
     const ModelHost* model;

@@ -31,8 +31,9 @@ constexpr int kNoAllocGridMax = kGridMax;
 // = 343 floats, padded to 16 bytes
 constexpr int kRecStride = 344;
 constexpr int kSnap = 13 * 13 + 21 * 8 + 12 * 4 + 2;  // 387 doubles per world
-// contact records one lane may spill beyond its on-chip ones: the bound for
-// cells of at least 0.4 m (the reference's default grid, csrc/arc_sim.c:36)
+// contact records one lane may spill beyond its two on-chip ones: the
+// quadruped's bound for cells of at least 0.4 m (the reference's default
+// cell, arc/task.py:22-23) is 29 records per lane
 constexpr int kSpillPerLane = 28;
 constexpr double kMinCell = 0.4;
 
@@ -45,8 +46,15 @@ constexpr size_t kOffToff = align256(kOffTime + sizeof(double) * kNoAllocMaxWorl
 constexpr size_t kOffTg = align256(kOffToff + sizeof(long long) * kNoAllocMaxWorlds);
 constexpr size_t kOffTgd = align256(kOffTg + sizeof(TerrainGeom<float>) * kNoAllocMaxWorlds);
 constexpr size_t kOffSpill = align256(kOffTgd + sizeof(TerrainGeomD) * kNoAllocMaxWorlds);
-constexpr size_t kScratchBytes =
-    align256(kOffSpill + sizeof(float) * (size_t)kNoAllocMaxWorlds * 4 * kSpillPerLane * 8);  // ~4.9 MB
+constexpr size_t kOffEnd = align256(kOffSpill + sizeof(float) * (size_t)kNoAllocMaxWorlds * 4 * kSpillPerLane * 8);
+#ifdef ARC_DEVICE_CHECKS
+// the checked build also records each world's grid, against which its
+// kernels test every terrain column they read
+constexpr size_t kOffGridOf = kOffEnd;
+constexpr size_t kScratchBytes = align256(kOffGridOf + sizeof(int) * kNoAllocMaxWorlds);
+#else
+constexpr size_t kScratchBytes = kOffEnd;  // ~4.9 MB
+#endif
 
 // Shared by every call on a device and kept between calls: calls whose
 // work overlaps on the GPU race on it.
@@ -83,6 +91,9 @@ __global__ void k_noalloc_in(unsigned char* scratch, const double* __restrict__ 
     reinterpret_cast<TerrainGeomD*>(scratch + kOffTgd)[i] = g;
     reinterpret_cast<TerrainGeom<float>*>(scratch + kOffTg)[i] =
         TerrainGeom<float>{grid, grid, (float)g.cell, (float)g.ox, (float)g.oy, (float)g.outside};
+#ifdef ARC_DEVICE_CHECKS
+    reinterpret_cast<int*>(scratch + kOffGridOf)[i] = grid;
+#endif
 }
 
 // FP32 records (scratch) -> snapshot (FP64, caller memory)
@@ -166,6 +177,14 @@ extern "C" int arc_step_noalloc(double* d_state, const float* d_heights, int gri
     if (!scratch)
         return ARC_ERR_CUDA;
     std::call_once(g_model_once, [] { build_leaper(g_model); });
+    // the most contact records one lane can make in a substep on these
+    // columns; the spill area holds all but the kernel's on-chip ones
+    const int lane_cap = lane_contact_bound(g_model, cell);
+    if (lane_cap > kSpillPerLane + kFastOnChipContacts) {
+        std::fprintf(stderr, "arc_step_noalloc: %d contacts per lane on %.3f m cells exceed the static spill area (%d)\n",
+                     lane_cap, cell, kSpillPerLane + kFastOnChipContacts);
+        return ARC_ERR_ARG;
+    }
     const DevModel<float> M = make_dev_model<float>(g_model, dt, substeps, 0.6);
 
     Worlds<float> W;
@@ -181,6 +200,9 @@ extern "C" int arc_step_noalloc(double* d_state, const float* d_heights, int gri
     W.tg = reinterpret_cast<const TerrainGeom<float>*>(scratch + kOffTg);
     W.tgd = reinterpret_cast<const TerrainGeomD*>(scratch + kOffTgd);
     W.n = n_worlds;
+#ifdef ARC_DEVICE_CHECKS
+    W.grid_of = reinterpret_cast<const int*>(scratch + kOffGridOf);
+#endif
 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int threads = 128, blocks = (n_worlds + threads - 1) / threads;
@@ -188,9 +210,10 @@ extern "C" int arc_step_noalloc(double* d_state, const float* d_heights, int gri
     if (cudaGetLastError() != cudaSuccess)
         return ARC_ERR_CUDA;
     Actuation A{d_targets, nullptr};
-    // lane bound for cells >= 0.4 m: 29 records, 4 of them on chip
-    if (launch_step_fast<float>(M, W, A, reinterpret_cast<float*>(scratch + kOffSpill), kSpillPerLane,
-                                kSpillPerLane + kFastOnChipContacts, 8, st) != cudaSuccess)
+    // a lane keeps kFastOnChipContacts (2) records on chip and spills the
+    // rest, at most lane_cap - 2 <= kSpillPerLane of them
+    if (launch_step_fast<float>(M, W, A, reinterpret_cast<float*>(scratch + kOffSpill), kSpillPerLane, lane_cap, 8,
+                                st) != cudaSuccess)
         return ARC_ERR_CUDA;
     k_noalloc_out<<<blocks, threads, 0, st>>>(scratch, d_state, n_worlds);
     return cudaGetLastError() == cudaSuccess ? ARC_OK : ARC_ERR_CUDA;

@@ -182,28 +182,6 @@ void rebuild_models(arc_sim* s)
     s->rm = make_reset_model(s->model);
 }
 
-// Upper bound of the contacts one lane of the leg-parallel kernel records in
-// a substep: a sphere of radius r touches at most (floor(2r/cell)+2)^2
-// columns, one contact each.
-int lane_contact_bound(const ModelHost& m, double cell)
-{
-    if (!m.leaper)
-        return 0;
-    int worst = 0;
-    for (int leg = 0; leg < kNumLegs; ++leg) {
-        long long sum = 0;
-        for (int it = 0; it < 6; ++it) {
-            int s = it == 0 ? (leg == 0 ? 0 : -1) : 5 * leg + it;
-            if (s < 0)
-                continue;
-            long long per = (long long)std::floor(2.0 * m.s[s].radius / cell) + 2;
-            sum += per * per;
-        }
-        worst = (int)std::max<long long>(worst, std::min<long long>(sum, kMaxContacts));
-    }
-    return worst;
-}
-
 int ensure_spill(arc_sim* s, double cell)
 {
     if (s->spill && cell >= s->spill_cell)
@@ -1479,27 +1457,46 @@ int ensure_step_host(arc_sim* s)
 {
     if (s->iota)
         return ARC_OK;
-    int* iota = nullptr;
-    if (check(s, cudaMalloc((void**)&s->chunk_done, sizeof(int) * s->n), "cudaMalloc(chunk lists)") ||
-        check(s, cudaMalloc((void**)&s->chunk_count, sizeof(int) * kMaxChunks), "cudaMalloc(chunk counts)") ||
-        check(s, cudaMalloc((void**)&s->part_queue, sizeof(int) * 2 * kMaxChunks), "cudaMalloc(part queues)") ||
-        check(s, cudaMalloc((void**)&iota, sizeof(int) * s->n), "cudaMalloc(world indices)"))
+    // everything is made into locals and handed to s only once all of it
+    // exists, so a failure part way leaves s as it was and leaks nothing
+    int *iota = nullptr, *chunk_done = nullptr, *chunk_count = nullptr, *part_queue = nullptr;
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    constexpr int kEvents = (int)(sizeof(s->ev) / sizeof(s->ev[0]));
+    cudaEvent_t ev[kEvents] = {};
+    auto release = [&] {
+        for (cudaEvent_t e : ev)
+            if (e)
+                cudaEventDestroy(e);
+        for (cudaStream_t c : {copy_in, copy_out})
+            if (c)
+                cudaStreamDestroy(c);
+        for (int* p : {iota, chunk_done, chunk_count, part_queue})
+            cudaFree(p);
         return ARC_ERR_CUDA;
+    };
+    if (check(s, cudaMalloc((void**)&chunk_done, sizeof(int) * s->n), "cudaMalloc(chunk lists)") ||
+        check(s, cudaMalloc((void**)&chunk_count, sizeof(int) * kMaxChunks), "cudaMalloc(chunk counts)") ||
+        check(s, cudaMalloc((void**)&part_queue, sizeof(int) * 2 * kMaxChunks), "cudaMalloc(part queues)") ||
+        check(s, cudaMalloc((void**)&iota, sizeof(int) * s->n), "cudaMalloc(world indices)"))
+        return release();
     k_iota<<<(s->n + 255) / 256, 256, 0, s->stream>>>(iota, s->n);
     // ready before any stream uses them (arc_env_step_part runs on the caller's)
     if (check(s, cudaGetLastError(), "world indices") ||
-        check(s, cudaMemsetAsync(s->part_queue, 0, sizeof(int) * 2 * kMaxChunks, s->stream), "zero part queues") ||
+        check(s, cudaMemsetAsync(part_queue, 0, sizeof(int) * 2 * kMaxChunks, s->stream), "zero part queues") ||
         check(s, cudaStreamSynchronize(s->stream), "world indices") ||
-        check(s, cudaStreamCreateWithFlags(&s->copy_in, cudaStreamNonBlocking), "copy stream") ||
-        check(s, cudaStreamCreateWithFlags(&s->copy_out, cudaStreamNonBlocking), "copy stream")) {
-        cudaFree(iota);
-        return ARC_ERR_CUDA;
-    }
-    for (cudaEvent_t& e : s->ev)
-        if (check(s, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event")) {
-            cudaFree(iota);
-            return ARC_ERR_CUDA;
-        }
+        check(s, cudaStreamCreateWithFlags(&copy_in, cudaStreamNonBlocking), "copy stream") ||
+        check(s, cudaStreamCreateWithFlags(&copy_out, cudaStreamNonBlocking), "copy stream"))
+        return release();
+    for (cudaEvent_t& e : ev)
+        if (check(s, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"))
+            return release();
+    s->chunk_done = chunk_done;
+    s->chunk_count = chunk_count;
+    s->part_queue = part_queue;
+    s->copy_in = copy_in;
+    s->copy_out = copy_out;
+    for (int i = 0; i < kEvents; ++i)
+        s->ev[i] = ev[i];
     s->iota = iota;
     return ARC_OK;
 }

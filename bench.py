@@ -56,9 +56,9 @@ RENDER_METRIC = "frames/s at 640x360, 4 samples per pixel"
 RENDER_WORLDS = 256
 RENDER_W, RENDER_H, RENDER_SAMPLES = 640, 360, 4
 # Work and DRAM traffic of k_render per frame of this workload, from one ncu
-# capture of a 16-frame launch (profiles/render_640x360.md): 786.8 M warp
-# instructions, 1.58 MB read + 76.73 MB written, over 16 frames. The kernel is
-# bound by instruction issue (4 warp instructions per SM per cycle).
+# capture of a 16-frame launch: 786.8 M warp instructions, 1.58 MB read +
+# 76.73 MB written, over 16 frames. The kernel is bound by instruction issue
+# (4 warp instructions per SM per cycle).
 RENDER_WARP_INST_PER_FRAME = 786.831e6 / 16
 RENDER_DRAM_BYTES_PER_FRAME = (1.5777e6 + 76.7283e6) / 16
 
@@ -70,7 +70,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--worlds", type=int, default=WORLDS)
-    p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length (all worlds)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--wpc", type=int, default=0, help="worlds per CTA (0: autotune)")
@@ -81,6 +81,8 @@ def parse():
     p.add_argument("--workload", choices=["step", "render"], default="step",
                    help="step: the world step (the headline); render: frames of the headless renderer")
     p.add_argument("--render-worlds", type=int, default=RENDER_WORLDS)
+    p.add_argument("--no-workloads", action="store_true",
+                   help="skip the other workloads' short legs (uneven OU batch, grid sizes, FP64, serving)")
     return p.parse_args()
 
 
@@ -440,6 +442,8 @@ def run_ours(args) -> dict | None:
     if e2e:
         out["e2e"] = e2e
         out["e2e_reference_abi"] = e2e_abi
+    if world == 1 and not args.no_workloads:
+        out["workloads"] = run_workloads(torch, n)
     if world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(args.cpu_seconds, n)
     return out
@@ -527,19 +531,193 @@ def run_e2e_reference_abi(sim, K) -> dict:
 
 
 # ---------------------------------------------------------------------------
+# the other workloads, short legs beside the headline (one GPU, rank 0)
+
+def ou_update(torch, ou, actions, gen, theta=0.15, sigma=0.3):
+    """One control step of a per-joint Ornstein-Uhlenbeck process (dt = one
+    control step), clipped to [-1, 1] into `actions`."""
+    ou.mul_(1.0 - theta).add_(torch.randn(ou.shape, device=ou.device, generator=gen), alpha=sigma)
+    torch.clamp(ou, -1.0, 1.0, out=actions)
+
+
+def timed_loop(torch, stream, one, k):
+    """k calls of one() on `stream`, each bracketed by CUDA events: total ms
+    and per-call ms."""
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream.synchronize()
+    t0.record(stream)
+    for a, b in ev:
+        a.record(stream)
+        one()
+        b.record(stream)
+    t1.record(stream)
+    t1.synchronize()
+    return t0.elapsed_time(t1), np.array([a.elapsed_time(b) for a, b in ev])
+
+
+def leg_uneven_ou(torch, n=4096, steps=300, warmup=20) -> dict:
+    """4,096 worlds, difficulty U[0, 1] per world, per-joint OU actions
+    (theta 0.15, sigma 0.3, clipped, seed 1), auto-reset on termination or
+    after 1,000 steps; each control step is the OU update (three torch
+    kernels) and the env's CUDA graph of the library's kernels."""
+    from arc_demo_b200.native import KERNEL_WARPS
+    from arc_demo_b200.task import TaskConfig
+    from arc_demo_b200.torch_env import DeviceVecEnv
+    env = DeviceVecEnv(n, TaskConfig(curriculum=False), seed=21)
+    env.set_levels(np.random.default_rng(1).uniform(0.0, 1.0, n))
+    env.set_kernel(KERNEL_WARPS)
+    env.sim.set_work_queue(True)
+    stream = torch.cuda.Stream()
+    gen = torch.Generator(device="cuda").manual_seed(1)
+    with torch.cuda.stream(stream):
+        env.reset()
+        ou = torch.zeros((n, 12), device="cuda")
+
+        def one():
+            ou_update(torch, ou, env.actions, gen)
+            env.step()
+        for _ in range(warmup):
+            one()
+        ms, lat = timed_loop(torch, stream, one, steps)
+        ended = int(env.done_count.item())
+    env.close()
+    return {"worlds": n, "steps": steps, "env_steps_per_s": round(n * steps / (ms * 1e-3), 1),
+            "ms_per_step": round(ms / steps, 4),
+            "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 4),
+                           "p99": round(float(np.percentile(lat, 99)), 4), "max": round(float(lat.max()), 4)},
+            "ended_in_last_step": ended,
+            "loop": "OU actions on the device, then DeviceVecEnv.step() (one CUDA graph: step with work queue, "
+                    "task, heights, reset of ended worlds)"}
+
+
+def leg_grid_sizes(torch, n=16384, steps=40, warmup=5) -> dict:
+    """16,384 worlds whose grids are 16..64 columns a side (uniform per
+    world), block heights U(0, 0.3 * difficulty * stand_height) written
+    per column, difficulty U[0, 1], OU actions; every control step is one
+    launch of the step kernel over all sizes (work queue)."""
+    import ctypes
+    from arc_demo_b200.native import KERNEL_WARPS, Sim
+    rng = np.random.default_rng(4)
+    grids = rng.integers(16, 65, n).astype(np.int32)
+    diffs = rng.uniform(0.0, 1.0, n)
+    sim = Sim(n, grids=grids, cell=0.4)
+    sim.set_kernel(KERNEL_WARPS)
+    sim.set_work_queue(True)
+    sim.reset(np.arange(n), rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32), diffs)
+    for i in range(n):
+        sim.set_terrain(i, rng.uniform(0.0, 0.3 * diffs[i] * sim.stand_height, (grids[i], grids[i])), 0.4,
+                        outside=-100.0)
+    st = sim.get_state()
+    st[:, : 13 * 13].reshape(n, 13, 13)[:, :, 2] += 0.2  # drop every robot onto its blocks
+    sim.set_state(st)
+    stream = torch.cuda.Stream()
+    gen = torch.Generator(device="cuda").manual_seed(1)
+    ou = torch.zeros((n, 12), device="cuda")
+    actions = torch.zeros((n, 12), device="cuda")
+    lib, ptr = sim._lib, sim.ptr
+    a, h = ctypes.c_void_p(actions.data_ptr()), ctypes.c_void_p(stream.cuda_stream)
+
+    def one():
+        ou_update(torch, ou, actions, gen)
+        lib.arc_sim_step_actions(ptr, a, h)
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            one()
+        ms, lat = timed_loop(torch, stream, one, steps)
+    sim.close()
+    return {"worlds": n, "steps": steps, "env_steps_per_s": round(n * steps / (ms * 1e-3), 1),
+            "ms_per_step": round(ms / steps, 4), "grid_sizes": "16..64 columns a side, uniform per world",
+            "columns_mean": round(float((grids.astype(np.float64) ** 2).mean()), 1),
+            "loop": "OU actions on the device, then arc_sim_step_actions: one launch of the warp-per-leg kernel "
+                    "over every world size through the work queue (physics step; no task layer)"}
+
+
+def leg_fp64(torch, n, steps=6, warmup=3) -> dict:
+    """The step in FP64 (the reference's precision) at the headline's world
+    count: the leg-parallel FP64 kernel, timed alone from settled states."""
+    import ctypes
+    from arc_demo_b200.native import KERNEL_LEGS
+    from arc_demo_b200.task import TaskConfig
+    from arc_demo_b200.torch_env import DeviceVecEnv
+    env = DeviceVecEnv(n, TaskConfig(curriculum=False), seed=3, fp64=True)
+    env.set_levels(levels_for(n, 17))
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        env.reset()
+        best = None
+        for wpc in (8, 16):
+            env.set_kernel(KERNEL_LEGS, wpc)
+            torch.nn.init.uniform_(env.actions, -1.0, 1.0)
+            for _ in range(warmup):
+                env.step()
+            lib, ptr = env.sim._lib, env.sim.ptr
+            a, h = ctypes.c_void_p(env.actions.data_ptr()), ctypes.c_void_p(stream.cuda_stream)
+            ms, _ = timed_loop(torch, stream, lambda: lib.arc_sim_step_actions(ptr, a, h), steps)
+            if best is None or ms < best[1]:
+                best = (wpc, ms)
+        wpc, ms = best
+        env.set_kernel(KERNEL_LEGS, wpc)
+        step_ms, _ = timed_loop(torch, stream, lambda: env.step(), steps)
+    env.close()
+    return {"worlds": n, "kernel": f"leg-parallel FP64, {wpc} worlds per CTA",
+            "step_kernel_ms": round(ms / steps, 4), "env_steps_per_s_step_kernel": round(n * steps / (ms * 1e-3), 1),
+            "control_step_ms": round(step_ms / steps, 4),
+            "env_steps_per_s_control_step": round(n * steps / (step_ms * 1e-3), 1),
+            "note": "actions fixed (uniform random); control step = step, task, heights, reset in one graph"}
+
+
+def leg_serving(seconds=3.0, clients=8, rate=200.0) -> dict:
+    """The serving engine with 8 Poisson clients at 200 requests/s each
+    (1..8,192 worlds log-uniform x 1..32 control steps, mixed difficulty),
+    the pool sized by a 40 GB budget."""
+    from arc_demo_b200.serve import WORLD_BYTES, Server, run_load
+    capacity = int(40e9 // WORLD_BYTES)
+    with Server(capacity, result="observe") as sv:
+        rid = sv.submit(np.arange(64, dtype=np.uint32), np.zeros(64), 2)
+        sv.wait(rid)
+        out = run_load(sv, clients, rate, seconds)
+    out.update({"clients": clients, "rate_per_client": rate, "capacity": capacity, "offered_seconds": seconds})
+    return out
+
+
+def run_workloads(torch, n) -> dict:
+    legs = {}
+    for name, fn in (("uneven_4096_ou", lambda: leg_uneven_ou(torch)),
+                     ("grid_sizes_16384", lambda: leg_grid_sizes(torch)),
+                     ("fp64", lambda: leg_fp64(torch, n)),
+                     ("serving", lambda: leg_serving())):
+        t = time.perf_counter()
+        try:
+            legs[name] = fn()
+        except Exception as e:  # a leg that fails is reported, the headline stands
+            legs[name] = {"error": f"{type(e).__name__}: {e}"}
+        legs[name]["wall_s"] = round(time.perf_counter() - t, 1)
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return legs
+
+
+# ---------------------------------------------------------------------------
 # the reference's CPU path
 
-def reference_loop(n: int, seconds: float | None, steps: int | None, warmup: int, threads: int) -> dict:
+REF_BUILD = {"": "-O3 -march=x86-64-v3 -ffp-contract=fast -fno-math-errno -fno-trapping-math -fopenmp (AVX2)",
+             "_v4": "-O3 -march=x86-64-v4 -ffp-contract=fast -fno-math-errno -fno-trapping-math -fopenmp (AVX-512)"}
+
+
+def reference_loop(n: int, seconds: float | None, steps: int | None, warmup: int, threads: int,
+                   variant: str | None = None) -> dict:
     """The reference's OpenMP step/observe/heights (its csrc/, oracle/_ref) with
     the task layer (obs, reward, done, auto-reset) in numpy, over n worlds of
     the workload, the same MLP policy on the host (torch, all threads)."""
     import torch
-    from oracle.oracle import RefSim, ref_available
+    from oracle.oracle import RefSim, fastest_ref_variant, ref_available
     from oracle.task_oracle import TaskConfig, TaskOracle
     if not ref_available():
         raise RuntimeError("oracle/_ref/libarcsim_ref.so not built")
+    variant = fastest_ref_variant() if variant is None else variant
     torch.set_num_threads(threads)
-    sim = RefSim(n, threads=threads)
+    sim = RefSim(n, threads=threads, variant=variant)
     task = TaskOracle(sim, TaskConfig(curriculum=False), seed=5)
     task.level[:] = levels_for(n, 17)
     task.reset(np.arange(n))
@@ -577,23 +755,31 @@ def reference_loop(n: int, seconds: float | None, steps: int | None, warmup: int
         if (steps is not None and k >= steps) or (seconds is not None and el >= seconds):
             break
     sim.close()
-    return {"value": n * k / el, "steps": k, "seconds": el, "lat": np.array(lat) * 1e3}
+    return {"value": n * k / el, "steps": k, "seconds": el, "lat": np.array(lat) * 1e3, "variant": variant}
 
 
 def cpu_baseline(seconds: float, full_n: int) -> dict:
+    """The reference's path over every world of the workload (like for
+    like), plus a 4,096-world sample and one thread on 1,024 worlds."""
     import torch
     threads = os.cpu_count() or 1
     torch_threads = torch.get_num_threads()
-    sample_n = 4096
-    r = reference_loop(sample_n, seconds, None, 2, threads)
+    r = reference_loop(full_n, seconds, None, 1, threads)
+    small_n = 4096
+    rs = reference_loop(small_n, seconds / 3, None, 2, threads)
     # the same loop on one thread (OpenMP and torch), a shorter sample
     one_n = 1024
     r1 = reference_loop(one_n, seconds / 3, None, 1, 1)
     torch.set_num_threads(torch_threads)
     return {"value": round(r["value"], 1), "unit": "env-steps/s", "cores": threads, "kind": "reference",
-            "sample": f"{sample_n} of the {full_n} worlds (same difficulty mix), {r['steps']} control steps "
+            "sample": f"all {full_n} worlds (same difficulty mix), {r['steps']} control steps "
                       f"in {r['seconds']:.1f} s: reference csrc/ step+observe+heights with OpenMP x{threads}, "
                       "numpy task layer with auto-reset, MLP policy in torch on the host",
+            "build": REF_BUILD[r["variant"]], "threads": threads,
+            "latency_ms": {"p50": round(float(np.percentile(r["lat"], 50)), 3),
+                           "p99": round(float(np.percentile(r["lat"], 99)), 3)},
+            "sample_4096": {"value": round(rs["value"], 1), "unit": "env-steps/s", "cores": threads,
+                            "sample": f"{small_n} worlds, {rs['steps']} control steps in {rs['seconds']:.1f} s"},
             "single_thread": {"value": round(r1["value"], 1), "unit": "env-steps/s", "cores": 1,
                               "sample": f"{one_n} worlds, {r1['steps']} control steps in {r1['seconds']:.1f} s, "
                                         "OpenMP and torch on one thread"}}
@@ -604,17 +790,17 @@ def run_reference(args) -> dict | None:
     if rank != 0:
         return None
     threads = os.cpu_count() or 1
-    sample_n = 4096
-    r = reference_loop(sample_n, None, max(args.steps, 1), max(args.warmup, 0), threads)
+    n = args.worlds
+    r = reference_loop(n, None, max(args.steps, 1), max(args.warmup, 0), threads)
     cpu = {"value": round(r["value"], 1), "unit": "env-steps/s", "cores": threads, "kind": "reference",
-           "sample": f"{sample_n} of the {args.worlds} worlds per step (same difficulty mix)"}
+           "sample": f"all {n} worlds of the workload, {r['steps']} control steps", "build": REF_BUILD[r["variant"]]}
     return {"metric": METRIC, "value": round(r["value"], 1), "unit": "env-steps/s", "impl": "reference",
             "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": r["steps"], "warmup": args.warmup,
             "ms_per_step": round(float(r["lat"].mean()), 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{sample_n}-world sample of the {args.worlds}-world quadruped workload, "
-                                   "difficulty uniform in {0,...,1.0}, checkpoints, auto-reset, MLP policy",
-                       "threads": threads},
+            "config": {"workload": f"{n} worlds of the quadruped, difficulty uniform in {{0,...,1.0}}, "
+                                   "checkpoints, auto-reset, MLP policy 195-256-256-12 tanh on the host",
+                       "worlds": n, "threads": threads, "build": REF_BUILD[r["variant"]]},
             "latency_ms": {"p50": round(float(np.percentile(r["lat"], 50)), 3),
                            "p99": round(float(np.percentile(r["lat"], 99)), 3)},
             "cpu_baseline": cpu,

@@ -79,8 +79,9 @@ void arc_sim_terrain_at(const arc_sim *s, const int *ids, const double *xy, int 
 /* Replaces csrc/arc_sim.h:56: a host FP64 copy of world i in the
  * reference's arc_world layout (arc_world.h), refreshed from the device by
  * this call and valid until the next arc_sim_world call on the same sim.
- * Render-only visuals and the last substep's contact list are not kept on
- * the device: n_visuals and n_contacts are 0. */
+ * The robot's render-only visuals are filled in from the model (n_visuals
+ * is the model's count); the last substep's contact list is not kept on the
+ * device, so n_contacts is 0. */
 const arc_world *arc_sim_world(const arc_sim *s, int i);
 
 /* ======================================================================
@@ -265,6 +266,9 @@ int arc_server_stats(arc_server *sv, double *stats);
  * substeps <= 1023;
  * larger requests return ARC_ERR_ARG. The first call on a device looks up the
  * array's device address; make that first call before any stream capture.
+ * That address is kept for the life of the process: after cudaDeviceReset on
+ * a device the array moves, so a process that resets a device must not call
+ * arc_step_noalloc on it again.
  * Every call shares the array, so calls whose work overlaps on the GPU race:
  * serialise them (one stream, or events). */
 int arc_step_noalloc(double *d_state, const float *d_heights, int grid, double cell, double outside,

@@ -554,7 +554,25 @@ typedef struct {
     osphere s[MAXS];
     ocontact c[MAXC];
     oterrain t;
+    /* Threshold margins of the last step. Test instrumentation: the tracing
+     * only reads values the step computes and changes none of its
+     * arithmetic. Per sphere, the closest call among its contact on/off
+     * decisions (csrc/arc_phys.c:570, the buried-edge tests :572-581, :587),
+     * in metres; per world, the closest friction-anchor reset (:519, the dot
+     * product's distance from 0.9), static/dynamic friction (:534, relative
+     * to the larger side) and joint-limit activation (:437-443, the sine
+     * tests and the angle's distance from the bound, radians). */
+    double m_contact[MAXS];
+    double m_anchor, m_fric, m_limit;
 } oworld;
+
+/* margin tracing: m = min(m, |v|) */
+static inline void tr_min(double *m, double v)
+{
+    v = fabs(v);
+    if (v < *m)
+        *m = v;
+}
 
 static inline int is_iso(v3r i) { return i.x == i.y && i.y == i.z; }
 
@@ -820,9 +838,13 @@ static void joint_positions(oworld *w, ojoint *j, real h)
     if (j->lo <= j->hi) {
         a1 = brot(bp, j->a1);
         joint_sincos(bp, bc, j, a1, &s, &c);
+        tr_min(&w->m_limit, (double)(s * j->lim[0] - c * j->lim[1]));
+        tr_min(&w->m_limit, (double)(j->lim[3] * c - j->lim[2] * s));
         if (j->hi - j->lo > K(ORC_PI) || s * j->lim[0] - c * j->lim[1] < K(0.0)
             || j->lim[3] * c - j->lim[2] * s < K(0.0)) {
             phi = R_ATAN2(s, c);
+            tr_min(&w->m_limit, (double)(phi - j->lo));
+            tr_min(&w->m_limit, (double)(phi - j->hi));
             if (phi < j->lo)
                 solve_rot_block(bp, bc, v_scale(a1, phi - j->lo));
             else if (phi > j->hi)
@@ -884,6 +906,8 @@ static inline void solve_friction(oworld *w, osphere *s, v3r n, real ln, real h)
     v3r c = v_add(b->x, brot(b, s->pos));
     v3r p = v_madd(c, n, -s->radius), e, r;
     real len, wt, lt, frac = K(1.0);
+    if (s->anchored)
+        tr_min(&w->m_anchor, (double)(v_dot(n, s->anchor_n) - K(0.9)));
     if (!s->anchored || v_dot(n, s->anchor_n) < K(0.9)) {
         v3r c0 = v_add(b->x_prev, q_rotate(b->q_prev, s->pos));
         s->anchor = v_madd(c0, n, -s->radius);
@@ -898,6 +922,10 @@ static inline void solve_friction(oworld *w, osphere *s, v3r n, real ln, real h)
     r = v_sub(p, b->x);
     wt = w_pos(b, r, v_scale(e, K(1.0) / len));
     lt = len / wt;
+    {
+        double a = fabs((double)lt), b = fabs((double)(w->mu_s * ln));
+        tr_min(&w->m_fric, ((double)lt - (double)(w->mu_s * ln)) / (a > b ? (a > 1e-300 ? a : 1e-300) : b));
+    }
     if (lt > w->mu_s * ln) {
         frac = r_min(w->mu_d * ln / lt, K(1.0));
         s->anchor = v_madd(s->anchor, e, K(1.0) - frac);
@@ -929,8 +957,25 @@ static void collide_sphere(oworld *w, osphere *s, real h)
             real y0 = t->oy + iy * t->cell, y1 = y0 + t->cell;
             real dist, depth;
             v3r q, diff, n;
+            double *mc = &w->m_contact[s - w->s];
+            tr_min(mc, (double)((c.z - rad) - top));
             if (c.z - rad >= top)
                 continue;
+            /* which neighbours the buried-edge tests read turns on c against
+             * the column's edges wherever a neighbour on that side is at
+             * least as high */
+            if (terrain_cell(t, ix + 1, iy) >= top || terrain_cell(t, ix + 1, iy + 1) >= top ||
+                terrain_cell(t, ix + 1, iy - 1) >= top)
+                tr_min(mc, (double)(c.x - x1));
+            if (terrain_cell(t, ix - 1, iy) >= top || terrain_cell(t, ix - 1, iy + 1) >= top ||
+                terrain_cell(t, ix - 1, iy - 1) >= top)
+                tr_min(mc, (double)(c.x - x0));
+            if (terrain_cell(t, ix, iy + 1) >= top || terrain_cell(t, ix + 1, iy + 1) >= top ||
+                terrain_cell(t, ix - 1, iy + 1) >= top)
+                tr_min(mc, (double)(c.y - y1));
+            if (terrain_cell(t, ix, iy - 1) >= top || terrain_cell(t, ix + 1, iy - 1) >= top ||
+                terrain_cell(t, ix - 1, iy - 1) >= top)
+                tr_min(mc, (double)(c.y - y0));
             sx = c.x > x1 ? 1 : (c.x < x0 ? -1 : 0);
             sy = c.y > y1 ? 1 : (c.y < y0 ? -1 : 0);
             if (sx && terrain_cell(t, ix + sx, iy) >= top)
@@ -943,6 +988,7 @@ static void collide_sphere(oworld *w, osphere *s, real h)
             diff = v_sub(c, q);
             dist = v_len(diff);
             if (dist > K(1e-9)) {
+                tr_min(mc, (double)(dist - rad));
                 if (dist >= rad)
                     continue;
                 n = v_scale(diff, K(1.0) / dist);
@@ -1061,8 +1107,11 @@ static void world_step(oworld *w, const double (*lim64)[4], double dt, int subst
     int s, i;
     for (i = 0; i < w->nb; ++i)
         body_sync(&w->b[i]);
-    for (i = 0; i < w->ns; ++i)
+    for (i = 0; i < w->ns; ++i) {
         w->s[i].touch = 0;
+        w->m_contact[i] = 1e30;
+    }
+    w->m_anchor = w->m_fric = w->m_limit = 1e30;
     for (i = 0; i < w->nj; ++i) {
         ojoint *j = &w->j[i];
         j->torque_acc = K(0.0);
@@ -1431,6 +1480,23 @@ EXPORT void ORC_EXPORT(terrain_at)(const osim *s, const int *ids, const double *
 EXPORT int ORC_EXPORT(state_size)(const osim *s)
 {
     return s->model.nb * SNAP_BODY + s->model.ns * SNAP_SPHERE + s->model.nj * SNAP_JOINT + 2;
+}
+
+/* Threshold margins of each world's last step (see oworld): per world, ns
+ * contact margins, then the anchor, friction and limit margins (1e30: no
+ * such decision was taken). */
+EXPORT void ORC_EXPORT(margins)(const osim *s, double *out)
+{
+    int i, k;
+    for (i = 0; i < s->n; ++i) {
+        const oworld *w = &s->worlds[i];
+        double *o = out + (size_t)i * (w->ns + 3);
+        for (k = 0; k < w->ns; ++k)
+            o[k] = w->m_contact[k];
+        o[w->ns] = w->m_anchor;
+        o[w->ns + 1] = w->m_fric;
+        o[w->ns + 2] = w->m_limit;
+    }
 }
 
 EXPORT void ORC_EXPORT(get_state)(const osim *s, const int *ids, int n_ids, double *out)

@@ -47,6 +47,22 @@ def ref_available() -> bool:
     return (HERE / "_ref" / "libarcsim_ref.so").exists()
 
 
+def host_has_avx512() -> bool:
+    try:
+        flags = Path("/proc/cpuinfo").read_text().split()
+    except OSError:
+        return False
+    return "avx512f" in flags and "avx512bw" in flags and "avx512vl" in flags and "avx512dq" in flags
+
+
+def fastest_ref_variant() -> str:
+    """The reference build for timing: AVX-512 where the host runs it (the
+    reference's own -march=native would use it there), else AVX2."""
+    if host_has_avx512() and (HERE / "_ref" / "libarcsim_ref_v4.so").exists():
+        return "_v4"
+    return ""
+
+
 # -- the restatement ----------------------------------------------------------
 
 _oracle_libs: dict[int, ctypes.CDLL] = {}
@@ -79,6 +95,7 @@ def oracle_lib(bits: int) -> ctypes.CDLL:
     d("terrain_at", None, _vp, _i32, _f64, _int, _f64)
     d("state_size", _int, _vp)
     d("get_state", None, _vp, _i32, _int, _f64)
+    d("margins", None, _vp, _f64)
     d("set_state", None, _vp, _i32, _int, _f64)
     d("set_terrain", None, _vp, _int, _int, _int, _dbl, _dbl, _f64)
     d("get_terrain", None, _vp, _int, _i32, _f64, _f64)
@@ -161,6 +178,15 @@ class OracleSim(_SimBase):
         out = np.zeros(len(ids))
         if len(ids):
             self._f("terrain_at")(self.ptr, ids, xy, len(ids), out)
+        return out
+
+    def margins(self) -> np.ndarray:
+        """Threshold margins of each world's last step (N x (NS + 3)):
+        per sphere the closest contact on/off decision in metres, then the
+        closest anchor reset, static/dynamic friction and limit decisions
+        (1e30 where none was taken)."""
+        out = np.zeros((self.num_worlds, NS + 3))
+        self._f("margins")(self.ptr, out)
         return out
 
     def get_state(self, ids=None) -> np.ndarray:
@@ -320,7 +346,8 @@ _ref_libs: dict[str, ctypes.CDLL] = {}
 
 
 def ref_lib(variant: str = "") -> ctypes.CDLL:
-    """variant "" (reference flags) or "_strict" (no FMA contraction)."""
+    """variant "" (reference flags, AVX2), "_v4" (the same with AVX-512) or
+    "_strict" (no FMA contraction)."""
     if variant in _ref_libs:
         return _ref_libs[variant]
     path = HERE / "_ref" / f"libarcsim_ref{variant}.so"

