@@ -38,6 +38,10 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxe
 # are far below the FP32 parity bounds its tests hold it to, and flushes
 # denormals to zero (no fix-up code for them: 3% less code and time)
 FILE_FLAGS = {"arc_step_warps.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
+              # the task layer runs the same warp-per-leg step inside its fused
+              # control-step kernel: the same flags, so the two give the same
+              # worlds (its own arithmetic is FP64, which they do not touch)
+              "arc_task.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
               # the renderer: the same, for code size (its output is 8-bit colour)
               "arc_render.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]}
 

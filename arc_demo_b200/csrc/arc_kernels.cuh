@@ -45,7 +45,8 @@ cudaError_t launch_step_plain(const DevModel<R>& M, const Worlds<R>& W, const Ac
                               int n_ids, cudaStream_t stream);
 
 // Leg-parallel step: four lanes per world, state staged in shared memory.
-// worlds_per_cta is a multiple of 8 (one warp steps eight worlds).
+// worlds_per_cta in {1, 2, 4, 8, 16, 32, 64} (a warp steps eight worlds;
+// CTAs of 1, 2 or 4 worlds are part of a warp).
 // spill: per world and lane, spill_per_lane contact records of 8 R beyond
 // the on-chip ones; lane_cap bounds the contacts one lane can record.
 template <class R>
@@ -58,10 +59,12 @@ template <class R> size_t fast_smem_bytes(int stride, int worlds_per_cta);
 // leg k of every world; same spill layout as launch_step_fast. Steps the
 // n_items worlds ids[0..n_items) (ids NULL: worlds 0..n_items-1). With a
 // queue (two device ints, zero between launches) one wave of resident CTAs
-// takes groups of 32 worlds from it until none is left.
+// takes groups of 32 worlds from it until none is left. tile in
+// 1 .. substeps - 1 (with tile_q: 13 x 4 floats per world): the control step
+// as launches of `tile` substeps each, the same worlds bit for bit.
 cudaError_t launch_step_warps(const DevModel<float>& M, const Worlds<float>& W, const Actuation& A, float* spill,
                               int spill_per_lane, int lane_cap, const int* ids, int n_items, int* queue,
-                              cudaStream_t stream);
+                              cudaStream_t stream, int tile = 0, float* tile_q = nullptr);
 size_t warps_smem_bytes();
 constexpr int kFastOnChipContacts = 2;
 constexpr int kWarpsOnChipContacts = 1;  // keeps four CTAs of the warp-per-leg kernel per SM

@@ -1,23 +1,34 @@
-// arc_serve.cu - a serving engine over one batch of resident worlds.
+// arc_serve.cu - a serving engine: client sessions of resident worlds with the
+// task layer, stepped by continuous batching.
 //
-// No counterpart in the reference, which steps one synchronous batch per
-// call (arc/env.py:96-117). Clients submit requests - n worlds (fresh
-// episodes: seeds, difficulties) to be stepped k control steps with given
-// actions, or with actions from a seeded Ornstein-Uhlenbeck process - and
-// wait for the worlds' final states. One engine thread runs continuous
-// batching over a fixed pool of world slots (the byte budget, decided at
-// create):
-//   - admission: queued requests are admitted first come, first served,
-//     while free slots hold them; their slots are reset (arc_sim_reset) at
-//     once;
-//   - one tick: every admitted request's worlds step together in one launch
-//     (arc_sim_step_ids over the active slot list), whatever request they
-//     belong to;
-//   - eviction: a request whose k steps are done has its final states read
-//     back and its slots freed at the end of that tick.
-// A world's result depends only on its own state and actions (worlds never
-// interact, and the step runs the same per-world code for any slot list),
-// so a request's results in the mix equal its results alone, bit for bit.
+// No counterpart in the reference, whose ArcVecEnv steps one synchronous batch
+// per call (arc/env.py:96-117). Here:
+//   - a session is one client's batch of n worlds with the task layer
+//     (ArcTask: observations, rewards, terminations, auto-reset). Opening it
+//     queues it for n slots of a fixed pool of worlds (the device-memory
+//     budget, decided at create). Once slots are free it is admitted: each
+//     world starts an episode at the session's difficulty, its random streams
+//     named by the session's key (arc_env_admit), so the session's worlds
+//     behave alike whichever slots they get. The session keeps its slots, and
+//     its worlds stay on the device, until it is closed.
+//   - a request steps one session's worlds k control steps, with given
+//     actions or a seeded Ornstein-Uhlenbeck process, and returns every
+//     step's rewards and done flags and the observations after the last
+//     step. A world whose episode ends (terminated or truncated,
+//     arc/task.py:196-220) is evicted from its slot at once and the slot
+//     reset with the world's next episode, as ArcVecEnv auto-resets
+//     (arc/env.py:99-117).
+//   - one engine thread runs continuous batching: each tick steps the worlds
+//     of every running request together (arc_env_step_ids: one launch of the
+//     fused control step over their slots), whatever session they belong to.
+//     A queued request starts running, first come first served, once its
+//     session is resident, runs no other request, and the tick has room for
+//     its worlds: at most tick_cap worlds run at once, so a burst of large
+//     requests lengthens the queue, not every tick; a request larger than
+//     the cap runs alone. It leaves the tick when its k steps are done.
+// Worlds never interact and the fused step runs the same per-world code for
+// any list of slots, so a session's results in the mix equal its results
+// alone, bit for bit.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -37,10 +48,8 @@
 namespace {
 
 constexpr int kJ = 12;
-constexpr int kReadChunk = 16384;  // worlds per read-back of final states
-// an observation row: root 13, rotation 9, joints 36, contacts 6, flag 1
-// (the blocks of arc_sim_observe, csrc/arc_sim.h:17-21)
-constexpr int kObsRow = 13 + 9 + 36 + 6 + 1;
+constexpr int kObs = 195;           // arc/task.py:231-259
+constexpr int kReadChunk = 16384;   // worlds per read-back of final observations
 
 // Counter-based normal draws for the OU actions: splitmix64 of (seed, count)
 // gives two uniforms, Box-Muller gives the normal.
@@ -59,9 +68,10 @@ __device__ __forceinline__ float normal_draw(unsigned long long seed, unsigned l
     return sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
 }
 
-// Actions of the listed slots for this tick: the request's own (host
-// actions, uploaded compactly beside the list) or the next value of the
-// slot's OU process, theta = 0.15, sigma = 0.3, clipped to [-1, 1].
+// Actions of the listed slots for this tick into the env's action rows: the
+// request's own (host actions, uploaded compactly beside the list) or the
+// next value of the slot's OU process, theta = 0.15, sigma = 0.3, clipped to
+// [-1, 1].
 __global__ void k_tick_actions(const int* __restrict__ ids, int n, const float* __restrict__ given,
                                const unsigned char* __restrict__ use_given, const unsigned long long* __restrict__ seed,
                                float* __restrict__ ou, int* __restrict__ t, float* __restrict__ actions)
@@ -85,8 +95,8 @@ __global__ void k_tick_actions(const int* __restrict__ ids, int n, const float* 
     t[s] = step + 1;
 }
 
-// New requests' slots: OU state zero, step count zero, the per-world seed.
-__global__ void k_admit(const int* __restrict__ ids, const unsigned long long* __restrict__ seeds, int n,
+// A starting request's slots: OU state zero, step count zero, the per-world seed.
+__global__ void k_start(const int* __restrict__ ids, const unsigned long long* __restrict__ seeds, int n,
                         unsigned long long* __restrict__ seed, float* __restrict__ ou, int* __restrict__ t)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -99,21 +109,53 @@ __global__ void k_admit(const int* __restrict__ ids, const unsigned long long* _
         ou[(size_t)s * kJ + c] = 0.0f;
 }
 
+// The tick's rewards and done flags (bit 0 terminated, bit 1 truncated), in
+// tick order.
+__global__ void k_gather_step(const int* __restrict__ ids, int n, const float* __restrict__ reward,
+                              const unsigned char* __restrict__ terminated, const unsigned char* __restrict__ truncated,
+                              float* __restrict__ out_reward, unsigned char* __restrict__ out_done)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    const int s = ids[k];
+    out_reward[k] = reward[s];
+    out_done[k] = (unsigned char)((terminated[s] ? 1 : 0) | (truncated[s] ? 2 : 0));
+}
+
+// Observation rows of the listed slots, in list order.
+__global__ void k_gather_obs(const int* __restrict__ ids, int n, const float* __restrict__ obs, float* __restrict__ out)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n * kObs)
+        return;
+    const int k = (int)(t / kObs), c = (int)(t % kObs);
+    out[t] = obs[(size_t)ids[k] * kObs + c];
+}
+
 using Clock = std::chrono::steady_clock;
+
+struct Session {
+    long long id = 0;
+    int n = 0;
+    unsigned long long key = 0;
+    std::vector<double> difficulty;
+    std::vector<int> slots;
+    bool admitted = false, closed = false, busy = false;
+    int pending = 0;  // requests submitted and not finished
+};
 
 struct Request {
     long long id = 0;
-    int n = 0, steps = 0, done_steps = 0;
-    std::vector<unsigned> seeds;
-    std::vector<double> difficulty;
+    std::shared_ptr<Session> ses;
+    int steps = 0, done_steps = 0;
     std::vector<float> actions;  // steps x n x 12, or empty: OU
     unsigned long long ou_seed = 0;
-    std::vector<int> slots;
-    double* user_out = nullptr;  // the caller's result buffer, or NULL
-    std::vector<double> out;     // the result when the caller gave none
-    double* dest() { return user_out ? user_out : out.data(); }
-    Clock::time_point t_submit, t_admit, t_done;
-    bool done = false;
+    float* obs = nullptr;            // n x 195, or NULL
+    float* reward = nullptr;         // steps x n, or NULL
+    unsigned char* done = nullptr;   // steps x n, or NULL
+    Clock::time_point t_submit, t_start, t_done;
+    bool finished = false;
     int status = 0;
 };
 
@@ -130,42 +172,42 @@ template <class T> struct HostArray {
 
 struct arc_server {
     arc_sim* sim = nullptr;
-    int capacity = 0, state_size = 0, device = 0;
-    int result = ARC_SERVE_STATE, row = 0;  // doubles per world in a result
+    int capacity = 0, tick_cap = 0, device = 0;
     std::vector<int> free_slots;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
-    std::deque<std::shared_ptr<Request>> queue;
-    std::vector<std::shared_ptr<Request>> active;  // engine thread only
+    std::unordered_map<long long, std::shared_ptr<Session>> sessions;
+    std::deque<std::shared_ptr<Session>> waiting;      // sessions waiting for slots
+    std::deque<std::shared_ptr<Request>> queue;        // requests not running yet
+    std::vector<std::shared_ptr<Request>> running;     // engine thread only
     std::unordered_map<long long, std::shared_ptr<Request>> by_id;
-    long long next_id = 0;
+    long long next_id = 1;
     bool stop = false;
     std::thread engine;
     cudaStream_t stream = nullptr;
-    // device and pinned staging, capacity-sized
-    DevArray<int> d_ids, d_admit_ids;
-    DevArray<float> d_actions, d_ou, d_given;
+    // the env's device buffers (rows indexed by slot)
+    float *env_actions = nullptr, *env_obs = nullptr, *env_reward = nullptr;
+    unsigned char *env_terminated = nullptr, *env_truncated = nullptr;
+    // per-slot OU state and per-tick staging, capacity-sized
+    DevArray<int> d_ids, d_start_ids;
+    DevArray<float> d_ou, d_given, d_reward, d_obs;
     DevArray<int> d_t;
-    DevArray<unsigned long long> d_seed, d_admit_seeds;
-    DevArray<unsigned char> d_use;
-    HostArray<int> h_ids, h_admit_ids;
-    HostArray<float> h_given;
-    HostArray<unsigned char> h_use;
-    HostArray<unsigned long long> h_admit_seeds;
-    HostArray<double> h_state;  // kReadChunk final states or observation blocks, pinned
-    HostArray<int> h_read_ids, h_flags;
-    DevArray<int> d_read_ids, d_flags;
-    DevArray<double> d_obs;     // root, rot, joints, contacts blocks of kReadChunk rows
+    DevArray<unsigned long long> d_seed, d_start_seeds;
+    DevArray<unsigned char> d_use, d_done;
+    HostArray<int> h_ids, h_start_ids;
+    HostArray<float> h_given, h_reward, h_obs;
+    HostArray<unsigned char> h_use, h_done;
+    HostArray<unsigned long long> h_start_seeds;
     // statistics (under mu)
-    long long ticks = 0, world_steps = 0, completed = 0;
+    long long ticks = 0, world_steps = 0, completed = 0, episodes_ended = 0;
     int max_active = 0;
-    double busy_s = 0.0, admit_s = 0.0, step_s = 0.0, evict_s = 0.0;
+    double busy_s = 0.0, admit_s = 0.0, step_s = 0.0, read_s = 0.0;
     int error = 0;
 };
 
 namespace {
 
-bool ok(cudaError_t e, arc_server* sv, const char* what)
+bool ok(cudaError_t e, const char* what)
 {
     if (e == cudaSuccess)
         return true;
@@ -173,170 +215,255 @@ bool ok(cudaError_t e, arc_server* sv, const char* what)
     return false;
 }
 
-// Admits queued requests in order while they fit; resets their worlds.
-bool admit(arc_server* sv)
+// A world's key: its session's key and its index in the session.
+unsigned world_key(unsigned long long session_key, int i)
 {
-    std::vector<std::shared_ptr<Request>> admitted;
-    {
-        std::lock_guard<std::mutex> lock(sv->mu);
-        while (!sv->queue.empty() && (int)sv->free_slots.size() >= sv->queue.front()->n) {
-            auto r = sv->queue.front();
-            sv->queue.pop_front();
-            r->slots.assign(sv->free_slots.end() - r->n, sv->free_slots.end());
-            sv->free_slots.resize(sv->free_slots.size() - r->n);
-            r->t_admit = Clock::now();
-            admitted.push_back(r);
-        }
-    }
-    if (admitted.empty())
-        return true;
-    int m = 0;
-    std::vector<int> ids;
-    std::vector<unsigned> seeds;
-    std::vector<double> diff;
-    for (auto& r : admitted) {
-        for (int i = 0; i < r->n; ++i) {
-            sv->h_admit_ids.p[m] = r->slots[i];
-            // one OU stream per (request, world)
-            sv->h_admit_seeds.p[m] = r->ou_seed * 0x9e3779b97f4a7c15ull + (unsigned long long)i;
-            ++m;
-        }
-        ids.insert(ids.end(), r->slots.begin(), r->slots.end());
-        seeds.insert(seeds.end(), r->seeds.begin(), r->seeds.end());
-        diff.insert(diff.end(), r->difficulty.begin(), r->difficulty.end());
-        sv->active.push_back(r);
-    }
-    arc_sim_reset(sv->sim, ids.data(), (int)ids.size(), seeds.data(), diff.data());
-    if (arc_sim_last_error(sv->sim))
-        return false;
-    if (!ok(cudaMemcpyAsync(sv->d_admit_ids.p, sv->h_admit_ids.p, sizeof(int) * m, cudaMemcpyHostToDevice,
-                            sv->stream), sv, "admit ids") ||
-        !ok(cudaMemcpyAsync(sv->d_admit_seeds.p, sv->h_admit_seeds.p, sizeof(unsigned long long) * m,
-                            cudaMemcpyHostToDevice, sv->stream), sv, "admit seeds"))
-        return false;
-    k_admit<<<(m + 127) / 128, 128, 0, sv->stream>>>(sv->d_admit_ids.p, sv->d_admit_seeds.p, m, sv->d_seed.p,
-                                                     sv->d_ou.p, sv->d_t.p);
-    return ok(cudaGetLastError(), sv, "admit kernel");
+    unsigned long long z = session_key * 0x9e3779b97f4a7c15ull + (unsigned long long)i + 1;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return (unsigned)((z ^ (z >> 31)) & 0x7fffffffu);
 }
 
-// One control step of every active world; completes finished requests.
+// Admits waiting sessions in order while free slots hold them; frees the
+// slots of closed sessions with nothing left to run.
+bool admit(arc_server* sv)
+{
+    std::vector<std::shared_ptr<Session>> admitted;
+    {
+        std::lock_guard<std::mutex> lock(sv->mu);
+        for (auto it = sv->sessions.begin(); it != sv->sessions.end();) {
+            Session& s = *it->second;
+            if (s.closed && s.pending == 0) {
+                if (s.admitted)
+                    sv->free_slots.insert(sv->free_slots.end(), s.slots.begin(), s.slots.end());
+                it = sv->sessions.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        while (!sv->waiting.empty() && (int)sv->free_slots.size() >= sv->waiting.front()->n) {
+            auto s = sv->waiting.front();
+            sv->waiting.pop_front();
+            if (s->closed)
+                continue;
+            s->slots.assign(sv->free_slots.end() - s->n, sv->free_slots.end());
+            sv->free_slots.resize(sv->free_slots.size() - s->n);
+            admitted.push_back(s);
+        }
+    }
+    for (auto& s : admitted) {
+        std::vector<unsigned> keys(s->n);
+        for (int i = 0; i < s->n; ++i)
+            keys[i] = world_key(s->key, i);
+        if (arc_env_admit(sv->sim, s->slots.data(), s->n, s->difficulty.data(), keys.data(), sv->stream) != ARC_OK)
+            return false;
+        std::lock_guard<std::mutex> lock(sv->mu);
+        s->admitted = true;
+    }
+    return true;
+}
+
+// Starts queued requests, first come first served, whose session is
+// resident and idle, while the tick has room.
+bool start(arc_server* sv)
+{
+    std::vector<std::shared_ptr<Request>> started;
+    {
+        std::lock_guard<std::mutex> lock(sv->mu);
+        int active = 0;
+        for (auto& r : sv->running)
+            active += r->ses->n;
+        for (auto it = sv->queue.begin(); it != sv->queue.end();) {
+            Request& r = **it;
+            if (!r.ses->admitted || r.ses->busy) {
+                ++it;
+                continue;
+            }
+            if (active > 0 && active + r.ses->n > sv->tick_cap)
+                break;  // the oldest runnable request waits for room; none overtakes it
+            r.ses->busy = true;
+            r.t_start = Clock::now();
+            active += r.ses->n;
+            started.push_back(*it);
+            it = sv->queue.erase(it);
+        }
+    }
+    if (started.empty())
+        return true;
+    int m = 0;
+    for (auto& r : started)
+        for (int i = 0; i < r->ses->n; ++i, ++m) {
+            sv->h_start_ids.p[m] = r->ses->slots[i];
+            // one OU stream per (request, world)
+            sv->h_start_seeds.p[m] = r->ou_seed * 0x9e3779b97f4a7c15ull + (unsigned long long)i;
+        }
+    if (!ok(cudaMemcpyAsync(sv->d_start_ids.p, sv->h_start_ids.p, sizeof(int) * m, cudaMemcpyHostToDevice, sv->stream),
+            "start ids") ||
+        !ok(cudaMemcpyAsync(sv->d_start_seeds.p, sv->h_start_seeds.p, sizeof(unsigned long long) * m,
+                            cudaMemcpyHostToDevice, sv->stream),
+            "start seeds"))
+        return false;
+    k_start<<<(m + 127) / 128, 128, 0, sv->stream>>>(sv->d_start_ids.p, sv->d_start_seeds.p, m, sv->d_seed.p,
+                                                     sv->d_ou.p, sv->d_t.p);
+    if (!ok(cudaGetLastError(), "start kernel"))
+        return false;
+    sv->running.insert(sv->running.end(), started.begin(), started.end());
+    return true;
+}
+
+// Reads back the final observations of finished requests, in pinned chunks.
+bool read_obs(arc_server* sv, const std::vector<std::shared_ptr<Request>>& finished)
+{
+    std::vector<std::pair<Request*, int>> owners;
+    size_t ri = 0;
+    int wi = 0;
+    while (ri < finished.size()) {
+        int m = 0;
+        owners.clear();
+        while (ri < finished.size() && m < kReadChunk) {
+            Request* r = finished[ri].get();
+            if (!r->obs) {
+                ++ri;
+                continue;
+            }
+            sv->h_ids.p[m] = r->ses->slots[wi];
+            owners.push_back({r, wi});
+            ++m;
+            if (++wi == r->ses->n) {
+                wi = 0;
+                ++ri;
+            }
+        }
+        if (m == 0)
+            break;
+        if (!ok(cudaMemcpyAsync(sv->d_ids.p, sv->h_ids.p, sizeof(int) * m, cudaMemcpyHostToDevice, sv->stream),
+                "obs ids"))
+            return false;
+        const long long total = (long long)m * kObs;
+        k_gather_obs<<<(unsigned)((total + 255) / 256), 256, 0, sv->stream>>>(sv->d_ids.p, m, sv->env_obs,
+                                                                              sv->d_obs.p);
+        if (!ok(cudaGetLastError(), "obs gather") ||
+            !ok(cudaMemcpyAsync(sv->h_obs.p, sv->d_obs.p, sizeof(float) * total, cudaMemcpyDeviceToHost, sv->stream),
+                "obs copy") ||
+            !ok(cudaStreamSynchronize(sv->stream), "obs read-back"))
+            return false;
+        for (int k = 0; k < m; ++k)
+            std::memcpy(owners[k].first->obs + (size_t)owners[k].second * kObs, sv->h_obs.p + (size_t)k * kObs,
+                        sizeof(float) * kObs);
+    }
+    return true;
+}
+
+// One control step of every running request's worlds; completes finished requests.
 bool tick(arc_server* sv)
 {
     const auto t0 = Clock::now();
     int n = 0;
     bool any_given = false;
-    for (auto& r : sv->active) {
+    for (auto& r : sv->running) {
         const bool given = !r->actions.empty();
         any_given |= given;
-        for (int i = 0; i < r->n; ++i, ++n) {
-            sv->h_ids.p[n] = r->slots[i];
+        const int rn = r->ses->n;
+        for (int i = 0; i < rn; ++i, ++n) {
+            sv->h_ids.p[n] = r->ses->slots[i];
             sv->h_use.p[n] = given;
             if (given)
                 std::memcpy(sv->h_given.p + (size_t)n * kJ,
-                            r->actions.data() + ((size_t)r->done_steps * r->n + i) * kJ, sizeof(float) * kJ);
+                            r->actions.data() + ((size_t)r->done_steps * rn + i) * kJ, sizeof(float) * kJ);
         }
     }
     if (n == 0)
         return true;
     cudaStream_t st = sv->stream;
-    if (!ok(cudaMemcpyAsync(sv->d_ids.p, sv->h_ids.p, sizeof(int) * n, cudaMemcpyHostToDevice, st), sv, "ids") ||
-        !ok(cudaMemcpyAsync(sv->d_use.p, sv->h_use.p, n, cudaMemcpyHostToDevice, st), sv, "flags"))
+    if (!ok(cudaMemcpyAsync(sv->d_ids.p, sv->h_ids.p, sizeof(int) * n, cudaMemcpyHostToDevice, st), "ids") ||
+        !ok(cudaMemcpyAsync(sv->d_use.p, sv->h_use.p, n, cudaMemcpyHostToDevice, st), "flags"))
         return false;
     if (any_given &&
-        !ok(cudaMemcpyAsync(sv->d_given.p, sv->h_given.p, sizeof(float) * kJ * n, cudaMemcpyHostToDevice, st), sv,
+        !ok(cudaMemcpyAsync(sv->d_given.p, sv->h_given.p, sizeof(float) * kJ * n, cudaMemcpyHostToDevice, st),
             "actions"))
         return false;
     k_tick_actions<<<(n + 127) / 128, 128, 0, st>>>(sv->d_ids.p, n, sv->d_given.p, sv->d_use.p, sv->d_seed.p,
-                                                    sv->d_ou.p, sv->d_t.p, sv->d_actions.p);
-    if (!ok(cudaGetLastError(), sv, "action kernel"))
+                                                    sv->d_ou.p, sv->d_t.p, sv->env_actions);
+    if (!ok(cudaGetLastError(), "action kernel"))
         return false;
-    if (arc_sim_step_ids(sv->sim, sv->d_ids.p, n, nullptr, sv->d_actions.p, st) != ARC_OK)
+    if (arc_env_step_ids(sv->sim, sv->d_ids.p, n, st) != ARC_OK)
         return false;
-    if (!ok(cudaStreamSynchronize(st), sv, "tick"))
+    k_gather_step<<<(n + 127) / 128, 128, 0, st>>>(sv->d_ids.p, n, sv->env_reward, sv->env_terminated,
+                                                   sv->env_truncated, sv->d_reward.p, sv->d_done.p);
+    if (!ok(cudaGetLastError(), "gather kernel") ||
+        !ok(cudaMemcpyAsync(sv->h_reward.p, sv->d_reward.p, sizeof(float) * n, cudaMemcpyDeviceToHost, st),
+            "rewards") ||
+        !ok(cudaMemcpyAsync(sv->h_done.p, sv->d_done.p, n, cudaMemcpyDeviceToHost, st), "done flags") ||
+        !ok(cudaStreamSynchronize(st), "tick"))
         return false;
     const auto t1 = Clock::now();
-    // evict finished requests
     std::vector<std::shared_ptr<Request>> keep, finished;
-    for (auto& r : sv->active)
+    long long ended = 0;
+    int off = 0;
+    for (auto& r : sv->running) {
+        const int rn = r->ses->n;
+        const size_t at = (size_t)r->done_steps * rn;
+        if (r->reward)
+            std::memcpy(r->reward + at, sv->h_reward.p + off, sizeof(float) * rn);
+        if (r->done)
+            std::memcpy(r->done + at, sv->h_done.p + off, rn);
+        for (int i = 0; i < rn; ++i)
+            ended += sv->h_done.p[off + i] != 0;
+        off += rn;
         (++r->done_steps >= r->steps ? finished : keep).push_back(r);
-    // results of every finished request, in pinned chunks
-    const size_t row_n = (size_t)sv->row;
-    for (auto& r : finished)
-        if (!r->user_out)
-            r->out.resize((size_t)r->n * row_n);
-    size_t total = 0;
-    for (auto& r : finished)
-        total += r->n;
-    std::vector<std::pair<Request*, int>> owners;  // (request, world index) of each row of the chunk
-    size_t row = 0, ri = 0, wi = 0;
-    while (row < total) {
-        const int m = (int)std::min<size_t>(kReadChunk, total - row);
-        owners.resize(m);
-        for (int k = 0; k < m; ++k) {
-            Request* r = finished[ri].get();
-            sv->h_read_ids.p[k] = r->slots[wi];
-            owners[k] = {r, (int)wi};
-            if (++wi == (size_t)r->n) {
-                wi = 0;
-                ++ri;
-            }
-        }
-        int rc = ARC_OK;
-        if (sv->result == ARC_SERVE_STATE) {
-            rc = arc_sim_get_state(sv->sim, sv->h_read_ids.p, m, sv->h_state.p);
-        } else {
-            double* d = sv->d_obs.p;
-            double *d_root = d, *d_rot = d + (size_t)m * 13, *d_j = d_rot + (size_t)m * 9,
-                   *d_c = d_j + (size_t)m * 36;
-            rc = (ok(cudaMemcpyAsync(sv->d_read_ids.p, sv->h_read_ids.p, sizeof(int) * m, cudaMemcpyHostToDevice,
-                                     sv->stream), sv, "read ids")
-                      ? arc_sim_observe_ids(sv->sim, sv->d_read_ids.p, m, d_root, d_rot, d_j, d_c, sv->d_flags.p,
-                                            sv->stream)
-                      : ARC_ERR_CUDA);
-            if (rc == ARC_OK &&
-                !(ok(cudaMemcpyAsync(sv->h_state.p, d, sizeof(double) * (size_t)m * (kObsRow - 1),
-                                     cudaMemcpyDeviceToHost, sv->stream), sv, "observations") &&
-                  ok(cudaMemcpyAsync(sv->h_flags.p, sv->d_flags.p, sizeof(int) * m, cudaMemcpyDeviceToHost,
-                                     sv->stream), sv, "flags") &&
-                  ok(cudaStreamSynchronize(sv->stream), sv, "read back")))
-                rc = ARC_ERR_CUDA;
-        }
-        for (int k = 0; k < m; ++k) {
-            Request* r = owners[k].first;
-            double* dst = r->dest() + (size_t)owners[k].second * row_n;
-            if (rc) {
-                r->status = rc;
-            } else if (sv->result == ARC_SERVE_STATE) {
-                std::memcpy(dst, sv->h_state.p + (size_t)k * row_n, sizeof(double) * row_n);
-            } else {
-                const double* h = sv->h_state.p;
-                std::memcpy(dst, h + (size_t)k * 13, sizeof(double) * 13);
-                std::memcpy(dst + 13, h + (size_t)m * 13 + (size_t)k * 9, sizeof(double) * 9);
-                std::memcpy(dst + 22, h + (size_t)m * 22 + (size_t)k * 36, sizeof(double) * 36);
-                std::memcpy(dst + 58, h + (size_t)m * 58 + (size_t)k * 6, sizeof(double) * 6);
-                dst[64] = (double)sv->h_flags.p[k];
-            }
-        }
-        row += m;
     }
-    sv->active.swap(keep);
+    const bool read = read_obs(sv, finished);
+    sv->running.swap(keep);
     std::lock_guard<std::mutex> lock(sv->mu);
     sv->step_s += std::chrono::duration<double>(t1 - t0).count();
-    sv->evict_s += std::chrono::duration<double>(Clock::now() - t1).count();
+    sv->read_s += std::chrono::duration<double>(Clock::now() - t1).count();
     ++sv->ticks;
     sv->world_steps += n;
+    sv->episodes_ended += ended;
     sv->max_active = std::max(sv->max_active, n);
     if (!finished.empty()) {
         const auto now = Clock::now();
         for (auto& r : finished) {
-            sv->free_slots.insert(sv->free_slots.end(), r->slots.begin(), r->slots.end());
             r->t_done = now;
-            r->done = true;
+            r->status = read ? 0 : ARC_ERR_CUDA;
+            r->finished = true;
+            r->ses->busy = false;
+            --r->ses->pending;
             ++sv->completed;
         }
         sv->cv_done.notify_all();
     }
-    return true;
+    return read;
+}
+
+bool has_work(arc_server* sv)
+{
+    if (sv->stop || !sv->running.empty())
+        return true;
+    for (auto& r : sv->queue)
+        if (r->ses->admitted && !r->ses->busy)
+            return true;
+    if (!sv->waiting.empty() && (int)sv->free_slots.size() >= sv->waiting.front()->n)
+        return true;
+    for (auto& kv : sv->sessions)
+        if (kv.second->closed && kv.second->pending == 0)
+            return true;
+    return false;
+}
+
+void fail_all(arc_server* sv, int status)
+{
+    for (auto& r : sv->running) {
+        r->status = status;
+        r->finished = true;
+    }
+    sv->running.clear();
+    for (auto& r : sv->queue) {
+        r->status = status;
+        r->finished = true;
+    }
+    sv->queue.clear();
+    sv->cv_done.notify_all();
 }
 
 void engine_loop(arc_server* sv)
@@ -345,33 +472,21 @@ void engine_loop(arc_server* sv)
     for (;;) {
         {
             std::unique_lock<std::mutex> lock(sv->mu);
-            sv->cv_work.wait(lock, [&] { return sv->stop || !sv->queue.empty() || !sv->active.empty(); });
+            sv->cv_work.wait(lock, [&] { return has_work(sv); });
             if (sv->stop)
                 return;
         }
         const auto t0 = Clock::now();
         bool good = admit(sv);
-        {
-            std::lock_guard<std::mutex> lock(sv->mu);
-            sv->admit_s += std::chrono::duration<double>(Clock::now() - t0).count();
-        }
-        good = good && tick(sv);
+        const auto t1 = Clock::now();
+        good = good && start(sv) && tick(sv);
         std::lock_guard<std::mutex> lock(sv->mu);
+        sv->admit_s += std::chrono::duration<double>(t1 - t0).count();
         sv->busy_s += std::chrono::duration<double>(Clock::now() - t0).count();
         if (!good) {
             // fail everything outstanding; the engine stops stepping
             sv->error = ARC_ERR_CUDA;
-            for (auto& r : sv->active) {
-                r->status = sv->error;
-                r->done = true;
-            }
-            sv->active.clear();
-            for (auto& r : sv->queue) {
-                r->status = sv->error;
-                r->done = true;
-            }
-            sv->queue.clear();
-            sv->cv_done.notify_all();
+            fail_all(sv, sv->error);
             sv->stop = true;
             return;
         }
@@ -380,9 +495,10 @@ void engine_loop(arc_server* sv)
 
 }  // namespace
 
-extern "C" arc_server* arc_server_create(int capacity, double dt, int substeps, int grid, double cell, int result)
+extern "C" arc_server* arc_server_create(int capacity, double dt, int substeps, int grid, double cell,
+                                         const arc_task_config* cfg, int tick_cap)
 {
-    if (capacity <= 0 || (result != ARC_SERVE_STATE && result != ARC_SERVE_OBSERVE))
+    if (capacity <= 0 || tick_cap < 0)
         return nullptr;
     auto* sv = new arc_server();
     cudaGetDevice(&sv->device);
@@ -391,36 +507,51 @@ extern "C" arc_server* arc_server_create(int capacity, double dt, int substeps, 
         delete sv;
         return nullptr;
     }
+    arc_task_config c;
+    if (cfg) {
+        c = *cfg;
+    } else {
+        arc_task_config_default(&c);
+        c.curriculum = 0;  // each session's worlds keep the difficulty it asked for
+    }
+    c.dt = dt;
     sv->capacity = capacity;
-    sv->state_size = arc_sim_state_size(sv->sim);
-    sv->result = result;
-    sv->row = result == ARC_SERVE_STATE ? sv->state_size : kObsRow;
-    const size_t chunk = (size_t)std::min(capacity, kReadChunk);
+    sv->tick_cap = tick_cap > 0 ? tick_cap : capacity;
     arc_sim_set_kernel(sv->sim, ARC_KERNEL_WARPS, 32);
+    arc_sim_set_work_queue(sv->sim, 1);
     sv->stream = static_cast<cudaStream_t>(arc_sim_stream(sv->sim));
-    const size_t c = (size_t)capacity;
-    const bool good = cudaMalloc(&sv->d_ids.p, c * sizeof(int)) == cudaSuccess &&
-                      cudaMalloc(&sv->d_admit_ids.p, c * sizeof(int)) == cudaSuccess &&
-                      cudaMalloc(&sv->d_actions.p, c * kJ * sizeof(float)) == cudaSuccess &&
-                      cudaMalloc(&sv->d_ou.p, c * kJ * sizeof(float)) == cudaSuccess &&
-                      cudaMalloc(&sv->d_given.p, c * kJ * sizeof(float)) == cudaSuccess &&
-                      cudaMalloc(&sv->d_t.p, c * sizeof(int)) == cudaSuccess &&
-                      cudaMalloc(&sv->d_seed.p, c * sizeof(unsigned long long)) == cudaSuccess &&
-                      cudaMalloc(&sv->d_admit_seeds.p, c * sizeof(unsigned long long)) == cudaSuccess &&
-                      cudaMalloc(&sv->d_use.p, c) == cudaSuccess &&
-                      cudaMallocHost(&sv->h_ids.p, c * sizeof(int)) == cudaSuccess &&
-                      cudaMallocHost(&sv->h_admit_ids.p, c * sizeof(int)) == cudaSuccess &&
-                      cudaMallocHost(&sv->h_given.p, c * kJ * sizeof(float)) == cudaSuccess &&
-                      cudaMallocHost(&sv->h_use.p, c) == cudaSuccess &&
-                      cudaMallocHost(&sv->h_admit_seeds.p, c * sizeof(unsigned long long)) == cudaSuccess &&
-                      cudaMallocHost(&sv->h_state.p, chunk * sv->row * sizeof(double)) == cudaSuccess &&
-                      cudaMallocHost(&sv->h_read_ids.p, chunk * sizeof(int)) == cudaSuccess &&
-                      cudaMallocHost(&sv->h_flags.p, chunk * sizeof(int)) == cudaSuccess &&
-                      cudaMalloc(&sv->d_read_ids.p, chunk * sizeof(int)) == cudaSuccess &&
-                      cudaMalloc(&sv->d_flags.p, chunk * sizeof(int)) == cudaSuccess &&
-                      cudaMalloc(&sv->d_obs.p, chunk * (kObsRow - 1) * sizeof(double)) == cudaSuccess;
+    void* p = nullptr;
+    bool good = arc_env_init(sv->sim, &c, 0x5eedull) == ARC_OK;
+    auto buffer = [&](int which) {
+        p = nullptr;
+        good = good && arc_env_buffer(sv->sim, which, &p, nullptr, nullptr, nullptr, nullptr) == ARC_OK;
+        return p;
+    };
+    sv->env_actions = static_cast<float*>(buffer(ARC_ENV_ACTIONS));
+    sv->env_obs = static_cast<float*>(buffer(ARC_ENV_OBS));
+    sv->env_reward = static_cast<float*>(buffer(ARC_ENV_REWARD));
+    sv->env_terminated = static_cast<unsigned char*>(buffer(ARC_ENV_TERMINATED));
+    sv->env_truncated = static_cast<unsigned char*>(buffer(ARC_ENV_TRUNCATED));
+    const size_t n = (size_t)capacity, chunk = (size_t)std::min(capacity, kReadChunk);
+    good = good && cudaMalloc(&sv->d_ids.p, n * sizeof(int)) == cudaSuccess &&
+           cudaMalloc(&sv->d_start_ids.p, n * sizeof(int)) == cudaSuccess &&
+           cudaMalloc(&sv->d_ou.p, n * kJ * sizeof(float)) == cudaSuccess &&
+           cudaMalloc(&sv->d_given.p, n * kJ * sizeof(float)) == cudaSuccess &&
+           cudaMalloc(&sv->d_reward.p, n * sizeof(float)) == cudaSuccess &&
+           cudaMalloc(&sv->d_obs.p, chunk * kObs * sizeof(float)) == cudaSuccess &&
+           cudaMalloc(&sv->d_t.p, n * sizeof(int)) == cudaSuccess &&
+           cudaMalloc(&sv->d_seed.p, n * sizeof(unsigned long long)) == cudaSuccess &&
+           cudaMalloc(&sv->d_start_seeds.p, n * sizeof(unsigned long long)) == cudaSuccess &&
+           cudaMalloc(&sv->d_use.p, n) == cudaSuccess && cudaMalloc(&sv->d_done.p, n) == cudaSuccess &&
+           cudaMallocHost(&sv->h_ids.p, n * sizeof(int)) == cudaSuccess &&
+           cudaMallocHost(&sv->h_start_ids.p, n * sizeof(int)) == cudaSuccess &&
+           cudaMallocHost(&sv->h_given.p, n * kJ * sizeof(float)) == cudaSuccess &&
+           cudaMallocHost(&sv->h_reward.p, n * sizeof(float)) == cudaSuccess &&
+           cudaMallocHost(&sv->h_obs.p, chunk * kObs * sizeof(float)) == cudaSuccess &&
+           cudaMallocHost(&sv->h_use.p, n) == cudaSuccess && cudaMallocHost(&sv->h_done.p, n) == cudaSuccess &&
+           cudaMallocHost(&sv->h_start_seeds.p, n * sizeof(unsigned long long)) == cudaSuccess;
     if (!good) {
-        std::fprintf(stderr, "arc_server_create: allocation failed for %d slots\n", capacity);
+        std::fprintf(stderr, "arc_server_create: set-up failed for %d slots\n", capacity);
         arc_sim_destroy(sv->sim);
         delete sv;
         return nullptr;
@@ -441,7 +572,7 @@ extern "C" void arc_server_destroy(arc_server* sv)
         sv->stop = true;
         for (auto& r : sv->queue) {
             r->status = ARC_ERR_ARG;
-            r->done = true;
+            r->finished = true;
         }
         sv->queue.clear();
         sv->cv_done.notify_all();
@@ -453,26 +584,51 @@ extern "C" void arc_server_destroy(arc_server* sv)
     delete sv;
 }
 
-extern "C" long long arc_server_submit(arc_server* sv, int n_worlds, int n_steps, const unsigned* seeds,
-                                       const double* difficulty, const float* actions, unsigned long long ou_seed,
-                                       double* out)
+extern "C" long long arc_server_open(arc_server* sv, int n_worlds, const double* difficulty, unsigned long long key)
 {
-    if (!sv || n_worlds <= 0 || n_worlds > sv->capacity || n_steps <= 0 || !seeds || !difficulty)
+    if (!sv || n_worlds <= 0 || !difficulty)
+        return ARC_ERR_ARG;
+    auto s = std::make_shared<Session>();
+    s->n = n_worlds;
+    s->key = key;
+    s->difficulty.assign(difficulty, difficulty + n_worlds);
+    {
+        std::lock_guard<std::mutex> lock(sv->mu);
+        if (sv->stop)
+            return sv->error ? sv->error : ARC_ERR_ARG;
+        if (n_worlds > sv->capacity)
+            return ARC_ERR_ARG;
+        s->id = sv->next_id++;
+        sv->sessions[s->id] = s;
+        sv->waiting.push_back(s);
+    }
+    sv->cv_work.notify_one();
+    return s->id;
+}
+
+extern "C" long long arc_server_request(arc_server* sv, long long session, int n_steps, const float* actions,
+                                        unsigned long long ou_seed, float* obs, float* reward, unsigned char* done)
+{
+    if (!sv || n_steps <= 0)
         return ARC_ERR_ARG;
     auto r = std::make_shared<Request>();
-    r->n = n_worlds;
     r->steps = n_steps;
-    r->seeds.assign(seeds, seeds + n_worlds);
-    r->difficulty.assign(difficulty, difficulty + n_worlds);
-    if (actions)
-        r->actions.assign(actions, actions + (size_t)n_steps * n_worlds * kJ);
     r->ou_seed = ou_seed;
-    r->user_out = out;
+    r->obs = obs;
+    r->reward = reward;
+    r->done = done;
     r->t_submit = Clock::now();
     {
         std::lock_guard<std::mutex> lock(sv->mu);
         if (sv->stop)
             return sv->error ? sv->error : ARC_ERR_ARG;
+        auto it = sv->sessions.find(session);
+        if (it == sv->sessions.end() || it->second->closed)
+            return ARC_ERR_ARG;
+        r->ses = it->second;
+        if (actions)
+            r->actions.assign(actions, actions + (size_t)n_steps * r->ses->n * kJ);
+        ++r->ses->pending;
         r->id = sv->next_id++;
         sv->by_id[r->id] = r;
         sv->queue.push_back(r);
@@ -481,7 +637,7 @@ extern "C" long long arc_server_submit(arc_server* sv, int n_worlds, int n_steps
     return r->id;
 }
 
-extern "C" int arc_server_wait(arc_server* sv, long long id, double timeout_s, double* out, double* times)
+extern "C" int arc_server_wait(arc_server* sv, long long id, double timeout_s, double* times)
 {
     if (!sv)
         return ARC_ERR_ARG;
@@ -494,20 +650,33 @@ extern "C" int arc_server_wait(arc_server* sv, long long id, double timeout_s, d
         r = it->second;
         const auto until = Clock::now() + std::chrono::duration_cast<Clock::duration>(
                                               std::chrono::duration<double>(std::max(timeout_s, 0.0)));
-        if (!sv->cv_done.wait_until(lock, until, [&] { return r->done; }))
+        if (!sv->cv_done.wait_until(lock, until, [&] { return r->finished; }))
             return 0;
         sv->by_id.erase(id);
     }
     if (r->status)
         return r->status;
-    if (out && !r->user_out)
-        std::memcpy(out, r->out.data(), sizeof(double) * r->out.size());
     if (times) {
-        times[0] = std::chrono::duration<double>(r->t_admit - r->t_submit).count();
-        times[1] = std::chrono::duration<double>(r->t_done - r->t_admit).count();
+        times[0] = std::chrono::duration<double>(r->t_start - r->t_submit).count();
+        times[1] = std::chrono::duration<double>(r->t_done - r->t_start).count();
         times[2] = std::chrono::duration<double>(r->t_done - r->t_submit).count();
     }
     return 1;
+}
+
+extern "C" int arc_server_close(arc_server* sv, long long session)
+{
+    if (!sv)
+        return ARC_ERR_ARG;
+    {
+        std::lock_guard<std::mutex> lock(sv->mu);
+        auto it = sv->sessions.find(session);
+        if (it == sv->sessions.end() || it->second->closed)
+            return ARC_ERR_ARG;
+        it->second->closed = true;
+    }
+    sv->cv_work.notify_one();
+    return ARC_OK;
 }
 
 extern "C" int arc_server_stats(arc_server* sv, double* stats)
@@ -515,6 +684,9 @@ extern "C" int arc_server_stats(arc_server* sv, double* stats)
     if (!sv || !stats)
         return ARC_ERR_ARG;
     std::lock_guard<std::mutex> lock(sv->mu);
+    int resident = 0;
+    for (auto& kv : sv->sessions)
+        resident += kv.second->admitted ? kv.second->n : 0;
     stats[0] = (double)sv->ticks;
     stats[1] = (double)sv->world_steps;
     stats[2] = sv->busy_s;
@@ -523,6 +695,9 @@ extern "C" int arc_server_stats(arc_server* sv, double* stats)
     stats[5] = (double)sv->queue.size();
     stats[6] = sv->admit_s;
     stats[7] = sv->step_s;
-    stats[8] = sv->evict_s;
+    stats[8] = sv->read_s;
+    stats[9] = (double)sv->episodes_ended;
+    stats[10] = (double)resident;
+    stats[11] = (double)sv->waiting.size();
     return sv->error;
 }

@@ -62,6 +62,9 @@ struct arc_sim {
     size_t th_count = 0;         // columns in the terrain pool
     int* queue = nullptr;        // work queue of the warp-per-leg kernel (two ints)
     bool use_queue = false;
+    bool fused = true;  // the env's control step as one launch where it applies (arc_env_set_fused)
+    int substep_tile = 0;      // warp-per-leg step: substeps per launch (0: the whole control step)
+    float* tile_q = nullptr;   // [n][13][4] position-pass quaternions between tiles
     void* spill = nullptr;
     int spill_per_lane = 0, lane_cap = 0;
     double spill_cell = 0.0;
@@ -83,7 +86,7 @@ struct arc_sim {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t graph_stream = nullptr;
-    int graph_kernel = -1, graph_wpc = -1, graph_queue = -1;  // the step form the graph captured
+    int graph_kernel = -1, graph_wpc = -1, graph_queue = -1, graph_fused = -1, graph_tile = -1;  // the captured form
     // arc_env_step_host: world indices 0..n-1, per-chunk ended-world lists and
     // counts, the two copy streams and their events
     int* iota = nullptr;
@@ -269,7 +272,7 @@ void free_all(arc_sim* s)
         cudaFree(p);
     void* ps[] = {s->rec, s->sph, s->unstable, s->time, s->th, s->toff, s->tg, s->tgd, s->grid_of, s->spill, s->queue,
                   s->st_in.p, s->st_in2.p, s->st_in3.p, s->st_out.p, s->iota, s->chunk_done, s->chunk_count,
-                  s->part_queue};
+                  s->part_queue, s->tile_q};
     for (void* p : ps)
         if (p)
             cudaFree(p);
@@ -578,7 +581,7 @@ template <> cudaError_t launch_warps_if_fp32<float>(arc_sim* s, const DevModel<f
                                                     cudaStream_t st)
 {
     return launch_step_warps(M, W, A, static_cast<float*>(s->spill), s->spill_per_lane, s->lane_cap, ids, n_items,
-                             queue, st);
+                             queue, st, s->substep_tile, s->tile_q);
 }
 
 // ids: device list of n_ids distinct worlds to step (NULL: all worlds).
@@ -921,8 +924,9 @@ int arc_sim_set_kernel(arc_sim* s, int kernel, int worlds_per_cta)
     if (kernel == ARC_KERNEL_LEGS) {
         if (!s->model.leaper)
             return fail(s, ARC_ERR_UNSUPPORTED, "leg-parallel kernel needs the quadruped's topology");
-        if (worlds_per_cta != 8 && worlds_per_cta != 16 && worlds_per_cta != 32 && worlds_per_cta != 64)
-            return fail(s, ARC_ERR_ARG, "worlds_per_cta must be 8, 16, 32 or 64");
+        if (worlds_per_cta != 1 && worlds_per_cta != 2 && worlds_per_cta != 4 && worlds_per_cta != 8 &&
+            worlds_per_cta != 16 && worlds_per_cta != 32 && worlds_per_cta != 64)
+            return fail(s, ARC_ERR_ARG, "worlds_per_cta must be 1, 2, 4, 8, 16, 32 or 64");
         const size_t smem = s->fp64 ? fast_smem_bytes<double>(s->stride, worlds_per_cta)
                                     : fast_smem_bytes<float>(s->stride, worlds_per_cta);
         if (smem > 227 * 1024)
@@ -1213,6 +1217,24 @@ int arc_sim_set_work_queue(arc_sim* s, int on)
     return ARC_OK;
 }
 
+int arc_sim_set_substep_tile(arc_sim* s, int tile)
+{
+    if (tile < 0)
+        return fail(s, ARC_ERR_ARG, "arc_sim_set_substep_tile: tile < 0");
+    if (tile > 0 && tile < s->substeps && !s->tile_q &&
+        check(s, cudaMalloc((void**)&s->tile_q, sizeof(float) * 13 * 4 * (size_t)std::max(s->n, 1)),
+              "cudaMalloc(tile quaternions)"))
+        return ARC_ERR_CUDA;
+    s->substep_tile = tile;
+    return ARC_OK;
+}
+
+int arc_env_set_fused(arc_sim* s, int on)
+{
+    s->fused = on != 0;
+    return ARC_OK;
+}
+
 int arc_device_checks(unsigned long long* failures, int* first_site, long long* first_index, int clear)
 {
     unsigned long long total = 0;
@@ -1371,9 +1393,33 @@ template <class R> int env_reset_done(arc_sim* s, cudaStream_t st)
                  "task reset kernel");
 }
 
+// Whether the env's control step runs as one launch (the warp-per-leg step
+// and the task layer in k_control_step): FP32, the quadruped, that kernel.
+bool fused_applies(const arc_sim* s)
+{
+    return s->fused && !s->fp64 && s->mf.leaper && s->substeps <= kFastMaxSubsteps && s->kernel == ARC_KERNEL_WARPS &&
+           (s->substep_tile <= 0 || s->substep_tile >= s->substeps);
+}
+
+// One launch of the fused control step over ids[0 .. n) (NULL: every
+// world), its ended worlds into O's list; O.done_count is zeroed first.
+int env_control_step(arc_sim* s, const float* actions, const TaskOut& O, const int* ids, int n, int* queue,
+                     cudaStream_t st)
+{
+    if (check(s, cudaMemsetAsync(O.done_count, 0, sizeof(int), st), "memset done_count"))
+        return ARC_ERR_CUDA;
+    return check(s,
+                 launch_control_step(s->mf, s->rm, view<float>(s), (TerrainGeom<float>*)s->tg, s->tgd, s->grid_of,
+                                     s->cell, s->tp, s->ts, O, actions, static_cast<float*>(s->spill),
+                                     s->spill_per_lane, s->lane_cap, ids, n, queue, st),
+                 "control step kernel");
+}
+
 // the whole control step of ArcVecEnv.step_wait, as launched into `st`
 int env_step_launches(arc_sim* s, const float* actions, cudaStream_t st)
 {
+    if (fused_applies(s))
+        return env_control_step(s, actions, s->to, nullptr, s->n, s->use_queue ? s->queue : nullptr, st);
     Actuation A{nullptr, actions};
     int rc = step_any(s, A, st);
     if (rc)
@@ -1506,12 +1552,16 @@ int ensure_step_host(arc_sim* s)
 // part >= 0: a part of arc_env_step_part (its own work queue).
 template <class R> int env_step_chunk(arc_sim* s, int first, int count, int c, cudaStream_t st, int part = -1)
 {
-    Actuation A{nullptr, s->actions};
-    if (int rc = step_any(s, A, st, s->iota + first, count, part))
-        return rc;
     TaskOut O = s->to;
     O.done_list = s->chunk_done + first;
     O.done_count = s->chunk_count + c;
+    if (fused_applies(s)) {
+        int* queue = !s->use_queue ? nullptr : (part >= 0 ? s->part_queue + 2 * part : s->queue);
+        return env_control_step(s, s->actions, O, s->iota + first, count, queue, st);
+    }
+    Actuation A{nullptr, s->actions};
+    if (int rc = step_any(s, A, st, s->iota + first, count, part))
+        return rc;
     if (check(s, launch_task_step<R>(dev_model<R>(s), view<R>(s), s->tp, s->ts, O, s->actions, 2, st, first, count),
               "task step kernel") ||
         check(s, launch_task_heights<R>(dev_model<R>(s), view<R>(s), s->tp, O, st, first, count), "task heights kernel"))
@@ -1765,6 +1815,80 @@ int arc_env_reset(arc_sim* s, const int* ids, int n_ids, void* stream)
     return check(s, cudaStreamSynchronize(st), "arc_env_reset");
 }
 
+int arc_env_admit(arc_sim* s, const int* ids, int n_ids, const double* difficulty, const unsigned* keys, void* stream)
+{
+    if (int rc = env_check(s))
+        return rc;
+    if (n_ids < 0 || (n_ids > 0 && (!ids || !difficulty || !keys)))
+        return fail(s, ARC_ERR_ARG, "arc_env_admit: bad arguments");
+    if (n_ids == 0)
+        return ARC_OK;
+    if (!ids_ok(s, ids, n_ids))
+        return fail(s, ARC_ERR_ARG, "arc_env_admit: world index out of range");
+    cudaStream_t st = stream_of(s, stream);
+    if (!s->ts.key) {
+        // every world keeps its index as its key until a tenant gives it one
+        bool ok = true;
+        unsigned* key = env_alloc<unsigned>(s, (size_t)s->n, ok);
+        if (!ok)
+            return fail(s, ARC_ERR_CUDA, "arc_env_admit: device allocation failed");
+        k_iota<<<(s->n + 255) / 256, 256, 0, st>>>(reinterpret_cast<int*>(key), s->n);
+        if (check(s, cudaGetLastError(), "world keys"))
+            return ARC_ERR_CUDA;
+        s->ts.key = key;
+    }
+    const size_t n = (size_t)n_ids;
+    unsigned char* d = (unsigned char*)grow(s, s->st_in3, n * (sizeof(int) + sizeof(double) + sizeof(unsigned)));
+    if (!d)
+        return ARC_ERR_CUDA;
+    double* d_diff = reinterpret_cast<double*>(d);
+    int* d_ids = reinterpret_cast<int*>(d + n * sizeof(double));
+    unsigned* d_keys = reinterpret_cast<unsigned*>(d + n * (sizeof(double) + sizeof(int)));
+    if (check(s, cudaMemcpyAsync(d_diff, difficulty, n * sizeof(double), cudaMemcpyHostToDevice, st), "admit") ||
+        check(s, cudaMemcpyAsync(d_ids, ids, n * sizeof(int), cudaMemcpyHostToDevice, st), "admit") ||
+        check(s, cudaMemcpyAsync(d_keys, keys, n * sizeof(unsigned), cudaMemcpyHostToDevice, st), "admit"))
+        return ARC_ERR_CUDA;
+    cudaError_t e =
+        s->fp64 ? launch_env_admit<double>(s->md, s->rm, view<double>(s), (TerrainGeom<double>*)s->tg, s->tgd,
+                                           s->grid_of, s->cell, s->tp, s->ts, s->to.obs, d_ids, d_diff, d_keys,
+                                           n_ids, st)
+                : launch_env_admit<float>(s->mf, s->rm, view<float>(s), (TerrainGeom<float>*)s->tg, s->tgd,
+                                          s->grid_of, s->cell, s->tp, s->ts, s->to.obs, d_ids, d_diff, d_keys,
+                                          n_ids, st);
+    if (check(s, e, "admit kernels"))
+        return ARC_ERR_CUDA;
+    return check(s, cudaStreamSynchronize(st), "arc_env_admit");
+}
+
+int arc_env_step_ids(arc_sim* s, const int* d_ids, int n_ids, void* stream)
+{
+    if (int rc = env_check(s))
+        return rc;
+    if (n_ids < 0 || (n_ids > 0 && !d_ids))
+        return fail(s, ARC_ERR_ARG, "arc_env_step_ids: bad arguments");
+    if (n_ids == 0)
+        return ARC_OK;
+    cudaStream_t st = stream_of(s, stream);
+    if (fused_applies(s))
+        return env_control_step(s, s->actions, s->to, d_ids, n_ids, s->use_queue ? s->queue : nullptr, st);
+    Actuation A{nullptr, s->actions};
+    if (int rc = step_any(s, A, st, d_ids, n_ids))
+        return rc;
+    if (check(s, cudaMemsetAsync(s->to.done_count, 0, sizeof(int), st), "memset done_count"))
+        return ARC_ERR_CUDA;
+    cudaError_t e = s->fp64 ? launch_task_step<double>(s->md, view<double>(s), s->tp, s->ts, s->to, s->actions, 2, st,
+                                                       0, n_ids, d_ids)
+                            : launch_task_step<float>(s->mf, view<float>(s), s->tp, s->ts, s->to, s->actions, 2, st,
+                                                      0, n_ids, d_ids);
+    if (check(s, e, "task step kernel"))
+        return ARC_ERR_CUDA;
+    e = s->fp64 ? launch_task_heights<double>(s->md, view<double>(s), s->tp, s->to, st, 0, n_ids, d_ids)
+                : launch_task_heights<float>(s->mf, view<float>(s), s->tp, s->to, st, 0, n_ids, d_ids);
+    if (check(s, e, "task heights kernel"))
+        return ARC_ERR_CUDA;
+    return s->fp64 ? env_reset_done<double>(s, st) : env_reset_done<float>(s, st);
+}
+
 int arc_env_step(arc_sim* s, const float* d_actions, void* stream)
 {
     if (int rc = env_check(s))
@@ -1773,8 +1897,9 @@ int arc_env_step(arc_sim* s, const float* d_actions, void* stream)
     if (d_actions)
         return env_step_launches(s, d_actions, st);
     // graph of the whole control step over the ARC_ENV_ACTIONS buffer
-    if (s->graph_exec &&
-        (s->graph_kernel != s->kernel || s->graph_wpc != s->wpc || s->graph_queue != (int)s->use_queue)) {
+    if (s->graph_exec && (s->graph_kernel != s->kernel || s->graph_wpc != s->wpc ||
+                          s->graph_queue != (int)s->use_queue || s->graph_fused != (int)s->fused ||
+                          s->graph_tile != s->substep_tile)) {
         cudaGraphExecDestroy(s->graph_exec);
         cudaGraphDestroy(s->graph);
         s->graph_exec = nullptr;
@@ -1802,6 +1927,8 @@ int arc_env_step(arc_sim* s, const float* d_actions, void* stream)
         s->graph_kernel = s->kernel;
         s->graph_wpc = s->wpc;
         s->graph_queue = (int)s->use_queue;
+        s->graph_fused = (int)s->fused;
+        s->graph_tile = s->substep_tile;
         return ARC_OK;
     }
     return check(s, cudaGraphLaunch(s->graph_exec, st), "graph launch");

@@ -138,6 +138,8 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
     R* s_con = reinterpret_cast<R*>(reinterpret_cast<unsigned char*>(s_tacc) + align16(sizeof(R) * WPC * 12));
 
     const int tid = threadIdx.x, wl = tid / kLanes, leg = tid % kLanes;
+    // the lanes of a warp that exist: CTAs of 1, 2 or 4 worlds are 4, 8 or 16 threads
+    constexpr unsigned kMask = WPC * kLanes >= 32 ? 0xffffffffu : (1u << (WPC * kLanes)) - 1u;
     const int w0 = blockIdx.x * WPC;
     const int nw = min(WPC, W.n - w0);
     const int world = w0 + wl;
@@ -207,7 +209,7 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
             S.store_pose(b, P);
         }
     }
-    __syncwarp();
+    __syncwarp(kMask);
 
     for (int sub = 0; sub < M.substeps; ++sub) {
         // integrate (csrc/arc_phys.c:658-672)
@@ -226,7 +228,7 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
                 S.set_prev(b, xp, qp);
             }
         }
-        __syncwarp();
+        __syncwarp(kMask);
 
         // joint positions: the six-slot wavefront
         for (int slot = 0; slot < kSlots; ++slot) {
@@ -245,7 +247,7 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
                 S.store_pose(p, Pp);
                 S.store_pose(c, Pc);
             }
-            __syncwarp();
+            __syncwarp(kMask);
         }
 
         // sphere contacts (csrc/arc_phys.c:731-732)
@@ -292,7 +294,7 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
             if (cur >= 0)
                 S.store_pose(cur, P);
         }
-        __syncwarp();
+        __syncwarp(kMask);
 
         // velocities from positions (csrc/arc_phys.c:674-687)
 #pragma unroll 1
@@ -308,7 +310,7 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
                 S.set_w(b, w);
             }
         }
-        __syncwarp();
+        __syncwarp(kMask);
 
         // drive damping: the same wavefront
         for (int slot = 0; slot < kSlots; ++slot) {
@@ -324,7 +326,7 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
                 S.set_w(p, wp);
                 S.set_w(c, wc);
             }
-            __syncwarp();
+            __syncwarp(kMask);
         }
 
         // contact velocities, in the reference's order and under its cap:
@@ -332,10 +334,10 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
         int base;
         {
             int x = nc;
-            int y = __shfl_up_sync(0xffffffffu, x, 1, kLanes);
+            int y = __shfl_up_sync(kMask, x, 1, kLanes);
             if (leg >= 1)
                 x += y;
-            y = __shfl_up_sync(0xffffffffu, x, 2, kLanes);
+            y = __shfl_up_sync(kMask, x, 2, kLanes);
             if (leg >= 2)
                 x += y;
             base = x - nc;
@@ -354,7 +356,7 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
                 S.set_w(b, w);
             }
         }
-        __syncwarp();
+        __syncwarp(kMask);
     }
 
     // epilogue (csrc/arc_phys.c:739-746)
@@ -381,8 +383,8 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
         }
     }
     int badi = bad ? 1 : 0;
-    badi |= __shfl_xor_sync(0xffffffffu, badi, 1, kLanes);
-    badi |= __shfl_xor_sync(0xffffffffu, badi, 2, kLanes);
+    badi |= __shfl_xor_sync(kMask, badi, 1, kLanes);
+    badi |= __shfl_xor_sync(kMask, badi, 2, kLanes);
     if (active) {
         uint32_t* sphw = W.sph + (size_t)world * 21;
 #pragma unroll
@@ -442,6 +444,9 @@ cudaError_t launch_step_fast(const DevModel<R>& M, const Worlds<R>& W, const Act
     if (!M.leaper)
         return cudaErrorInvalidValue;
     switch (worlds_per_cta) {
+    case 1: return launch_fast_wpc<R, 1>(M, W, A, spill, spill_per_lane, lane_cap, stream);
+    case 2: return launch_fast_wpc<R, 2>(M, W, A, spill, spill_per_lane, lane_cap, stream);
+    case 4: return launch_fast_wpc<R, 4>(M, W, A, spill, spill_per_lane, lane_cap, stream);
     case 8: return launch_fast_wpc<R, 8>(M, W, A, spill, spill_per_lane, lane_cap, stream);
     case 16: return launch_fast_wpc<R, 16>(M, W, A, spill, spill_per_lane, lane_cap, stream);
     case 32: return launch_fast_wpc<R, 32>(M, W, A, spill, spill_per_lane, lane_cap, stream);

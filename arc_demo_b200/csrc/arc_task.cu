@@ -1,6 +1,7 @@
 // arc_task.cu - task layer kernels (arc/task.py on the device) and the
 // warp-cooperative world reset (csrc/arc_sim.c:88-110).
 #include "arc_task.cuh"
+#include "arc_step_warps.cuh"
 
 namespace arc {
 
@@ -105,6 +106,9 @@ __device__ __forceinline__ uint64_t stream_u64(uint64_t seed, int world, uint32_
 }
 
 __device__ __forceinline__ double unit(uint64_t x) { return (double)(x >> 11) * (1.0 / 9007199254740992.0); }
+
+// the identity of world i's streams: its index, or the key its tenant gave it
+__device__ __forceinline__ int key_of(const TaskState& S, int i) { return S.key ? (int)S.key[i] : i; }
 
 // ---------------------------------------------------------------------------
 // world read-out in FP64 (what arc_sim_observe returns, csrc/arc_sim.c:140-183)
@@ -265,9 +269,10 @@ __device__ void place_target(const TaskParams& P, const Worlds<R>& W, const Task
     double tx = 0.5 * pos.x, ty = 0.5 * pos.y;
     for (int t = 0; t < 20; ++t) {
         const unsigned k = S.draws[i]++;
-        const double ang = -kPi + 2.0 * kPi * unit(stream_u64(P.seed, i, 1u, 2u * k));
+        const double ang = -kPi + 2.0 * kPi * unit(stream_u64(P.seed, key_of(S, i), 1u, 2u * k));
         const double dist = P.checkpoint_min_dist +
-                            (P.checkpoint_max_dist - P.checkpoint_min_dist) * unit(stream_u64(P.seed, i, 1u, 2u * k + 1u));
+                            (P.checkpoint_max_dist - P.checkpoint_min_dist) *
+                                unit(stream_u64(P.seed, key_of(S, i), 1u, 2u * k + 1u));
         const double cx = pos.x + dist * cos(ang), cy = pos.y + dist * sin(ang);
         if (fabs(cx) < limit && fabs(cy) < limit) {
             tx = cx;
@@ -287,15 +292,11 @@ __device__ void place_target(const TaskParams& P, const Worlds<R>& W, const Task
 // ---------------------------------------------------------------------------
 // arc/task.py:155-220 (+ 231-259 for the observation): one thread per world
 
+// One world's step of the task layer; returns whether its episode ended.
 template <class R>
-__global__ void k_task_step(const __grid_constant__ DevModel<R> M, Worlds<R> W, const __grid_constant__ TaskParams P,
-                            TaskState S, TaskOut O, const float* __restrict__ actions, int write_obs_rows, int first,
-                            int count)
+__device__ bool task_step_world(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskState& S,
+                                const TaskOut& O, const float* __restrict__ actions, int write_obs_rows, int i)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= count)
-        return;
-    const int i = first + k;
     Obs64 o;
     read_world(M, W, i, o);
     const int steps = S.steps[i] + 1;
@@ -385,6 +386,19 @@ __global__ void k_task_step(const __grid_constant__ DevModel<R> M, Worlds<R> W, 
                 t[k] = row[k];
         }
     }
+    return done;
+}
+
+// Worlds first + k (or ids[k]) for k < count, one thread each.
+template <class R>
+__global__ void k_task_step(const __grid_constant__ DevModel<R> M, Worlds<R> W, const __grid_constant__ TaskParams P,
+                            TaskState S, TaskOut O, const float* __restrict__ actions, int write_obs_rows, int first,
+                            int count, const int* __restrict__ ids)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count)
+        return;
+    task_step_world(M, W, P, S, O, actions, write_obs_rows, ids ? ids[k] : first + k);
 }
 
 // The observations' terrain heights of worlds first .. first + count - 1,
@@ -401,15 +415,11 @@ constexpr int kHeightsAt = 9 + 3 * kNumJoints + 3;  // offset of the heights in 
 constexpr int kHeightThreads = 128;
 constexpr int kHeightBlocks = 8;
 
+// Part `part` (kHeightsPer samples) of world i's observation heights.
 template <class R>
-__global__ void __launch_bounds__(kHeightThreads, kHeightBlocks)
-    k_task_heights(const __grid_constant__ DevModel<R> M, Worlds<R> W, const __grid_constant__ TaskParams P, TaskOut O,
-                   int first, int count)
+__device__ __forceinline__ void task_heights_part(const Worlds<R>& W, const TaskParams& P, const TaskOut& O, int i,
+                                                  int part)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)count * kHeightParts)
-        return;
-    const int i = first + (int)(t / kHeightParts), part = (int)(t % kHeightParts);
     const int m0 = part * kHeightsPer, m1 = m0 + kHeightsPer < kNumOffsets ? m0 + kHeightsPer : kNumOffsets;
     const R* b0 = W.rec + (size_t)i * W.stride;  // the torso's pose, as read_world reads it
     const V3<double> x{(double)b0[0], (double)b0[1], (double)b0[2]};
@@ -421,6 +431,18 @@ __global__ void __launch_bounds__(kHeightThreads, kHeightBlocks)
         for (int m = m0; m < m1; ++m)
             t_row[m] = row[m];
     }
+}
+
+template <class R>
+__global__ void __launch_bounds__(kHeightThreads, kHeightBlocks)
+    k_task_heights(const __grid_constant__ DevModel<R> M, Worlds<R> W, const __grid_constant__ TaskParams P, TaskOut O,
+                   int first, int count, const int* __restrict__ ids)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)count * kHeightParts)
+        return;
+    const int k = (int)(t / kHeightParts);
+    task_heights_part(W, P, O, ids ? ids[k] : first + k, (int)(t % kHeightParts));
 }
 
 template <class R>
@@ -667,7 +689,39 @@ k_reset_warp(const __grid_constant__ ResetModel RM, Worlds<R> W, TerrainGeom<R>*
     }
 }
 
-// ArcTask.reset (arc/task.py:113-125) + the observation of the new episode
+// ArcTask.reset (arc/task.py:113-125) + the observation of the new episode,
+// by the 32 lanes of one warp.
+template <class R>
+__device__ void task_reset_world(ResetSmem& sm, const DevModel<R>& M, const ResetModel& RM, const Worlds<R>& W,
+                                 TerrainGeom<R>* tg, TerrainGeomD* tgd, const int* __restrict__ grid_of, double cell,
+                                 const TaskParams& P, const TaskState& S, float* obs, int i)
+{
+    const int lane = threadIdx.x & 31;
+    uint32_t seed = 0;
+    if (lane == 0) {
+        const unsigned e = S.episode[i]++;
+        seed = (uint32_t)stream_u64(P.seed, key_of(S, i), 2u, e);
+        S.difficulty[i] = S.level[i];
+    }
+    seed = __shfl_sync(0xffffffffu, seed, 0);
+    __syncwarp();
+    reset_world_warp(sm, RM, W, tg, tgd, i, seed, S.difficulty[i], grid_of ? grid_of[i] : kGridMax, cell);
+    __syncwarp();
+    if (lane == 0) {
+        for (int j = 0; j < kNumJoints; ++j)
+            S.prev_action[(size_t)i * kNumJoints + j] = 0.0f;
+        S.torso_steps[i] = 0;
+        S.steps[i] = 0;
+        S.checkpoints[i] = 0;
+        Obs64 o;
+        read_world(M, W, i, o);
+        place_target(P, W, S, i, o.x, o.rot);
+        if (obs)
+            write_obs(P, W, S, i, o, obs + (size_t)i * kObsSize);
+    }
+    __syncwarp();
+}
+
 template <class R>
 __global__ void __launch_bounds__(32)
 k_task_reset(const __grid_constant__ DevModel<R> M, const __grid_constant__ ResetModel RM, Worlds<R> W,
@@ -678,33 +732,8 @@ k_task_reset(const __grid_constant__ DevModel<R> M, const __grid_constant__ Rese
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ResetSmem& sm = *reinterpret_cast<ResetSmem*>(smem_raw);
     const int n = count_dev ? min(*count_dev, max_n) : max_n;
-    const int lane = threadIdx.x & 31;
-    for (int k = blockIdx.x; k < n; k += gridDim.x) {
-        const int i = ids[k];
-        uint32_t seed = 0;
-        if (lane == 0) {
-            const unsigned e = S.episode[i]++;
-            seed = (uint32_t)stream_u64(P.seed, i, 2u, e);
-            S.difficulty[i] = S.level[i];
-        }
-        seed = __shfl_sync(0xffffffffu, seed, 0);
-        __syncwarp();
-        reset_world_warp(sm, RM, W, tg, tgd, i, seed, S.difficulty[i], grid_of ? grid_of[i] : kGridMax, cell);
-        __syncwarp();
-        if (lane == 0) {
-            for (int j = 0; j < kNumJoints; ++j)
-                S.prev_action[(size_t)i * kNumJoints + j] = 0.0f;
-            S.torso_steps[i] = 0;
-            S.steps[i] = 0;
-            S.checkpoints[i] = 0;
-            Obs64 o;
-            read_world(M, W, i, o);
-            place_target(P, W, S, i, o.x, o.rot);
-            if (obs)
-                write_obs(P, W, S, i, o, obs + (size_t)i * kObsSize);
-        }
-        __syncwarp();
-    }
+    for (int k = blockIdx.x; k < n; k += gridDim.x)
+        task_reset_world(sm, M, RM, W, tg, tgd, grid_of, cell, P, S, obs, ids[k]);
 }
 
 template <class R>
@@ -729,6 +758,112 @@ __global__ void k_task_set_targets(Worlds<R> W, const __grid_constant__ TaskPara
     S.in_view[i] = S.prev_gaze[i] < P.fov_rad;
 }
 
+// ---------------------------------------------------------------------------
+// The whole control step of ArcVecEnv.step_wait (arc/env.py:99-117) in one
+// launch, for the quadruped in FP32: each CTA steps a group of 32 worlds with
+// the warp-per-leg step (arc_step_warps.cuh), then runs the task layer on
+// those worlds - rewards, terminations and observations (one thread per
+// world), the observations' terrain heights (all threads), and the reset of
+// the worlds whose episode ended (one warp per world) - before it takes the
+// next group. Every world sees exactly the work of the separate kernels
+// (k_step_warps, k_task_step, k_task_heights, k_task_reset), in the same
+// order, so the results are theirs bit for bit; the ended-world list is filled
+// in completion order, as the separate task kernel fills it.
+
+struct ControlSmem {
+    union {
+        wl::Smem step;
+        ResetSmem reset[wl::kWarps];  // one per warp, after the group's step
+    };
+    int ended[wl::kWorlds];  // worlds of the group whose episode ended
+    int n_ended;
+    int next;  // the next group from the work queue
+};
+
+__global__ void __launch_bounds__(wl::kThreads, 4)
+k_control_step(const __grid_constant__ DevModel<float> M, const __grid_constant__ ResetModel RM, Worlds<float> W,
+               TerrainGeom<float>* tg, TerrainGeomD* tgd, const int* __restrict__ grid_of, double cell,
+               const __grid_constant__ TaskParams P, TaskState S, TaskOut O, const float* __restrict__ actions,
+               float* __restrict__ spill, int spill_per_lane, int lane_cap, const int* __restrict__ ids, int n_items,
+               int* queue)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ControlSmem& cs = *reinterpret_cast<ControlSmem*>(smem_raw);
+    const int tid = threadIdx.x, leg = tid / wl::kWorlds, j = tid % wl::kWorlds;
+    const int n_groups = (n_items + wl::kWorlds - 1) / wl::kWorlds;
+    const Actuation A{nullptr, actions};
+    auto world_of = [&](int item) {
+        const int w = item < n_items ? (ids ? ids[item] : item) : -1;
+        return w >= 0 && w < W.n ? w : -1;
+    };
+    int first = blockIdx.x;
+    if (queue) {
+        if (tid == 0)
+            cs.next = atomicAdd(queue, 1);
+        __syncthreads();
+        first = cs.next;
+    }
+#pragma unroll 1
+    for (int group = first; group < n_groups;) {
+        wl::step_group(cs.step, M, W, A, spill, spill_per_lane, lane_cap, ids, n_items, group, tid, leg, j, 0,
+                       M.substeps, nullptr);
+        if (tid == 0)
+            cs.n_ended = 0;
+        __syncthreads();
+        // arc/task.py:155-259 but the heights; warp 0's lane j takes the world
+        // its own lane stepped as leg 0 (time and unstable written by it)
+        if (tid < wl::kWorlds) {
+            const int world = world_of(group * wl::kWorlds + j);
+            if (world >= 0 && task_step_world(M, W, P, S, O, actions, 2, world))
+                cs.ended[atomicAdd(&cs.n_ended, 1)] = world;
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int t = tid; t < wl::kWorlds * kHeightParts; t += wl::kThreads) {
+            const int world = world_of(group * wl::kWorlds + t / kHeightParts);
+            if (world >= 0)
+                task_heights_part(W, P, O, world, t % kHeightParts);
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int e = leg; e < cs.n_ended; e += wl::kWarps)
+            task_reset_world(cs.reset[leg], M, RM, W, tg, tgd, grid_of, cell, P, S, O.obs, cs.ended[e]);
+        if (!queue)
+            break;
+        __syncthreads();  // the resets' shared memory is the next group's step
+        if (tid == 0)
+            cs.next = atomicAdd(queue, 1);
+        __syncthreads();
+        group = cs.next;
+    }
+    if (queue) {
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            if (atomicAdd(queue + 1, 1) == (int)gridDim.x - 1) {
+                queue[0] = 0;
+                queue[1] = 0;
+                __threadfence();
+            }
+        }
+    }
+}
+
+template <class R>
+__global__ void k_env_admit(TaskState S, const int* __restrict__ ids, const double* __restrict__ difficulty,
+                            const unsigned* __restrict__ keys, int n)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    const int i = ids[k];
+    S.level[i] = difficulty[k];
+    S.difficulty[i] = difficulty[k];
+    S.key[i] = keys[k];
+    S.episode[i] = 0;
+    S.draws[i] = 0;
+}
+
 int reset_grid(int n)
 {
     int dev = 0, sms = 148;
@@ -743,27 +878,27 @@ int reset_grid(int n)
 template <class R>
 cudaError_t launch_task_step(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskState& S,
                              const TaskOut& O, const float* actions, int write_obs_rows, cudaStream_t stream, int first,
-                             int count)
+                             int count, const int* ids)
 {
     if (count < 0)
         count = W.n - first;
-    if (count <= 0 || first < 0 || first + count > W.n)
+    if (count <= 0 || (!ids && (first < 0 || first + count > W.n)))
         return count == 0 ? cudaSuccess : cudaErrorInvalidValue;
-    k_task_step<R><<<(count + 127) / 128, 128, 0, stream>>>(M, W, P, S, O, actions, write_obs_rows, first, count);
+    k_task_step<R><<<(count + 127) / 128, 128, 0, stream>>>(M, W, P, S, O, actions, write_obs_rows, first, count, ids);
     return cudaGetLastError();
 }
 
 template <class R>
 cudaError_t launch_task_heights(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskOut& O,
-                                cudaStream_t stream, int first, int count)
+                                cudaStream_t stream, int first, int count, const int* ids)
 {
     if (count < 0)
         count = W.n - first;
-    if (count <= 0 || first < 0 || first + count > W.n)
+    if (count <= 0 || (!ids && (first < 0 || first + count > W.n)))
         return count == 0 ? cudaSuccess : cudaErrorInvalidValue;
     const long long threads = (long long)count * kHeightParts;
     k_task_heights<R><<<(unsigned)((threads + kHeightThreads - 1) / kHeightThreads), kHeightThreads, 0, stream>>>(
-        M, W, P, O, first, count);
+        M, W, P, O, first, count, ids);
     return cudaGetLastError();
 }
 
@@ -831,12 +966,68 @@ cudaError_t launch_reset_warp(const ResetModel& RM, const Worlds<R>& W, TerrainG
     return cudaGetLastError();
 }
 
+template <class R>
+cudaError_t launch_env_admit(const DevModel<R>& M, const ResetModel& RM, const Worlds<R>& W, TerrainGeom<R>* tg,
+                             TerrainGeomD* tgd, const int* grid_of, double cell, const TaskParams& P,
+                             const TaskState& S, float* obs, const int* ids, const double* difficulty,
+                             const unsigned* keys, int n, cudaStream_t stream)
+{
+    if (n <= 0)
+        return cudaSuccess;
+    if (!S.key)
+        return cudaErrorInvalidValue;
+    k_env_admit<R><<<(n + 127) / 128, 128, 0, stream>>>(S, ids, difficulty, keys, n);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return e;
+    return launch_task_reset<R>(M, RM, W, tg, tgd, grid_of, cell, P, S, obs, ids, nullptr, n, stream);
+}
+
+cudaError_t launch_control_step(const DevModel<float>& M, const ResetModel& RM, const Worlds<float>& W,
+                                TerrainGeom<float>* tg, TerrainGeomD* tgd, const int* grid_of, double cell,
+                                const TaskParams& P, const TaskState& S, const TaskOut& O, const float* actions,
+                                float* spill, int spill_per_lane, int lane_cap, const int* ids, int n_items, int* queue,
+                                cudaStream_t stream)
+{
+    if (W.n <= 0 || n_items <= 0)
+        return cudaSuccess;
+    if (!M.leaper)
+        return cudaErrorInvalidValue;
+    const int smem = (int)sizeof(ControlSmem);
+    static std::atomic<unsigned long long> configured{0};
+    static int resident[64] = {};
+    cudaError_t e = once_per_device(configured, [&](int dev) {
+        cudaError_t r = cudaFuncSetAttribute(k_control_step, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        int sms = 0, per_sm = 0;
+        if (r == cudaSuccess)
+            r = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (r == cudaSuccess)
+            r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_control_step, wl::kThreads, smem);
+        if (r == cudaSuccess)
+            resident[dev] = sms * (per_sm > 0 ? per_sm : 1);
+        return r;
+    });
+    if (e != cudaSuccess)
+        return e;
+    const int groups = (n_items + wl::kWorlds - 1) / wl::kWorlds;
+    int grid = groups;
+    if (queue) {
+        int dev = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess)
+            return e;
+        grid = groups < resident[dev] ? groups : resident[dev];
+    }
+    k_control_step<<<grid, wl::kThreads, smem, stream>>>(M, RM, W, tg, tgd, grid_of, cell, P, S, O, actions, spill,
+                                                         spill_per_lane, lane_cap, ids, n_items, queue);
+    return cudaGetLastError();
+}
+
 #define ARC_INSTANTIATE_TASK(R)                                                                                    \
     template cudaError_t launch_task_step<R>(const DevModel<R>&, const Worlds<R>&, const TaskParams&,            \
                                              const TaskState&, const TaskOut&, const float*, int, cudaStream_t,  \
-                                             int, int);                                                          \
+                                             int, int, const int*);                                              \
     template cudaError_t launch_task_heights<R>(const DevModel<R>&, const Worlds<R>&, const TaskParams&,         \
-                                                const TaskOut&, cudaStream_t, int, int);                         \
+                                                const TaskOut&, cudaStream_t, int, int, const int*);             \
     template cudaError_t launch_task_observe<R>(const DevModel<R>&, const Worlds<R>&, const TaskParams&,         \
                                                 const TaskState&, float*, const int*, int, cudaStream_t);        \
     template cudaError_t launch_task_reset<R>(const DevModel<R>&, const ResetModel&, const Worlds<R>&,           \
@@ -845,6 +1036,10 @@ cudaError_t launch_reset_warp(const ResetModel& RM, const Worlds<R>& W, TerrainG
                                               const int*, int, cudaStream_t);                                    \
     template cudaError_t launch_task_set_targets<R>(const Worlds<R>&, const TaskParams&, const TaskState&,       \
                                                     const int*, const double*, int, cudaStream_t);               \
+    template cudaError_t launch_env_admit<R>(const DevModel<R>&, const ResetModel&, const Worlds<R>&,            \
+                                             TerrainGeom<R>*, TerrainGeomD*, const int*, double, const TaskParams&, \
+                                             const TaskState&, float*, const int*, const double*, const unsigned*, \
+                                             int, cudaStream_t);                                                  \
     template cudaError_t launch_reset_warp<R>(const ResetModel&, const Worlds<R>&, TerrainGeom<R>*,              \
                                               TerrainGeomD*, const int*, int, const unsigned*, const double*,    \
                                               const int*, double, cudaStream_t);

@@ -47,6 +47,7 @@ struct TaskState {
     unsigned char* in_view;  // [N]
     unsigned* episode;    // [N] resets so far (device RNG counter)
     unsigned* draws;      // [N] checkpoint draws so far (device RNG counter)
+    unsigned* key;        // [N] identity of each world's RNG streams (NULL: the world index)
 };
 
 // Outputs of one env step, device arrays.
@@ -64,16 +65,17 @@ struct TaskOut {
 };
 
 template <class R>
-// Worlds first .. first + count - 1 (count < 0: to the last world).
+// Worlds first .. first + count - 1 (count < 0: to the last world), or with
+// ids the count worlds ids[0 .. count) (device array).
 // write_obs: 0 no observation rows, 1 whole rows, 2 rows without the terrain
 // heights, which launch_task_heights then writes with more threads.
 cudaError_t launch_task_step(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskState& S,
                              const TaskOut& O, const float* actions, int write_obs, cudaStream_t stream, int first = 0,
-                             int count = -1);
+                             int count = -1, const int* ids = nullptr);
 
 template <class R>
 cudaError_t launch_task_heights(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskOut& O,
-                                cudaStream_t stream, int first = 0, int count = -1);
+                                cudaStream_t stream, int first = 0, int count = -1, const int* ids = nullptr);
 
 template <class R>
 cudaError_t launch_task_observe(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskState& S,
@@ -87,6 +89,30 @@ cudaError_t launch_task_reset(const DevModel<R>& M, const ResetModel& RM, const 
                               TerrainGeomD* tgd, const int* grid_of, double cell, const TaskParams& P,
                               const TaskState& S, float* obs, const int* ids, const int* count_dev, int max_n,
                               cudaStream_t stream);
+
+// The whole control step (step, rewards, terminations, observations, resets
+// of ended worlds) in one launch, for the quadruped in FP32: the warp-per-leg
+// step of each group of 32 worlds followed by the task layer on them. The
+// worlds are ids[0 .. n_items) (ids nullptr: 0 .. n_items - 1); with a queue
+// (two device ints, zero between launches) one wave of resident CTAs takes
+// the groups. O.done_count must be zero before the launch. The results equal
+// launch_step_warps, launch_task_step (write_obs 2), launch_task_heights and
+// launch_task_reset over O.done_list in turn, bit for bit.
+cudaError_t launch_control_step(const DevModel<float>& M, const ResetModel& RM, const Worlds<float>& W,
+                                TerrainGeom<float>* tg, TerrainGeomD* tgd, const int* grid_of, double cell,
+                                const TaskParams& P, const TaskState& S, const TaskOut& O, const float* actions,
+                                float* spill, int spill_per_lane, int lane_cap, const int* ids, int n_items, int* queue,
+                                cudaStream_t stream);
+
+// Starts worlds ids[0 .. n) (device arrays) afresh as new tenants of their
+// slots: level and difficulty, RNG key and RNG counters set, then a task
+// reset (terrain, pose, task state, checkpoint, observation), so that what a
+// world draws depends on its key, not on its slot. S.key must be allocated.
+template <class R>
+cudaError_t launch_env_admit(const DevModel<R>& M, const ResetModel& RM, const Worlds<R>& W, TerrainGeom<R>* tg,
+                             TerrainGeomD* tgd, const int* grid_of, double cell, const TaskParams& P,
+                             const TaskState& S, float* obs, const int* ids, const double* difficulty,
+                             const unsigned* keys, int n, cudaStream_t stream);
 
 // Checkpoints at given points (host-injected; parity tests and callers that
 // draw their own): target, target_z, prev_dist, prev_gaze, in_view.

@@ -103,6 +103,7 @@ def sim_lib() -> ctypes.CDLL:
     d("arc_sim_create_sized", _vp, _int, _i32, _dbl, _int, _dbl, _uint)
     d("arc_sim_step_ids", _int, _vp, _vp, _int, _vp, _vp, _vp)
     d("arc_sim_set_work_queue", _int, _vp, _int)
+    d("arc_sim_set_substep_tile", _int, _vp, _int)
     d("arc_device_checks", _int, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(_int),
       ctypes.POINTER(ctypes.c_longlong), _int)
     return lib
@@ -348,3 +349,8 @@ class Sim:
 
     def set_work_queue(self, on: bool) -> None:
         self._check(self._lib.arc_sim_set_work_queue(self._ptr, int(bool(on))))
+
+    def set_substep_tile(self, tile: int) -> None:
+        """Warp-per-leg kernel: `tile` substeps per launch (0: the whole
+        control step in one launch)."""
+        self._check(self._lib.arc_sim_set_substep_tile(self._ptr, int(tile)))

@@ -64,6 +64,12 @@ class DeviceVecEnv:
     def set_kernel(self, kernel: int, worlds_per_cta: int = 16) -> None:
         self.sim.set_kernel(kernel, worlds_per_cta)
 
+    def set_fused(self, on: bool) -> None:
+        """With the warp-per-leg kernel, each control step is one fused launch
+        (the default) or the step kernel followed by the task, heights and
+        reset kernels; the results are the same bit for bit."""
+        self.sim._check(self.gpu.lib.arc_env_set_fused(self.sim.ptr, int(bool(on))))
+
     def set_levels(self, levels) -> None:
         """Per-world terrain difficulty levels (the curriculum state)."""
         import numpy as np

@@ -176,27 +176,41 @@ def policy_forward(torch, params, obs, out):
     torch.mm(h[1], w3, out=out).add_(b3)
 
 
-def autotune(env, torch, stream, candidates=("warps", "warps+queue", 8, 16), steps=4):
-    """Step kernel and worlds-per-CTA, by timing the step kernel: the
-    warp-per-leg kernel (32 worlds per CTA; one CTA per group, or one wave of
-    resident CTAs taking groups from a work queue) and the leg-parallel kernel
-    at several worlds per CTA. Every candidate starts from the same world
-    states: the step's cost grows over the first steps after a reset, as the
-    robots settle and their contacts multiply, so timing the candidates one
-    after another from a running state would favour the first."""
+def apply_candidate(env, cand):
+    """Puts the env's step kernel in the form a candidate names: "warps" (one
+    CTA per group of 32 worlds), "warps+queue" (one wave of resident CTAs
+    taking groups from a work queue), "tileK" (warps+queue, K substeps per
+    launch) or an int (the leg-parallel kernel at that many worlds per CTA)."""
     from arc_demo_b200.native import KERNEL_LEGS, KERNEL_WARPS
+    c = str(cand)
+    env.sim.set_substep_tile(int(c[4:]) if c.startswith("tile") else 0)
+    env.sim.set_work_queue(c == "warps+queue" or c.startswith("tile"))
+    if c.startswith("warps") or c.startswith("tile"):
+        env.set_kernel(KERNEL_WARPS)
+    else:
+        env.set_kernel(KERNEL_LEGS, int(c))
+
+
+def autotune(env, torch, stream,
+             candidates=("warps", "warps+queue", "tile10", "tile5", "tile2", 1, 2, 4, 8, 16), steps=4):
+    """Step kernel, worlds per CTA and substep tiling, by timing the step
+    kernel: the warp-per-leg kernel (32 worlds per CTA; one CTA per group, or
+    one wave of resident CTAs taking groups from a work queue; the whole
+    control step in one launch, or in launches of 10, 5 or 2 substeps with
+    the state through device memory in between) and the leg-parallel kernel
+    at 1, 2, 4, 8 and 16 worlds per CTA. Every candidate starts from the same
+    world states: the step's cost grows over the first steps after a reset,
+    as the robots settle and their contacts multiply, so timing the
+    candidates one after another from a running state would favour the
+    first."""
     lib, ptr = env.sim._lib, env.sim.ptr
     best, table = None, {}
     stream.synchronize()
     start = env.sim.get_state()
-    for wpc in candidates:
+    for cand in candidates:
         env.sim.set_state(start)
         torch.cuda.synchronize()
-        env.sim.set_work_queue(wpc == "warps+queue")
-        if wpc in ("warps", "warps+queue"):
-            env.set_kernel(KERNEL_WARPS)
-        else:
-            env.set_kernel(KERNEL_LEGS, wpc)
+        apply_candidate(env, cand)
         a = ctypes.c_void_p(env.actions.data_ptr())
         st = ctypes.c_void_p(stream.cuda_stream)
         for _ in range(2):
@@ -208,28 +222,31 @@ def autotune(env, torch, stream, candidates=("warps", "warps+queue", 8, 16), ste
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / steps
-        table[str(wpc)] = round(ms, 4)
+        table[str(cand)] = round(ms, 4)
         if best is None or ms < table[str(best)]:
-            best = wpc
+            best = cand
     env.sim.set_state(start)
     torch.cuda.synchronize()
-    env.sim.set_work_queue(best == "warps+queue")
-    if best in ("warps", "warps+queue"):
-        env.set_kernel(KERNEL_WARPS)
-    else:
-        env.set_kernel(KERNEL_LEGS, best)
+    apply_candidate(env, best)
     return best, table
 
 
-def autotune_parts(env, torch, stream, one_step, candidates=(1, 2, 4), steps=6):
-    """How many world ranges the control step runs in (DeviceVecEnv.step_parts;
-    1: the policy, then the whole step as one CUDA graph), by timing whole
-    control steps, each candidate from the same world states."""
+def autotune_parts(env, torch, stream, one_step, candidates=("1", "1 separate", "2", "4"), steps=6):
+    """How the control step runs (by timing whole control steps, each
+    candidate from the same world and task states): "1", the policy then the
+    whole step as one CUDA graph whose step is one fused launch (each group's
+    physics, rewards, observations and resets in one kernel); "1 separate",
+    the same graph with the step kernel followed by the task, heights and
+    reset kernels; "2", "4", the worlds in that many ranges on their own
+    streams (DeviceVecEnv.step_parts), each range's policy then its step."""
     table = {}
     stream.synchronize()
-    start = env.sim.get_state()
-    for parts in candidates:
+    start, tstart = env.sim.get_state(), env.gpu.get_state()
+    for cand in candidates:
+        parts = int(cand.split()[0])
+        env.set_fused(cand != "1 separate")
         env.sim.set_state(start)
+        env.gpu.set_state(tstart)
         torch.cuda.synchronize()
         for _ in range(2):
             one_step(parts)
@@ -239,11 +256,13 @@ def autotune_parts(env, torch, stream, one_step, candidates=(1, 2, 4), steps=6):
             one_step(parts)
         e1.record(stream)
         e1.synchronize()
-        table[str(parts)] = round(e0.elapsed_time(e1) / steps, 4)
+        table[cand] = round(e0.elapsed_time(e1) / steps, 4)
     env.sim.set_state(start)
+    env.gpu.set_state(tstart)
     torch.cuda.synchronize()
-    best = min(candidates, key=lambda p: table[str(p)])
-    return best, table
+    best = min(candidates, key=lambda c: table[c])
+    env.set_fused(best != "1 separate")
+    return int(best.split()[0]), best, table
 
 
 def max_over_ranks(torch, dist, x: float) -> float:
@@ -293,8 +312,8 @@ def run_ours(args) -> dict | None:
             env.set_kernel(KERNEL_LEGS, args.wpc)
             best_wpc, tune = args.wpc, None
         elif args.kernel == "warps":
-            env.set_kernel(KERNEL_WARPS)
-            best_wpc, tune = "warps", None
+            apply_candidate(env, "warps+queue")
+            best_wpc, tune = "warps+queue", None
         else:
             best_wpc, tune = autotune(env, torch, stream)
         part_params = [{"layers": params["layers"], "hidden": {}} for _ in range(16)]  # one set per stream
@@ -310,9 +329,9 @@ def run_ours(args) -> dict | None:
                 env.step_parts(part_policy, parts)
 
         if args.parts:
-            parts, parts_tune = args.parts, None
+            parts, form, parts_tune = args.parts, str(args.parts), None
         else:
-            parts, parts_tune = autotune_parts(env, torch, stream, one_step)
+            parts, form, parts_tune = autotune_parts(env, torch, stream, one_step)
         env.reset()
 
         for _ in range(max(args.warmup, 3)):
@@ -377,11 +396,20 @@ def run_ours(args) -> dict | None:
             q1.synchronize()
             plain_kernel_ms = q0.elapsed_time(q1) / 3
             plain = {"ms_per_step": round(plain_ms, 3), "env_steps_per_s": round(n / plain_ms * 1e3),
-                     "step_kernel_ms": round(plain_kernel_ms, 3)}
-            if best_wpc in ("warps", "warps+queue"):
-                env.set_kernel(KERNEL_WARPS)
-            else:
-                env.set_kernel(KERNEL_LEGS, best_wpc)
+                     "step_kernel_ms": round(plain_kernel_ms, 3),
+                     "loop": "the same policy and env.step() graph with the plain per-world kernel (one thread "
+                             "per world) and the separate task, heights and reset kernels"}
+            apply_candidate(env, best_wpc)
+
+        # the whole env step alone (no policy): the fused control-step launch
+        # (or the separate kernels) over every world, as the graph replays it
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        for _ in range(M):
+            env.step()
+        c1.record(stream)
+        c1.synchronize()
+        control_step_ms = c0.elapsed_time(c1) / M
 
         e2e = None
         if not args.no_e2e:
@@ -402,6 +430,16 @@ def run_ours(args) -> dict | None:
 
     value = whole_job_rate(world, n, K, ms_total)
     achieved = n * FLOP_PER_ENV_STEP / (step_kernel_ms * 1e-3)
+    cand = str(best_wpc)
+    kernel_name = ("warp-per-leg" + (", work queue" if cand != "warps" else "") +
+                   (f", {cand[4:]} substeps per launch" if cand.startswith("tile") else "")
+                   if cand.startswith(("warps", "tile")) else "leg-parallel")
+    fused = form != "1 separate" and cand.startswith("warps")
+    # our launches per control step: the fused control step (one per range)
+    # or the step, task, heights and reset kernels (per range), the ranges'
+    # merge, the memset of the ended-world count not counted (not a kernel)
+    per_part = 1 if fused else 4
+    launches = (per_part * parts + (1 if parts > 1 else 0)) * K
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "env-steps/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": round(ms_total / K, 4), "higher_is_better": True,
@@ -409,12 +447,14 @@ def run_ours(args) -> dict | None:
         "config": {"workload": f"{n} worlds of the quadruped per GPU, difficulty uniform in {{0,...,1.0}}, "
                                "checkpoints, auto-reset, random-init MLP policy 195-256-256-12 tanh FP32 in the loop",
                    "worlds_per_gpu": n, "substeps": 20, "dt": 1 / 30,
-                   "kernel": {"warps": "warp-per-leg", "warps+queue": "warp-per-leg, work queue"}.get(
-                       str(best_wpc), "leg-parallel"),
-                   "worlds_per_cta": 32 if str(best_wpc).startswith("warps") else best_wpc,
+                   "kernel": kernel_name,
+                   "worlds_per_cta": 32 if cand.startswith(("warps", "tile")) else best_wpc,
+                   "substeps_per_launch": int(cand[4:]) if cand.startswith("tile") else 20,
                    "autotune_step_kernel_ms": tune,
                    "parts": parts,
-                   "autotune_parts_ms_per_step": parts_tune,
+                   "control_step": ("one fused launch per world range (step, rewards, observations, resets)"
+                                    if fused else "step kernel, then task, heights and reset kernels"),
+                   "autotune_control_step_ms": parts_tune,
                    "loop": ("policy then env.step() (one CUDA graph) per control step" if parts == 1 else
                             f"policy and step of {parts} world ranges, each on its own stream "
                             "(DeviceVecEnv.step_parts), joined every control step"),
@@ -423,19 +463,19 @@ def run_ours(args) -> dict | None:
                        "p99": round(float(np.percentile(lat, 99)), 4), "max": round(float(lat.max()), 4)},
         "plain_kernel": plain,
         "speedup_vs_plain": round(plain["ms_per_step"] / (ms_total / K), 2) if plain else None,
+        "speedup_vs_plain_step_kernel": round(plain["step_kernel_ms"] / step_kernel_ms, 2) if plain else None,
+        "control_step_ms_without_policy": round(control_step_ms, 4),
         "roofline": {"bound": "fp32", "achieved": round(achieved / 1e12, 3),
                      "peak": round(peak.value / 1e12, 3), "unit": "TFLOP/s",
                      "frac": round(achieved / peak.value, 4) if peak.value else None,
-                     "traffic": round(n * WARPS_DRAM_BYTES_PER_WORLD) if str(best_wpc).startswith("warps") else None,
+                     "traffic": round(n * WARPS_DRAM_BYTES_PER_WORLD) if cand.startswith("warps") else None,
                      "traffic_unit": "bytes per launch (ncu, scaled from 16,384 worlds)",
-                     "kernel": ("warp-per-leg" if str(best_wpc).startswith("warps") else "leg-parallel") + " step",
+                     "kernel": kernel_name + " step",
                      "kernel_ms": round(step_kernel_ms, 4),
                      "flop_per_env_step": FLOP_PER_ENV_STEP,
                      "peak_source": "measured FP32 FMA probe (arc_probe_fp32_peak) on this GPU",
                      "hbm_gbs_algorithmic": round(n * HBM_BYTES_PER_ENV_STEP / (step_kernel_ms * 1e-3) / 1e9, 1)},
-        # step, task, terrain heights, reset of ended worlds (per part), and the
-        # merge of the parts' ended-world lists
-        "gpu_launches": (4 * parts + (1 if parts > 1 else 0)) * K,
+        "gpu_launches": launches,
         "ended_in_last_step": ended,
         "clocks": clock,
     }
@@ -667,17 +707,24 @@ def leg_fp64(torch, n, steps=6, warmup=3) -> dict:
             "note": "actions fixed (uniform random); control step = step, task, heights, reset in one graph"}
 
 
-def leg_serving(seconds=3.0, clients=8, rate=200.0) -> dict:
-    """The serving engine with 8 Poisson clients at 200 requests/s each
-    (1..8,192 worlds log-uniform x 1..32 control steps, mixed difficulty),
-    the pool sized by a 40 GB budget."""
+def leg_serving(seconds=3.0, clients=8, rates=(200.0, 50.0), tick_cap=131072) -> dict:
+    """The serving engine with 8 Poisson clients (each request steps one of
+    the client's resident sessions of 1..8,192 worlds, log-uniform, for
+    1..32 control steps with the task layer; worlds reset in place when their
+    episode ends), the pool sized by a 40 GB budget, at 200 requests/s per
+    client (more than one GPU steps: the latency includes queueing) and at
+    50 (below saturation)."""
     from arc_demo_b200.serve import WORLD_BYTES, Server, run_load
     capacity = int(40e9 // WORLD_BYTES)
-    with Server(capacity, result="observe") as sv:
-        rid = sv.submit(np.arange(64, dtype=np.uint32), np.zeros(64), 2)
-        sv.wait(rid)
-        out = run_load(sv, clients, rate, seconds)
-    out.update({"clients": clients, "rate_per_client": rate, "capacity": capacity, "offered_seconds": seconds})
+    out = {"clients": clients, "capacity": capacity, "tick_cap": tick_cap, "offered_seconds": seconds,
+           "bytes_per_world": WORLD_BYTES}
+    with Server(capacity, tick_cap=tick_cap) as sv:
+        sid = sv.open(np.zeros(64))
+        sv.wait(sv.request(sid, 2))
+        sv.close_session(sid)
+        for rate in rates:
+            r = run_load(sv, clients, rate, seconds, seed=int(rate))
+            out[f"rate_{int(rate)}"] = {k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()}
     return out
 
 

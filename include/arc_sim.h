@@ -117,8 +117,9 @@ arc_sim *arc_sim_create_sized(int n_worlds, const int *grids, double dt, int sub
 int arc_sim_last_error(const arc_sim *s);
 const char *arc_sim_error_message(const arc_sim *s);
 
-/* Kernel choice; worlds_per_cta in {8, 16, 32, 64} for ARC_KERNEL_LEGS
- * (ARC_KERNEL_WARPS always steps 32 worlds per CTA). */
+/* Kernel choice; worlds_per_cta in {1, 2, 4, 8, 16, 32, 64} for
+ * ARC_KERNEL_LEGS, four threads per world (ARC_KERNEL_WARPS always steps 32
+ * worlds per CTA). */
 int arc_sim_set_kernel(arc_sim *s, int kernel, int worlds_per_cta);
 int arc_sim_get_kernel(const arc_sim *s, int *kernel, int *worlds_per_cta);
 /* 4 for FP32, 8 for FP64 */
@@ -195,6 +196,12 @@ int arc_sim_observe_ids(const arc_sim *s, const int *d_ids, int n_ids, double *r
 /* on != 0: the warp-per-leg kernel runs one wave of resident CTAs that take
  * groups of 32 worlds from a device work queue, instead of one CTA per group */
 int arc_sim_set_work_queue(arc_sim *s, int on);
+/* Substep tiling of the warp-per-leg kernel: tile in 1 .. substeps - 1 runs
+ * each control step as launches of `tile` substeps, the state going through
+ * device memory between them (the same worlds bit for bit); 0 (the default)
+ * or >= substeps: the whole control step in one launch, the state on chip
+ * throughout. */
+int arc_sim_set_substep_tile(arc_sim *s, int tile);
 
 /* The checked build (libarcsim_checked.so, compiled with ARC_DEVICE_CHECKS)
  * tests the kernels' data-dependent indexes - terrain columns against their
@@ -211,43 +218,6 @@ int arc_device_checks(unsigned long long *failures, int *first_site, long long *
 /* Measured FP32 FMA throughput of the current device (FLOP/s, an FMA
  * counted as 2): the roofline denominator of the step kernels. */
 int arc_probe_fp32_peak(double *flops_per_s, double *seconds);
-
-/* ---- serving engine. No counterpart in the reference. A fixed pool of
- * `capacity` world slots (the state budget) and one engine thread doing
- * continuous batching: queued requests are admitted first come, first
- * served, while free slots hold them, and their worlds reset; each tick
- * steps every admitted world of every request in one launch; a request
- * whose steps are done has its final states read back and its slots freed.
- * Thread-safe: any number of client threads may submit and wait. */
-typedef struct arc_server arc_server;
-/* results: the final state of each world (arc_sim_state_size doubles, the
- * arc_sim_get_state layout) or its final observation (65 doubles: root 13,
- * rot 9, joints 36, contacts 6, flag 1, as arc_sim_observe) */
-#define ARC_SERVE_STATE 0
-#define ARC_SERVE_OBSERVE 1
-arc_server *arc_server_create(int capacity, double dt, int substeps, int grid, double cell, int result);
-/* Stops the engine; requests still queued fail. */
-void arc_server_destroy(arc_server *sv);
-/* A request: n_worlds fresh episodes (seeds, difficulty as arc_sim_reset)
- * stepped n_steps control steps with actions (n_steps x n_worlds x 12 FP32,
- * as arc_sim_step_actions; copied) or, with actions NULL, an
- * Ornstein-Uhlenbeck process per world (theta 0.15, sigma 0.3, clipped to
- * [-1, 1]) seeded by ou_seed. out: n_worlds results (kept alive by the
- * caller until the wait returns), or NULL to receive them through
- * arc_server_wait. Returns the request id (>= 0) or < 0. */
-long long arc_server_submit(arc_server *sv, int n_worlds, int n_steps, const unsigned *seeds,
-                            const double *difficulty, const float *actions, unsigned long long ou_seed,
-                            double *out);
-/* Waits up to timeout_s for request id: 1 when done (out, for a request
- * submitted without one: the n_worlds results; times:
- * seconds queued, running, total; either may be NULL), 0 on timeout, < 0 on
- * error. An id is returned once. */
-int arc_server_wait(arc_server *sv, long long id, double timeout_s, double *out, double *times);
-/* stats (9 doubles): ticks, world-steps, engine busy seconds, most worlds
- * in one tick, completed requests, queued requests, then the busy seconds
- * split into admission (resets), stepping (actions and the step launch) and
- * eviction (reading back final states). Returns the engine's error (0 ok). */
-int arc_server_stats(arc_server *sv, double *stats);
 
 /* ---- one control step without any device allocation. No counterpart in
  * the reference: for callers that cannot call cudaMalloc (a host runtime
@@ -309,8 +279,32 @@ int arc_env_reset(arc_sim *s, const int *ids, int n_ids, void *stream);
  * rewards, terminations, checkpoints, curriculum, observations, and the
  * reset of every world that ended (their pre-reset observation goes to
  * ARC_ENV_TERMINAL_OBS). d_actions == NULL: the ARC_ENV_ACTIONS buffer,
- * through a CUDA graph of the whole step captured on first use. */
+ * through a CUDA graph of the whole step captured on first use. With the
+ * warp-per-leg kernel (FP32) the whole step is one kernel launch: each group
+ * of 32 worlds is stepped and then gets its rewards, observations and
+ * resets in the same kernel (see arc_env_set_fused). */
 int arc_env_step(arc_sim *s, const float *d_actions, void *stream);
+
+/* Starts the listed worlds (host ids) afresh for a new tenant: difficulty
+ * (level) per world, and a key per world that names its random streams
+ * (reset seeds, checkpoints) in place of its index, with those streams
+ * restarted; then ArcTask.reset and the observation. What such a world
+ * draws depends on its key and not on which world slot it occupies, so a
+ * tenant's worlds behave alike in any slots. Synchronous. */
+int arc_env_admit(arc_sim *s, const int *ids, int n_ids, const double *difficulty, const unsigned *keys,
+                  void *stream);
+
+/* One control step of ArcVecEnv.step_wait for the listed worlds only
+ * (device ids, distinct): their actions from the ARC_ENV_ACTIONS rows of
+ * those worlds, their outputs in the env buffers' rows of those worlds, the
+ * ended ones (ARC_ENV_DONE_LIST / DONE_COUNT) reset. Asynchronous on stream. */
+int arc_env_step_ids(arc_sim *s, const int *d_ids, int n_ids, void *stream);
+
+/* on != 0 (the default): with the warp-per-leg kernel, the env's control
+ * step (arc_env_step, arc_env_step_part, arc_env_step_host) is one fused
+ * launch; 0: the step kernel, then the task, heights and reset kernels. Both
+ * give the same results bit for bit. */
+int arc_env_set_fused(arc_sim *s, int on);
 
 /*
  * The same control step with host buffers, as ArcVecEnv.step_wait's caller
@@ -392,6 +386,59 @@ int arc_env_get_task_state(const arc_sim *s, const int *ids, int n_ids, double *
 int arc_env_set_task_state(arc_sim *s, const int *ids, int n_ids, const double *in);
 /* Places checkpoints at given points (target_z, prev_dist, prev_gaze follow). */
 int arc_env_set_targets(arc_sim *s, const int *ids, int n_ids, const double *xy);
+
+/* ---- serving engine. No counterpart in the reference, which steps one
+ * synchronous batch per call. A fixed pool of `capacity` world slots (the
+ * device-memory budget) with the task layer, and one engine thread doing
+ * continuous batching for any number of client threads:
+ *   - a session is one client's batch of worlds. It waits for free slots,
+ *     then is admitted: each world starts an episode at the session's
+ *     difficulty (its random streams named by the session's key, so the
+ *     same session gives the same worlds whichever slots it gets). Its worlds
+ *     stay resident, episode after episode, until the session is closed.
+ *   - a request steps one session's worlds n_steps control steps with the
+ *     task layer; a world whose episode ends is evicted from its slot and the
+ *     slot reset with its next episode at once (ArcVecEnv's auto-reset,
+ *     arc/env.py:99-117), and the request goes on.
+ *   - each tick steps the worlds of every running request in one launch. A
+ *     queued request starts running, first come first served, when its
+ *     session is resident and idle and the tick holds at most tick_cap
+ *     worlds with it (a request larger than tick_cap runs alone).
+ * A session's results in the mix equal its results alone, bit for bit. */
+typedef struct arc_server arc_server;
+/* dt, substeps, grid, cell as arc_sim_create; cfg the task (NULL: the
+ * defaults with the curriculum off, so worlds keep their session's
+ * difficulty); tick_cap 0: capacity. NULL on failure. */
+arc_server *arc_server_create(int capacity, double dt, int substeps, int grid, double cell,
+                              const arc_task_config *cfg, int tick_cap);
+/* Stops the engine; queued requests fail. */
+void arc_server_destroy(arc_server *sv);
+/* A session of n_worlds worlds at difficulty[i] (copied), random streams
+ * named by key. Returns its id (> 0) or < 0. */
+long long arc_server_open(arc_server *sv, int n_worlds, const double *difficulty, unsigned long long key);
+/* A request on a session: n_steps control steps with actions (n_steps x
+ * n_worlds x 12 float32 in [-1, 1], copied) or, with actions NULL, an
+ * Ornstein-Uhlenbeck process per world (theta 0.15, sigma 0.3, clipped to
+ * [-1, 1]) seeded by ou_seed. Results into the caller's buffers, kept alive
+ * until the wait returns (any may be NULL): obs n_worlds x 195 float32 after
+ * the last step, reward n_steps x n_worlds float32, done n_steps x n_worlds
+ * (bit 0 terminated, bit 1 truncated; the world was reset after that step).
+ * A session's requests run one after another in submission order. Returns
+ * the request id (> 0) or < 0. */
+long long arc_server_request(arc_server *sv, long long session, int n_steps, const float *actions,
+                             unsigned long long ou_seed, float *obs, float *reward, unsigned char *done);
+/* Waits up to timeout_s for a request: 1 done (times: seconds queued,
+ * running, total; may be NULL), 0 on timeout, < 0 on error. An id is
+ * returned once. */
+int arc_server_wait(arc_server *sv, long long request, double timeout_s, double *times);
+/* Closes a session: its slots are freed once its submitted requests are
+ * done; later requests on it fail. */
+int arc_server_close(arc_server *sv, long long session);
+/* stats (12 doubles): ticks, world-steps, engine busy seconds, most worlds
+ * in one tick, completed requests, queued requests, busy seconds in
+ * admission, stepping and reading results back, episodes ended, resident
+ * worlds, sessions waiting for slots. Returns the engine's error (0 ok). */
+int arc_server_stats(arc_server *sv, double *stats);
 
 #ifdef __cplusplus
 }

@@ -1,11 +1,17 @@
-"""The serving engine (csrc/arc_serve.cu): continuous batching over a pool of
-world slots must not change any request's results.
+"""The serving engine (csrc/arc_serve.cu): sessions of resident worlds with the
+task layer, stepped by continuous batching.
 
-- A request's final states in a mix of concurrent requests equal its final
-  states when it runs alone, bit for bit (worlds never interact; the step
-  runs the same per-world code for any list of slots).
-- A request with explicit actions equals the same worlds reset and stepped
-  directly through arc_sim_step_ids with those actions.
+- A session's results (per-step rewards and done flags, final observations)
+  in a mix of concurrent sessions and requests equal its results when it
+  runs alone, bit for bit: worlds never interact, the fused control step
+  runs the same per-world code for any list of slots, and a world's random
+  draws are named by its session's key, not by its slot.
+- Worlds stay resident across requests: a session stepped 3 + 4 steps in two
+  requests equals the same session stepped 7 steps in one.
+- A world whose episode ends is reset in place and the request goes on
+  (arc/env.py:99-117): with max_steps 5, every world that does not fall is
+  truncated after steps 5 and 10 of a 12-step request.
+- Admission by the slot budget, the per-tick world cap, and the errors.
 """
 
 import threading
@@ -13,122 +19,112 @@ import threading
 import numpy as np
 import pytest
 
-from arc_demo_b200.native import KERNEL_WARPS, Sim
 from arc_demo_b200.serve import Server
+from arc_demo_b200.task import TaskConfig
 
 pytestmark = pytest.mark.gpu
 
+CFG = TaskConfig(curriculum=False, max_steps=5)
 
-def make_requests(seed):
+
+def session_plan(seed):
+    """Sessions (difficulties, key) and, per session, its requests (steps,
+    given actions or None, OU seed)."""
     rng = np.random.default_rng(seed)
-    reqs = []
-    for n, k in ((5, 3), (40, 6), (100, 2), (1, 7), (33, 5), (64, 4), (17, 1)):
-        seeds = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
-        reqs.append((seeds, rng.uniform(0, 1, n), k, int(rng.integers(2**63))))
-    return reqs
+    plan = []
+    for n, ks in ((5, (3, 4)), (40, (6,)), (100, (2, 9)), (1, (7,)), (33, (5, 1)), (64, (4,))):
+        reqs = []
+        for k in ks:
+            given = rng.random() < 0.5
+            act = rng.uniform(-1.2, 1.2, (k, n, 12)).astype(np.float32) if given else None
+            reqs.append((k, act, int(rng.integers(2**63))))
+        plan.append((rng.uniform(0, 1, n), int(rng.integers(2**63)), reqs))
+    return plan
+
+
+def run_session(sv, diff, key, reqs):
+    sid = sv.open(diff, key)
+    outs = []
+    for k, act, ou in reqs:
+        (obs, rew, done), times = sv.wait(sv.request(sid, k, actions=act, ou_seed=ou))
+        assert times[2] >= times[1] >= 0
+        outs.append((obs, rew, done))
+    sv.close_session(sid)
+    return outs
 
 
 def test_mix_equals_alone():
-    reqs = make_requests(1)
-    with Server(256) as sv:
-        ids = [None] * len(reqs)
+    plan = session_plan(1)
+    with Server(512, config=CFG) as sv:
+        mixed = [None] * len(plan)
 
-        def submit(i):
-            s, d, k, ou = reqs[i]
-            ids[i] = sv.submit(s, d, k, ou_seed=ou)
+        def client(i):
+            mixed[i] = run_session(sv, *plan[i])
 
-        threads = [threading.Thread(target=submit, args=(i,)) for i in range(len(reqs))]
+        threads = [threading.Thread(target=client, args=(i,)) for i in range(len(plan))]
         for t in threads:
             t.start()
         for t in threads:
             t.join()
-        mixed = [sv.wait(ids[i])[0] for i in range(len(reqs))]
         st = sv.stats()
-        assert st["error"] == 0 and st["completed"] == len(reqs)
-    with Server(256) as sv:
-        for i, (s, d, k, ou) in enumerate(reqs):
-            alone, times = sv.wait(sv.submit(s, d, k, ou_seed=ou))
-            assert np.array_equal(alone, mixed[i]), f"request {i} differs in the mix"
-            assert times[2] >= times[1] >= 0
+        assert st["error"] == 0 and st["completed"] == sum(len(p[2]) for p in plan)
+        assert st["episodes_ended"] > 0
+    for i, p in enumerate(plan):
+        with Server(512, config=CFG) as sv:
+            alone = run_session(sv, *p)
+        for (a, b) in zip(alone, mixed[i]):
+            for x, y in zip(a, b):
+                assert np.array_equal(x, y), f"session {i} differs in the mix"
 
 
-def test_given_actions_equal_direct_stepping():
-    import torch
-
+def test_resident_worlds_continue_across_requests():
     rng = np.random.default_rng(2)
-    n, k = 45, 4
-    seeds = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    n = 48
     diff = rng.uniform(0, 1, n)
-    actions = rng.uniform(-1.2, 1.2, (k, n, 12)).astype(np.float32)
-    with Server(64) as sv:
-        served, _ = sv.wait(sv.submit(seeds, diff, k, actions=actions))
-    sim = Sim(n)
-    sim.set_kernel(KERNEL_WARPS)
-    sim.reset(np.arange(n), seeds, diff)
-    d_ids = torch.arange(n, dtype=torch.int32, device="cuda")
-    for t in range(k):
-        d_a = torch.as_tensor(actions[t], device="cuda")
-        torch.cuda.synchronize()
-        sim.step_ids(d_ids.data_ptr(), n, d_actions=d_a.data_ptr())
-        sim.synchronize()
-    assert np.array_equal(served, sim.get_state())
+    act = rng.uniform(-1, 1, (7, n, 12)).astype(np.float32)
+    with Server(64, config=CFG) as sv:
+        split = run_session(sv, diff, 9, [(3, act[:3], 0), (4, act[3:], 0)])
+        whole = run_session(sv, diff, 9, [(7, act, 0)])
+    assert np.array_equal(np.concatenate([split[0][1], split[1][1]]), whole[0][1])
+    assert np.array_equal(np.concatenate([split[0][2], split[1][2]]), whole[0][2])
+    assert np.array_equal(split[1][0], whole[0][0])
 
 
-def test_observation_results_match_observe():
-    """A server returning observations gives, per world, the blocks
-    arc_sim_observe gives for the same worlds stepped the same way."""
-    rng = np.random.default_rng(3)
-    n, k = 37, 3
-    seeds = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
-    diff = rng.uniform(0, 1, n)
-    actions = rng.uniform(-1, 1, (k, n, 12)).astype(np.float32)
-    with Server(128, result="state") as a, Server(128, result="observe") as b:
-        state, _ = a.wait(a.submit(seeds, diff, k, actions=actions))
-        obs, _ = b.wait(b.submit(seeds, diff, k, actions=actions))
-    sim = Sim(n)
-    sim.set_state(state)
-    root, joints, contacts, flags = sim.observe()
-    assert obs.shape == (n, 65)
-    assert np.array_equal(obs[:, :13], root)
-    assert np.array_equal(obs[:, 13:22], sim.rot.reshape(n, 9))
-    assert np.array_equal(obs[:, 22:58], joints)
-    assert np.array_equal(obs[:, 58:64], contacts)
-    assert np.array_equal(obs[:, 64], flags.astype(np.float64))
+def test_episode_end_resets_in_place():
+    n, k = 64, 12
+    with Server(n, config=CFG) as sv:
+        sid = sv.open(np.zeros(n), 3)
+        (obs, rew, done), _ = sv.wait(sv.request(sid, k, actions=np.zeros((k, n, 12), np.float32)))
+    assert np.isfinite(obs).all() and np.isfinite(rew).all()
+    ended = done != 0
+    # a flat world under zero actions stands: truncated (bit 1) after 5 and 10 steps
+    assert np.array_equal(done[4], np.full(n, 2, np.uint8)) and np.array_equal(done[9], np.full(n, 2, np.uint8))
+    assert ended.sum() == 2 * n
+    # the step after an episode end starts the next episode: its reward is an ordinary step's
+    assert np.all(np.abs(rew[5]) < 10.0)
 
 
-def test_request_larger_than_the_pool_is_refused():
-    with Server(16) as sv:
+def test_slots_budget_ticks_and_errors():
+    with Server(100, config=CFG, tick_cap=60) as sv:
+        a = sv.open(np.zeros(70), 1)
+        b = sv.open(np.zeros(50), 2)          # waits: only 30 slots left
+        ra = sv.request(a, 3)
+        rb = sv.request(b, 2)
+        sv.wait(ra)
+        st = sv.stats()
+        assert st["waiting_sessions"] == 1 and st["resident"] == 70
+        sv.close_session(a)                    # frees 70 slots: b is admitted
+        sv.wait(rb)
+        c = sv.open(np.zeros(40), 3)
+        rc = [sv.request(c, 4) for _ in range(2)]
+        rb2 = sv.request(b, 4)
+        for r in rc + [rb2]:
+            sv.wait(r)
+        st = sv.stats()
+        assert st["error"] == 0
+        assert st["max_active"] <= 70          # the first session alone (70 > cap), then <= 60 a tick
         with pytest.raises(RuntimeError):
-            sv.submit(np.arange(17, dtype=np.uint32), np.zeros(17), 1)
-        # the engine keeps serving
-        out, _ = sv.wait(sv.submit(np.arange(16, dtype=np.uint32), np.zeros(16), 2))
-        assert np.isfinite(out).all()
-
-
-def test_malformed_requests_are_refused_and_the_engine_keeps_serving():
-    """Faults made on the host: bad sizes are refused at submit, an unknown
-    request id at wait, and none of it disturbs the engine."""
-    import ctypes
-
-    from arc_demo_b200.serve import serve_lib
-
-    lib = serve_lib()
-    with Server(32) as sv:
-        seeds = np.arange(4, dtype=np.uint32)
-        diff = np.zeros(4)
-        for n, k in ((0, 1), (4, 0), (4, -3), (33, 1)):
-            rid = lib.arc_server_submit(sv._ptr, n, k, seeds, diff, None, 0, None)
-            assert rid < 0, (n, k)
-        assert lib.arc_server_wait(sv._ptr, 123456, 0.1, None, None) < 0
-        out, _ = sv.wait(sv.submit(seeds, diff, 3))
-        assert np.isfinite(out).all() and sv.stats()["error"] == 0
-
-
-def test_client_that_never_waits_leaves_the_server_clean():
-    """A client that submits and goes away: its request still runs, its
-    result is dropped with the server, and other clients are served."""
-    with Server(64) as sv:
-        sv.submit(np.arange(20, dtype=np.uint32), np.zeros(20), 5)     # never waited for
-        out, _ = sv.wait(sv.submit(np.arange(8, dtype=np.uint32), np.zeros(8), 2))
-        assert np.isfinite(out).all()
-    # the engine thread and every buffer were released by the close above
+            sv.open(np.zeros(101), 4)          # larger than the pool
+        sv.close_session(c)
+        with pytest.raises(RuntimeError):
+            sv.request(c, 1)                   # closed

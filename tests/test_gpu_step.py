@@ -274,10 +274,11 @@ def test_warp_per_leg_kernel_on_a_fine_grid():
     assert np.percentile(dx, 95) <= 1e-5 and np.percentile(dx, 99) <= 5e-5
 
 
-@pytest.mark.parametrize("wpc", [16, 32, 64])
+@pytest.mark.parametrize("wpc", [1, 2, 4, 16, 32, 64])
 def test_worlds_per_cta_and_ragged_batches_bitwise(wpc):
-    """Any worlds-per-CTA, and world counts that are not a multiple of it,
-    give bit-identical states (the per-world code is the same)."""
+    """Any worlds-per-CTA (CTAs of 1, 2 or 4 worlds are part of a warp), and
+    world counts that are not a multiple of it, give bit-identical states
+    (the per-world code is the same)."""
     n = 2 * wpc + 5
     seeds, diffs = seeds_diffs(n, 4)
     a, b = Sim(n), Sim(n)

@@ -193,3 +193,59 @@ def test_env_auto_reset_writes_terminal_observation():
     assert np.all(st[:, 23] == 2)        # second episode of every world
     assert torch.isfinite(env.terminal_obs).all()
     assert not torch.equal(env.terminal_obs, env.obs)
+
+
+@pytest.mark.parametrize("queue", [False, True])
+def test_fused_control_step_equals_separate_kernels(queue):
+    """The control step as one launch (k_control_step: each group's physics
+    then its rewards, observations, heights and resets in the same kernel)
+    gives the same worlds, outputs, ended-world lists and task state, bit
+    for bit, as the step kernel followed by the task, heights and reset
+    kernels; through the graph step, the step in parts and the host-buffer
+    step, with resets on most steps (max_steps 6, curriculum on)."""
+    import torch
+    from arc_demo_b200.native import KERNEL_WARPS
+    from arc_demo_b200.torch_env import DeviceVecEnv
+    n = 200
+    envs = [DeviceVecEnv(n, TaskConfig(curriculum=True, max_steps=6), seed=13) for _ in range(2)]
+    envs[1].set_fused(False)
+    for e in envs:
+        e.set_kernel(KERNEL_WARPS)
+        e.sim.set_work_queue(queue)
+        e.set_levels(np.linspace(0, 1, n))
+        e.reset()
+    rng = np.random.default_rng(8)
+    ranges = [envs[0].part_range(p, 3) for p in range(3)]
+    ended = 0
+    for k in range(15):
+        a = rng.uniform(-1.2, 1.2, (n, 12)).astype(np.float32)
+        d_a = torch.from_numpy(a).cuda()
+        torch.cuda.synchronize()
+
+        def policy(p, obs, act):
+            first, count = ranges[p]
+            act.copy_(d_a[first:first + count])
+        for e in envs:
+            if k % 3 == 0:
+                e.step(d_a)
+            elif k % 3 == 1:
+                e.step_parts(policy, 3)
+            else:
+                e.step_host(torch.from_numpy(a))
+        torch.cuda.synchronize()
+        x, y = envs
+        for u, v in ((x.obs, y.obs), (x.reward, y.reward), (x.terminated, y.terminated),
+                     (x.truncated, y.truncated), (x.cause, y.cause)):
+            assert torch.equal(u, v), k
+        if k % 3 == 2:  # the host-buffer step's outputs are its pinned tensors
+            for u, v in zip(x._host_out, y._host_out):
+                assert torch.equal(u, v), k
+        nd = int(x.done_count.item())
+        assert nd == int(y.done_count.item())
+        ended += nd
+        assert sorted(x.done_list[:nd].tolist()) == sorted(y.done_list[:nd].tolist())
+        done = x.done_list[:nd].long()
+        assert torch.equal(x.terminal_obs[done], y.terminal_obs[done])
+        assert np.array_equal(x.sim.get_state(), y.sim.get_state(), equal_nan=True)
+        assert np.array_equal(x.gpu.get_state(), y.gpu.get_state(), equal_nan=True)
+    assert ended > n  # most worlds went through at least one reset
