@@ -28,6 +28,7 @@ constexpr int kGridMax = 64;     // csrc/arc_terrain.h:10
 constexpr int kBodyRec = 13;
 constexpr int kSphereRec = 6;
 constexpr int kJointRec = 4;
+constexpr int kContactRec = 8;
 constexpr int kNumLegs = 4;      // csrc/arc_robot.h:19-20
 constexpr int kNumJoints = 12;
 
@@ -68,6 +69,11 @@ template <class R> struct Worlds {
     const TerrainGeom<R>* tg;
     const TerrainGeomD* tgd;
     int n;
+    // the last substep's contact list per world (csrc/arc_phys.h:100-112),
+    // written by the step kernels when not NULL: kMaxContacts records of
+    // kContactRec R (body, local3, n3, unused) and the count
+    R* lastc = nullptr;
+    int* lastn = nullptr;
 #ifdef ARC_DEVICE_CHECKS
     const int* grid_of = nullptr;  // terrain capacity of each world: grid_of[i]^2 columns
 #endif

@@ -63,6 +63,8 @@ struct arc_sim {
     int* queue = nullptr;        // work queue of the warp-per-leg kernel (two ints)
     bool use_queue = false;
     bool fused = true;  // the env's control step as one launch where it applies (arc_env_set_fused)
+    void* lastc = nullptr;     // [n][kMaxContacts][kContactRec] R: the last substep's contacts (recording on)
+    int* lastn = nullptr;      // [n] their counts
     int substep_tile = 0;      // warp-per-leg step: substeps per launch (0: the whole control step)
     float* tile_q = nullptr;   // [n][13][4] position-pass quaternions between tiles
     void* spill = nullptr;
@@ -87,6 +89,7 @@ struct arc_sim {
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t graph_stream = nullptr;
     int graph_kernel = -1, graph_wpc = -1, graph_queue = -1, graph_fused = -1, graph_tile = -1;  // the captured form
+    void* graph_lastc = nullptr;
     // arc_env_step_host: world indices 0..n-1, per-chunk ended-world lists and
     // counts, the two copy streams and their events
     int* iota = nullptr;
@@ -171,6 +174,8 @@ template <class R> Worlds<R> view(const arc_sim* s)
     w.tg = static_cast<const TerrainGeom<R>*>(s->tg);
     w.tgd = s->tgd;
     w.n = s->n;
+    w.lastc = static_cast<R*>(s->lastc);
+    w.lastn = s->lastn;
 #ifdef ARC_DEVICE_CHECKS
     w.grid_of = s->grid_of;
 #endif
@@ -272,7 +277,7 @@ void free_all(arc_sim* s)
         cudaFree(p);
     void* ps[] = {s->rec, s->sph, s->unstable, s->time, s->th, s->toff, s->tg, s->tgd, s->grid_of, s->spill, s->queue,
                   s->st_in.p, s->st_in2.p, s->st_in3.p, s->st_out.p, s->iota, s->chunk_done, s->chunk_count,
-                  s->part_queue, s->tile_q};
+                  s->part_queue, s->tile_q, s->lastc, s->lastn};
     for (void* p : ps)
         if (p)
             cudaFree(p);
@@ -887,6 +892,41 @@ const arc_world* arc_sim_world(const arc_sim* s, int i)
         o.lim[2] = std::cos(t.hi);
         o.lim[3] = std::sin(t.hi);
     }
+    // the contact list of the last substep (csrc/arc_phys.c:493-499), once
+    // the kernels record it: the first call turns recording on
+    if (!s->lastc) {
+        arc_sim_set_record_contacts(ms, 1);
+    } else {
+        const size_t rec = (size_t)kMaxContacts * kContactRec;
+        int count = 0;
+        std::vector<double> c(rec);
+        cudaStream_t st = s->stream;
+        bool good = check(s, cudaMemcpyAsync(&count, s->lastn + i, sizeof(int), cudaMemcpyDeviceToHost, st),
+                          "contact count") == ARC_OK;
+        if (s->fp64) {
+            good = good && check(s, cudaMemcpyAsync(c.data(), static_cast<double*>(s->lastc) + (size_t)i * rec,
+                                                    sizeof(double) * rec, cudaMemcpyDeviceToHost, st),
+                                 "contacts") == ARC_OK;
+            good = good && check(s, cudaStreamSynchronize(st), "contacts") == ARC_OK;
+        } else {
+            std::vector<float> f(rec);
+            good = good && check(s, cudaMemcpyAsync(f.data(), static_cast<float*>(s->lastc) + (size_t)i * rec,
+                                                    sizeof(float) * rec, cudaMemcpyDeviceToHost, st),
+                                 "contacts") == ARC_OK;
+            good = good && check(s, cudaStreamSynchronize(st), "contacts") == ARC_OK;
+            for (size_t k = 0; k < rec; ++k)
+                c[k] = f[k];
+        }
+        if (!good)
+            return nullptr;
+        w->n_contacts = std::max(0, std::min(count, kMaxContacts));
+        for (int k = 0; k < w->n_contacts; ++k) {
+            const double* r = c.data() + (size_t)k * kContactRec;
+            w->contacts[k].body = (int)r[0];
+            w->contacts[k].local = arcw_vec3{r[1], r[2], r[3]};
+            w->contacts[k].n = arcw_vec3{r[4], r[5], r[6]};
+        }
+    }
     w->n_visuals = m.nv;
     for (int k = 0; k < m.nv; ++k) {
         const ModelHost::Visual& v = m.v[k];
@@ -1214,6 +1254,34 @@ int arc_sim_step_ids(arc_sim* s, const int* d_ids, int n_ids, const double* d_ta
 int arc_sim_set_work_queue(arc_sim* s, int on)
 {
     s->use_queue = on != 0;
+    return ARC_OK;
+}
+
+int arc_sim_set_record_contacts(arc_sim* s, int on)
+{
+    if (!on) {
+        cudaFree(s->lastc);
+        cudaFree(s->lastn);
+        s->lastc = nullptr;
+        s->lastn = nullptr;
+        return ARC_OK;
+    }
+    if (s->lastc)
+        return ARC_OK;
+    const size_t n = (size_t)std::max(s->n, 1);
+    void* c = nullptr;
+    int* k = nullptr;
+    if (check(s, cudaMalloc(&c, n * kMaxContacts * kContactRec * real_size(s)), "cudaMalloc(contact lists)"))
+        return ARC_ERR_CUDA;
+    if (check(s, cudaMalloc((void**)&k, n * sizeof(int)), "cudaMalloc(contact counts)") ||
+        check(s, cudaMemsetAsync(k, 0, n * sizeof(int), s->stream), "zero contact counts") ||
+        check(s, cudaStreamSynchronize(s->stream), "contact lists")) {
+        cudaFree(c);
+        cudaFree(k);
+        return ARC_ERR_CUDA;
+    }
+    s->lastc = c;
+    s->lastn = k;
     return ARC_OK;
 }
 
@@ -1899,7 +1967,7 @@ int arc_env_step(arc_sim* s, const float* d_actions, void* stream)
     // graph of the whole control step over the ARC_ENV_ACTIONS buffer
     if (s->graph_exec && (s->graph_kernel != s->kernel || s->graph_wpc != s->wpc ||
                           s->graph_queue != (int)s->use_queue || s->graph_fused != (int)s->fused ||
-                          s->graph_tile != s->substep_tile)) {
+                          s->graph_tile != s->substep_tile || s->graph_lastc != s->lastc)) {
         cudaGraphExecDestroy(s->graph_exec);
         cudaGraphDestroy(s->graph);
         s->graph_exec = nullptr;
@@ -1929,6 +1997,7 @@ int arc_env_step(arc_sim* s, const float* d_actions, void* stream)
         s->graph_queue = (int)s->use_queue;
         s->graph_fused = (int)s->fused;
         s->graph_tile = s->substep_tile;
+        s->graph_lastc = s->lastc;
         return ARC_OK;
     }
     return check(s, cudaGraphLaunch(s->graph_exec, st), "graph launch");

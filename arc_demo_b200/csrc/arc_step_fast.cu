@@ -344,12 +344,23 @@ k_step_fast(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, R* 
         }
         if (active) {
             const int ncl = nc < lane_cap ? nc : lane_cap;
+            // the last substep's list (lane-major is the reference's order)
+            R* lastc = W.lastc && sub == M.substeps - 1 ? W.lastc + (size_t)world * kMaxContacts * kContactRec
+                                                        : nullptr;
+            if (lastc && leg == kLanes - 1)
+                W.lastn[world] = base + ncl < kMaxContacts ? base + ncl : kMaxContacts;
             for (int c = 0; c < ncl && base + c < kMaxContacts; ++c) {
                 if (c >= kOnChip && !ARC_IN_BOUNDS(c - kOnChip, spill_per_lane, kCheckSpillRead))
                     continue;
                 const R* src = c < kOnChip ? con + c * kCRec : spl + (size_t)(c - kOnChip) * kCRec;
                 ContactRec<R> cr{V3<R>{src[0], src[1], src[2]}, V3<R>{src[3], src[4], src[5]}};
                 const int b = (int)src[6];
+                if (lastc) {
+                    R* d = lastc + (size_t)(base + c) * kContactRec;
+                    d[0] = (R)b;
+                    for (int f = 0; f < 6; ++f)
+                        d[1 + f] = src[f];
+                }
                 V3<R> v = S.v(b), w = S.w(b);
                 contact_velocity(S.rotm(b), S.iiw(b), sm.body[b].inv_mass, v, w, cr);
                 S.set_v(b, v);

@@ -109,6 +109,16 @@ k_step_plain(const __grid_constant__ DevModel<R> M, Worlds<R> W, Actuation A, co
             const int b = CB[c];
             contact_velocity(P[b].rot, P[b].iiw, M.body[b].inv_mass, V[b], Wv[b], C[c]);
         }
+        if (W.lastc && sub == M.substeps - 1) {
+            // the list the reference leaves in its world after a step
+            R* d = W.lastc + (size_t)i * kMaxContacts * kContactRec;
+            for (int c = 0; c < nc; ++c, d += kContactRec) {
+                d[0] = (R)CB[c];
+                d[1] = C[c].local.x; d[2] = C[c].local.y; d[3] = C[c].local.z;
+                d[4] = C[c].n.x; d[5] = C[c].n.y; d[6] = C[c].n.z;
+            }
+            W.lastn[i] = nc;
+        }
     }
 
     // epilogue (csrc/arc_phys.c:739-746)

@@ -476,6 +476,9 @@ __device__ __forceinline__ void step_group(Smem& sm, const DevModel<F>& M, const
             touches |= (unsigned long long)(sphr[0] & 1023u) << 50;
     }
     const uint32_t* ops = &kOps[capped ? 1 : 0][leg][0];
+    // this lane's contact records in the last substep, and how many of them
+    // the torso's sphere made (they lead the torso warp's list)
+    int last_nc = 0, last_nt = 0;
     __syncthreads();
 
     for (int sub = sub0; sub < sub1; ++sub) {
@@ -578,6 +581,8 @@ __device__ __forceinline__ void step_group(Smem& sm, const DevModel<F>& M, const
                         setv(ra, 3, ss.anchor_n);
                     }
                     store_pose(r, pose);
+                    if (a == 0)
+                        last_nt = nc;
                     break;
                 }
                 case OP_UPD:
@@ -673,8 +678,59 @@ __device__ __forceinline__ void step_group(Smem& sm, const DevModel<F>& M, const
             if (arrive)
                 bar_arrive(arrive);
         }
+        last_nc = nc;
     }
     __syncthreads();
+
+    if (last_tile && W.lastc) {
+        // the last substep's contact list in the reference's order
+        // (csrc/arc_phys.c:493-499): sphere by sphere, the torso's first. The
+        // torso's records lead the torso warp's list; with the uncapped lists
+        // that is warp 3, so its torso records go first and its leg records
+        // last; with the capped lists (warp 0 owns the torso) the lists are in
+        // warp order. Counts go through the (now free) count array.
+        sm.nc[0][leg][j] = last_nc < lane_cap ? last_nc : lane_cap;
+        sm.nc[1][leg][j] = last_nt;
+        __syncthreads();
+        if (active) {
+            int before = 0, total = 0;  // records of the warps listed ahead of this one; of all
+            for (int l = 0; l < kWarps; ++l) {
+                total += sm.nc[0][l][j];
+                if (l < leg)
+                    before += sm.nc[0][l][j];
+            }
+            const int nt = capped ? 0 : sm.nc[1][kWarps - 1][j];
+            const int mine = sm.nc[0][leg][j];
+            F* dst = W.lastc + (size_t)world * kMaxContacts * kContactRec;
+#pragma unroll 1
+            for (int c = 0; c < mine; ++c) {
+                int at = before + c;
+                if (!capped)
+                    at = leg == kWarps - 1 ? (c < nt ? c : before + c) : nt + before + c;
+                if (at >= kMaxContacts)
+                    continue;
+                F rc[7];
+                if (c < kOnChip) {
+#pragma unroll
+                    for (int f = 0; f < 7; ++f)
+                        rc[f] = sm.con[leg][c * 7 + f][j];
+                } else {
+                    if (!ARC_IN_BOUNDS(c - kOnChip, spill_per_lane, kCheckSpillRead))
+                        continue;
+                    const F* src = spill + (((size_t)wi * kWarps + leg) * (size_t)spill_per_lane + (c - kOnChip)) * 8;
+#pragma unroll
+                    for (int f = 0; f < 7; ++f)
+                        rc[f] = src[f];
+                }
+                F* d = dst + (size_t)at * kContactRec;
+                d[0] = rc[6];
+                for (int f = 0; f < 6; ++f)
+                    d[1 + f] = rc[f];
+            }
+            if (leg == 0)
+                W.lastn[world] = total < kMaxContacts ? total : kMaxContacts;
+        }
+    }
 
     if (!last_tile) {
         // hand the state to the next tile

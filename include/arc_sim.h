@@ -80,8 +80,11 @@ void arc_sim_terrain_at(const arc_sim *s, const int *ids, const double *xy, int 
  * reference's arc_world layout (arc_world.h), refreshed from the device by
  * this call and valid until the next arc_sim_world call on the same sim.
  * The robot's render-only visuals are filled in from the model (n_visuals
- * is the model's count); the last substep's contact list is not kept on the
- * device, so n_contacts is 0. */
+ * is the model's count). The contact list (n_contacts, contacts) is the last
+ * substep's, in the reference's order, once the step kernels record it: the
+ * first arc_sim_world call on a sim turns recording on (see
+ * arc_sim_set_record_contacts), so it returns n_contacts = 0 and later calls
+ * return the list of the latest step. */
 const arc_world *arc_sim_world(const arc_sim *s, int i);
 
 /* ======================================================================
@@ -202,6 +205,11 @@ int arc_sim_set_work_queue(arc_sim *s, int on);
  * or >= substeps: the whole control step in one launch, the state on chip
  * throughout. */
 int arc_sim_set_substep_tile(arc_sim *s, int tile);
+/* on != 0: the step kernels keep each world's contact list of the last
+ * substep on the device (128 records a world: 4 KB in FP32, 8 KB in FP64),
+ * which arc_sim_world returns; 0 frees it. Off until set or until the first
+ * arc_sim_world call. */
+int arc_sim_set_record_contacts(arc_sim *s, int on);
 
 /* The checked build (libarcsim_checked.so, compiled with ARC_DEVICE_CHECKS)
  * tests the kernels' data-dependent indexes - terrain columns against their

@@ -483,3 +483,67 @@ def test_large_copies_through_staging_equal_small_ones():
     only = np.zeros_like(joints)
     g._lib.arc_sim_observe(g.ptr, None, None, only.ctypes.data, None, None)
     assert np.array_equal(only, joints)
+
+
+def contact_lists(world_fn, n):
+    """Per world: (bodies, local and normal vectors) of its arc_world contact list."""
+    out = []
+    for i in range(n):
+        w = world_fn(i)
+        c = [w.contacts[k] for k in range(w.n_contacts)]
+        out.append((np.array([x.body for x in c], dtype=int),
+                    np.array([[x.local.x, x.local.y, x.local.z, x.n.x, x.n.y, x.n.z] for x in c]).reshape(-1, 6)))
+    return out
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("fp64,kernel,cell", [(True, KERNEL_PLAIN, 0.4), (True, KERNEL_LEGS, 0.4),
+                                              (False, KERNEL_WARPS, 0.4), (False, KERNEL_WARPS, 0.05),
+                                              (False, KERNEL_LEGS, 0.4)])
+def test_world_contact_list_matches_reference(fp64, kernel, cell):
+    """arc_sim_world's contact list (csrc/arc_phys.h:100-112) is the last
+    substep's, in the reference's order (sphere by sphere, torso first, at most
+    128): after a teacher-forced step the bodies of the list equal the
+    reference's wherever the sphere touch counts agree, and the records'
+    local points and normals agree to the step's precision. The 5 cm grid
+    makes lists long enough for the warp-per-leg kernel's capped form."""
+    import ctypes
+    from oracle.oracle import World
+
+    n = 48
+    seeds, diffs = seeds_diffs(n, 61)
+    diffs[:] = np.maximum(diffs, 0.3)
+    ref = RefSim(n, cell=cell)
+    g = Sim(n, cell=cell, fp64=fp64)
+    g.set_kernel(kernel, 8)
+    lib = g._lib
+    lib.arc_sim_world.restype = ctypes.POINTER(World)
+    lib.arc_sim_world.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    assert lib.arc_sim_world(g.ptr, 0).contents.n_contacts == 0  # the first call turns recording on
+    ref.reset(np.arange(n), seeds, diffs)
+    g.reset(np.arange(n), seeds, diffs)
+    rng = np.random.default_rng(3)
+    for _ in range(15):
+        ref.step(ref.default_angles + 0.6 * rng.uniform(-1, 1, (n, 12)))
+    g.set_state(ref.get_state())
+    t = ref.default_angles + 0.6 * rng.uniform(-1, 1, (n, 12))
+    ref.step(t)
+    g.step(t)
+    same_touch = (touches(ref.get_state()) == touches(g.get_state())).all(1)
+    mine = contact_lists(lambda i: lib.arc_sim_world(g.ptr, i).contents, n)
+    theirs = contact_lists(ref.world, n)
+    tol = 1e-9 if fp64 else 1e-3
+    compared, longest, differ = 0, 0, []
+    for i in range(n):
+        longest = max(longest, len(theirs[i][0]))
+        if not same_touch[i]:
+            continue
+        compared += 1
+        if not np.array_equal(mine[i][0], theirs[i][0]) or (
+                len(mine[i][0]) and np.abs(mine[i][1] - theirs[i][1]).max() > tol):
+            differ.append(i)
+    print(f"contact lists: {compared}/{n} worlds compared, longest list {longest}, differing {differ}")
+    assert compared >= 0.8 * n and longest > 0
+    # FP64 lists are the reference's; in FP32 a contact at a column edge may
+    # move to the neighbouring column without changing the touch counts
+    assert len(differ) <= (0 if fp64 else max(1, compared // 20)), differ
