@@ -55,8 +55,9 @@ cudaError_t launch_step_fast(const DevModel<R>& M, const Worlds<R>& W, const Act
 
 template <class R> size_t fast_smem_bytes(int stride, int worlds_per_cta);
 
-// Warp-per-leg step (FP32): a CTA of four warps steps 32 worlds, warp k runs
-// leg k of every world; same spill layout as launch_step_fast. Steps the
+// Warp-per-leg step (FP32, arc_task.cu): a CTA of four warps steps 32
+// worlds, warp k runs leg k of every world; same spill layout as
+// launch_step_fast. Steps the
 // n_items worlds ids[0..n_items) (ids NULL: worlds 0..n_items-1). With a
 // queue (two device ints, zero between launches) one wave of resident CTAs
 // takes groups of 32 worlds from it until none is left. tile in
@@ -65,7 +66,6 @@ template <class R> size_t fast_smem_bytes(int stride, int worlds_per_cta);
 cudaError_t launch_step_warps(const DevModel<float>& M, const Worlds<float>& W, const Actuation& A, float* spill,
                               int spill_per_lane, int lane_cap, const int* ids, int n_items, int* queue,
                               cudaStream_t stream, int tile = 0, float* tile_q = nullptr);
-size_t warps_smem_bytes();
 constexpr int kFastOnChipContacts = 2;
 constexpr int kWarpsOnChipContacts = 1;  // keeps four CTAs of the warp-per-leg kernel per SM
 // the fewest on-chip records of any kernel: a spill area of lane_cap minus

@@ -244,8 +244,8 @@ bool admit(arc_server* sv)
         while (!sv->waiting.empty() && (int)sv->free_slots.size() >= sv->waiting.front()->n) {
             auto s = sv->waiting.front();
             sv->waiting.pop_front();
-            if (s->closed)
-                continue;
+            if (s->closed && s->pending == 0)
+                continue;  // closed before admission with nothing to run (a closed session's queued requests still run)
             s->slots.assign(sv->free_slots.end() - s->n, sv->free_slots.end());
             sv->free_slots.resize(sv->free_slots.size() - s->n);
             admitted.push_back(s);

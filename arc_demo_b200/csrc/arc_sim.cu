@@ -62,7 +62,7 @@ struct arc_sim {
     size_t th_count = 0;         // columns in the terrain pool
     int* queue = nullptr;        // work queue of the warp-per-leg kernel (two ints)
     bool use_queue = false;
-    bool fused = true;  // the env's control step as one launch where it applies (arc_env_set_fused)
+    int fused = 0;  // env control step: 0 separate kernels, 1 fused step and task, 2 and resets (arc_env_set_fused)
     void* lastc = nullptr;     // [n][kMaxContacts][kContactRec] R: the last substep's contacts (recording on)
     int* lastn = nullptr;      // [n] their counts
     int substep_tile = 0;      // warp-per-leg step: substeps per launch (0: the whole control step)
@@ -1297,9 +1297,11 @@ int arc_sim_set_substep_tile(arc_sim* s, int tile)
     return ARC_OK;
 }
 
-int arc_env_set_fused(arc_sim* s, int on)
+int arc_env_set_fused(arc_sim* s, int mode)
 {
-    s->fused = on != 0;
+    if (mode < 0 || mode > 2)
+        return fail(s, ARC_ERR_ARG, "arc_env_set_fused: mode 0, 1 or 2");
+    s->fused = mode;
     return ARC_OK;
 }
 
@@ -1461,26 +1463,36 @@ template <class R> int env_reset_done(arc_sim* s, cudaStream_t st)
                  "task reset kernel");
 }
 
-// Whether the env's control step runs as one launch (the warp-per-leg step
-// and the task layer in k_control_step): FP32, the quadruped, that kernel.
+// Whether the env's control step runs fused (the warp-per-leg step and the
+// task layer in k_control_step): FP32, the quadruped, that kernel, whole
+// control steps.
 bool fused_applies(const arc_sim* s)
 {
-    return s->fused && !s->fp64 && s->mf.leaper && s->substeps <= kFastMaxSubsteps && s->kernel == ARC_KERNEL_WARPS &&
+    return s->fused > 0 && !s->fp64 && s->mf.leaper && s->substeps <= kFastMaxSubsteps && s->kernel == ARC_KERNEL_WARPS &&
            (s->substep_tile <= 0 || s->substep_tile >= s->substeps);
 }
 
-// One launch of the fused control step over ids[0 .. n) (NULL: every
-// world), its ended worlds into O's list; O.done_count is zeroed first.
+// The fused control step over ids[0 .. n) (NULL: every world), its ended
+// worlds into O's list (O.done_count zeroed first) and reset in the kernel
+// (fused == 2) or by the reset kernel after it (fused == 1).
 int env_control_step(arc_sim* s, const float* actions, const TaskOut& O, const int* ids, int n, int* queue,
                      cudaStream_t st)
 {
-    if (check(s, cudaMemsetAsync(O.done_count, 0, sizeof(int), st), "memset done_count"))
+    const bool resets = s->fused >= 2;
+    if (check(s, cudaMemsetAsync(O.done_count, 0, sizeof(int), st), "memset done_count") ||
+        check(s,
+              launch_control_step(s->mf, s->rm, view<float>(s), (TerrainGeom<float>*)s->tg, s->tgd, s->grid_of,
+                                  s->cell, s->tp, s->ts, O, actions, static_cast<float*>(s->spill),
+                                  s->spill_per_lane, s->lane_cap, ids, n, queue, resets, st),
+              "control step kernel"))
         return ARC_ERR_CUDA;
+    if (resets)
+        return ARC_OK;
     return check(s,
-                 launch_control_step(s->mf, s->rm, view<float>(s), (TerrainGeom<float>*)s->tg, s->tgd, s->grid_of,
-                                     s->cell, s->tp, s->ts, O, actions, static_cast<float*>(s->spill),
-                                     s->spill_per_lane, s->lane_cap, ids, n, queue, st),
-                 "control step kernel");
+                 launch_task_reset<float>(s->mf, s->rm, view<float>(s), (TerrainGeom<float>*)s->tg, s->tgd,
+                                          s->grid_of, s->cell, s->tp, s->ts, s->to.obs, O.done_list, O.done_count, n,
+                                          st),
+                 "task reset kernel");
 }
 
 // the whole control step of ArcVecEnv.step_wait, as launched into `st`
@@ -1966,7 +1978,7 @@ int arc_env_step(arc_sim* s, const float* d_actions, void* stream)
         return env_step_launches(s, d_actions, st);
     // graph of the whole control step over the ARC_ENV_ACTIONS buffer
     if (s->graph_exec && (s->graph_kernel != s->kernel || s->graph_wpc != s->wpc ||
-                          s->graph_queue != (int)s->use_queue || s->graph_fused != (int)s->fused ||
+                          s->graph_queue != (int)s->use_queue || s->graph_fused != s->fused ||
                           s->graph_tile != s->substep_tile || s->graph_lastc != s->lastc)) {
         cudaGraphExecDestroy(s->graph_exec);
         cudaGraphDestroy(s->graph);
@@ -1995,7 +2007,7 @@ int arc_env_step(arc_sim* s, const float* d_actions, void* stream)
         s->graph_kernel = s->kernel;
         s->graph_wpc = s->wpc;
         s->graph_queue = (int)s->use_queue;
-        s->graph_fused = (int)s->fused;
+        s->graph_fused = s->fused;
         s->graph_tile = s->substep_tile;
         s->graph_lastc = s->lastc;
         return ARC_OK;

@@ -31,14 +31,11 @@
 // q (and, after the velocity update, the normalised q the next substep
 // starts from).
 //
-// This header holds the step of one group, `step_group`, which two kernels
-// run: k_step_warps (the physics step, arc_step_warps.cu) and the fused
-// control step of the task layer (arc_task.cu), which follows each group's
-// physics with its rewards, observations and resets. Both translation units
-// are compiled with the same floating-point flags, so the two kernels give
-// the same worlds bit for bit. Everything here has internal linkage: each
-// translation unit keeps its own copy of the operation lists in its constant
-// bank.
+// This header holds the step of one group, `step_group`, which the control
+// step kernel of arc_task.cu runs, alone (the physics step) or followed by
+// the task layer on the group's worlds (the fused control step). Everything
+// here has internal linkage: the operation lists live in that translation
+// unit's constant bank.
 #pragma once
 
 #include "arc_kernels.cuh"

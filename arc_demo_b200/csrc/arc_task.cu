@@ -293,8 +293,10 @@ __device__ void place_target(const TaskParams& P, const Worlds<R>& W, const Task
 // arc/task.py:155-220 (+ 231-259 for the observation): one thread per world
 
 // One world's step of the task layer; returns whether its episode ended.
+// Compiled once (not inlined): the separate task kernel and the fused
+// control step run the same code.
 template <class R>
-__device__ bool task_step_world(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskState& S,
+__device__ __noinline__ bool task_step_world(const DevModel<R>& M, const Worlds<R>& W, const TaskParams& P, const TaskState& S,
                                 const TaskOut& O, const float* __restrict__ actions, int write_obs_rows, int i)
 {
     Obs64 o;
@@ -415,9 +417,10 @@ constexpr int kHeightsAt = 9 + 3 * kNumJoints + 3;  // offset of the heights in 
 constexpr int kHeightThreads = 128;
 constexpr int kHeightBlocks = 8;
 
-// Part `part` (kHeightsPer samples) of world i's observation heights.
+// Part `part` (kHeightsPer samples) of world i's observation heights
+// (compiled once, as task_step_world).
 template <class R>
-__device__ __forceinline__ void task_heights_part(const Worlds<R>& W, const TaskParams& P, const TaskOut& O, int i,
+__device__ __noinline__ void task_heights_part(const Worlds<R>& W, const TaskParams& P, const TaskOut& O, int i,
                                                   int part)
 {
     const int m0 = part * kHeightsPer, m1 = m0 + kHeightsPer < kNumOffsets ? m0 + kHeightsPer : kNumOffsets;
@@ -690,9 +693,9 @@ k_reset_warp(const __grid_constant__ ResetModel RM, Worlds<R> W, TerrainGeom<R>*
 }
 
 // ArcTask.reset (arc/task.py:113-125) + the observation of the new episode,
-// by the 32 lanes of one warp.
+// by the 32 lanes of one warp (compiled once, as task_step_world).
 template <class R>
-__device__ void task_reset_world(ResetSmem& sm, const DevModel<R>& M, const ResetModel& RM, const Worlds<R>& W,
+__device__ __noinline__ void task_reset_world(ResetSmem& sm, const DevModel<R>& M, const ResetModel& RM, const Worlds<R>& W,
                                  TerrainGeom<R>* tg, TerrainGeomD* tgd, const int* __restrict__ grid_of, double cell,
                                  const TaskParams& P, const TaskState& S, float* obs, int i)
 {
@@ -759,16 +762,23 @@ __global__ void k_task_set_targets(Worlds<R> W, const __grid_constant__ TaskPara
 }
 
 // ---------------------------------------------------------------------------
-// The whole control step of ArcVecEnv.step_wait (arc/env.py:99-117) in one
-// launch, for the quadruped in FP32: each CTA steps a group of 32 worlds with
-// the warp-per-leg step (arc_step_warps.cuh), then runs the task layer on
-// those worlds - rewards, terminations and observations (one thread per
-// world), the observations' terrain heights (all threads), and the reset of
-// the worlds whose episode ended (one warp per world) - before it takes the
-// next group. Every world sees exactly the work of the separate kernels
-// (k_step_warps, k_task_step, k_task_heights, k_task_reset), in the same
-// order, so the results are theirs bit for bit; the ended-world list is filled
-// in completion order, as the separate task kernel fills it.
+// The warp-per-leg step (FP32, the quadruped) and, fused with it, the task
+// layer of ArcVecEnv.step_wait (arc/env.py:99-117). One kernel serves every
+// form, so all of them run the same compiled physics:
+//   kPhysics      the step alone (arc_sim_step, the separate env step, tiles
+//                 of substeps);
+//   kWithTask     each CTA steps a group of 32 worlds, then, before its next
+//                 group, runs the task step on them (warp 0, one lane per
+//                 world) and their observations' heights (all threads); the
+//                 ended worlds go to the ended-world list, which a separate
+//                 reset launch then takes;
+//   kWithResets   the same, and the group's ended worlds are reset in the
+//                 kernel too, one warp each.
+// The task functions are compiled once (not inlined) and called both from
+// here and from the separate task kernels, so every form gives the same
+// results bit for bit; the ended-world list is filled in completion order,
+// as the separate task kernel fills it.
+enum : int { kPhysics = 0, kWithTask = 1, kWithResets = 2 };
 
 struct ControlSmem {
     union {
@@ -783,19 +793,21 @@ struct ControlSmem {
 __global__ void __launch_bounds__(wl::kThreads, 4)
 k_control_step(const __grid_constant__ DevModel<float> M, const __grid_constant__ ResetModel RM, Worlds<float> W,
                TerrainGeom<float>* tg, TerrainGeomD* tgd, const int* __restrict__ grid_of, double cell,
-               const __grid_constant__ TaskParams P, TaskState S, TaskOut O, const float* __restrict__ actions,
+               const __grid_constant__ TaskParams P, TaskState S, TaskOut O, Actuation A,
                float* __restrict__ spill, int spill_per_lane, int lane_cap, const int* __restrict__ ids, int n_items,
-               int* queue)
+               int* queue, int mode, int sub0, int sub1, float* __restrict__ tile_q)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ControlSmem& cs = *reinterpret_cast<ControlSmem*>(smem_raw);
     const int tid = threadIdx.x, leg = tid / wl::kWorlds, j = tid % wl::kWorlds;
     const int n_groups = (n_items + wl::kWorlds - 1) / wl::kWorlds;
-    const Actuation A{nullptr, actions};
     auto world_of = [&](int item) {
         const int w = item < n_items ? (ids ? ids[item] : item) : -1;
         return w >= 0 && w < W.n ? w : -1;
     };
+    // with a queue every group, the first included, is taken from it: a CTA
+    // that becomes resident only when others leave finds the queue empty
+    // instead of holding back a group of its own
     int first = blockIdx.x;
     if (queue) {
         if (tid == 0)
@@ -805,32 +817,36 @@ k_control_step(const __grid_constant__ DevModel<float> M, const __grid_constant_
     }
 #pragma unroll 1
     for (int group = first; group < n_groups;) {
-        wl::step_group(cs.step, M, W, A, spill, spill_per_lane, lane_cap, ids, n_items, group, tid, leg, j, 0,
-                       M.substeps, nullptr);
-        if (tid == 0)
-            cs.n_ended = 0;
-        __syncthreads();
-        // arc/task.py:155-259 but the heights; warp 0's lane j takes the world
-        // its own lane stepped as leg 0 (time and unstable written by it)
-        if (tid < wl::kWorlds) {
-            const int world = world_of(group * wl::kWorlds + j);
-            if (world >= 0 && task_step_world(M, W, P, S, O, actions, 2, world))
-                cs.ended[atomicAdd(&cs.n_ended, 1)] = world;
-        }
-        __syncthreads();
+        wl::step_group(cs.step, M, W, A, spill, spill_per_lane, lane_cap, ids, n_items, group, tid, leg, j, sub0, sub1,
+                       tile_q);
+        if (mode != kPhysics) {
+            if (tid == 0)
+                cs.n_ended = 0;
+            __syncthreads();
+            // arc/task.py:155-259 but the heights; warp 0's lane j takes the
+            // world its own lane stepped as leg 0 (time and unstable written by it)
+            if (tid < wl::kWorlds) {
+                const int world = world_of(group * wl::kWorlds + j);
+                if (world >= 0 && task_step_world(M, W, P, S, O, A.actions32, 2, world))
+                    cs.ended[atomicAdd(&cs.n_ended, 1)] = world;
+            }
+            __syncthreads();
 #pragma unroll 1
-        for (int t = tid; t < wl::kWorlds * kHeightParts; t += wl::kThreads) {
-            const int world = world_of(group * wl::kWorlds + t / kHeightParts);
-            if (world >= 0)
-                task_heights_part(W, P, O, world, t % kHeightParts);
-        }
-        __syncthreads();
+            for (int t = tid; t < wl::kWorlds * kHeightParts; t += wl::kThreads) {
+                const int world = world_of(group * wl::kWorlds + t / kHeightParts);
+                if (world >= 0)
+                    task_heights_part(W, P, O, world, t % kHeightParts);
+            }
+            if (mode == kWithResets) {
+                __syncthreads();
 #pragma unroll 1
-        for (int e = leg; e < cs.n_ended; e += wl::kWarps)
-            task_reset_world(cs.reset[leg], M, RM, W, tg, tgd, grid_of, cell, P, S, O.obs, cs.ended[e]);
+                for (int e = leg; e < cs.n_ended; e += wl::kWarps)
+                    task_reset_world(cs.reset[leg], M, RM, W, tg, tgd, grid_of, cell, P, S, O.obs, cs.ended[e]);
+            }
+        }
         if (!queue)
             break;
-        __syncthreads();  // the resets' shared memory is the next group's step
+        __syncthreads();  // this group's task and reset work is done with the shared memory
         if (tid == 0)
             cs.next = atomicAdd(queue, 1);
         __syncthreads();
@@ -847,6 +863,45 @@ k_control_step(const __grid_constant__ DevModel<float> M, const __grid_constant_
             }
         }
     }
+}
+
+// One launch of k_control_step over the n_items worlds ids[0 .. n_items).
+cudaError_t control_launch(const DevModel<float>& M, const ResetModel& RM, const Worlds<float>& W,
+                           TerrainGeom<float>* tg, TerrainGeomD* tgd, const int* grid_of, double cell,
+                           const TaskParams& P, const TaskState& S, const TaskOut& O, const Actuation& A,
+                           float* spill, int spill_per_lane, int lane_cap, const int* ids, int n_items, int* queue,
+                           int mode, int sub0, int sub1, float* tile_q, cudaStream_t stream)
+{
+    const int smem = (int)sizeof(ControlSmem);
+    // per device: the shared-memory attribute, and how many CTAs are resident
+    // at once (the work queue's wave)
+    static std::atomic<unsigned long long> configured{0};
+    static int resident[64] = {};
+    cudaError_t e = once_per_device(configured, [&](int dev) {
+        cudaError_t r = cudaFuncSetAttribute(k_control_step, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        int sms = 0, per_sm = 0;
+        if (r == cudaSuccess)
+            r = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (r == cudaSuccess)
+            r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_control_step, wl::kThreads, smem);
+        if (r == cudaSuccess)
+            resident[dev] = sms * (per_sm > 0 ? per_sm : 1);
+        return r;
+    });
+    if (e != cudaSuccess)
+        return e;
+    const int groups = (n_items + wl::kWorlds - 1) / wl::kWorlds;
+    int grid = groups;
+    if (queue) {
+        int dev = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess)
+            return e;
+        grid = groups < resident[dev] ? groups : resident[dev];  // one wave of resident CTAs
+    }
+    k_control_step<<<grid, wl::kThreads, smem, stream>>>(M, RM, W, tg, tgd, grid_of, cell, P, S, O, A, spill,
+                                                         spill_per_lane, lane_cap, ids, n_items, queue, mode, sub0,
+                                                         sub1, tile_q);
+    return cudaGetLastError();
 }
 
 template <class R>
@@ -987,39 +1042,39 @@ cudaError_t launch_control_step(const DevModel<float>& M, const ResetModel& RM, 
                                 TerrainGeom<float>* tg, TerrainGeomD* tgd, const int* grid_of, double cell,
                                 const TaskParams& P, const TaskState& S, const TaskOut& O, const float* actions,
                                 float* spill, int spill_per_lane, int lane_cap, const int* ids, int n_items, int* queue,
-                                cudaStream_t stream)
+                                bool resets, cudaStream_t stream)
 {
     if (W.n <= 0 || n_items <= 0)
         return cudaSuccess;
     if (!M.leaper)
         return cudaErrorInvalidValue;
-    const int smem = (int)sizeof(ControlSmem);
-    static std::atomic<unsigned long long> configured{0};
-    static int resident[64] = {};
-    cudaError_t e = once_per_device(configured, [&](int dev) {
-        cudaError_t r = cudaFuncSetAttribute(k_control_step, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        int sms = 0, per_sm = 0;
-        if (r == cudaSuccess)
-            r = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (r == cudaSuccess)
-            r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_control_step, wl::kThreads, smem);
-        if (r == cudaSuccess)
-            resident[dev] = sms * (per_sm > 0 ? per_sm : 1);
-        return r;
-    });
-    if (e != cudaSuccess)
-        return e;
-    const int groups = (n_items + wl::kWorlds - 1) / wl::kWorlds;
-    int grid = groups;
-    if (queue) {
-        int dev = 0;
-        if ((e = cudaGetDevice(&dev)) != cudaSuccess)
+    return control_launch(M, RM, W, tg, tgd, grid_of, cell, P, S, O, Actuation{nullptr, actions}, spill,
+                          spill_per_lane, lane_cap, ids, n_items, queue, resets ? kWithResets : kWithTask, 0,
+                          M.substeps, nullptr, stream);
+}
+
+cudaError_t launch_step_warps(const DevModel<float>& M, const Worlds<float>& W, const Actuation& A, float* spill,
+                              int spill_per_lane, int lane_cap, const int* ids, int n_items, int* queue,
+                              cudaStream_t stream, int tile, float* tile_q)
+{
+    if (W.n <= 0 || n_items <= 0)
+        return cudaSuccess;
+    if (!M.leaper)
+        return cudaErrorInvalidValue;
+    // the task layer's parameters, which the physics alone does not read
+    static const ResetModel RM{};
+    static const TaskParams P{};
+    if (tile <= 0 || tile >= M.substeps || !tile_q)
+        tile = M.substeps;
+    for (int sub0 = 0; sub0 < M.substeps; sub0 += tile) {
+        const int sub1 = sub0 + tile < M.substeps ? sub0 + tile : M.substeps;
+        cudaError_t e = control_launch(M, RM, W, nullptr, nullptr, nullptr, 0.0, P, TaskState{}, TaskOut{}, A, spill,
+                                       spill_per_lane, lane_cap, ids, n_items, queue, kPhysics, sub0, sub1, tile_q,
+                                       stream);
+        if (e != cudaSuccess)
             return e;
-        grid = groups < resident[dev] ? groups : resident[dev];
     }
-    k_control_step<<<grid, wl::kThreads, smem, stream>>>(M, RM, W, tg, tgd, grid_of, cell, P, S, O, actions, spill,
-                                                         spill_per_lane, lane_cap, ids, n_items, queue);
-    return cudaGetLastError();
+    return cudaSuccess;
 }
 
 #define ARC_INSTANTIATE_TASK(R)                                                                                    \

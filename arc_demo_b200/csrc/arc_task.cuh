@@ -90,19 +90,22 @@ cudaError_t launch_task_reset(const DevModel<R>& M, const ResetModel& RM, const 
                               const TaskState& S, float* obs, const int* ids, const int* count_dev, int max_n,
                               cudaStream_t stream);
 
-// The whole control step (step, rewards, terminations, observations, resets
-// of ended worlds) in one launch, for the quadruped in FP32: the warp-per-leg
-// step of each group of 32 worlds followed by the task layer on them. The
-// worlds are ids[0 .. n_items) (ids nullptr: 0 .. n_items - 1); with a queue
-// (two device ints, zero between launches) one wave of resident CTAs takes
-// the groups. O.done_count must be zero before the launch. The results equal
-// launch_step_warps, launch_task_step (write_obs 2), launch_task_heights and
-// launch_task_reset over O.done_list in turn, bit for bit.
+// The control step (step, rewards, terminations, observations and, with
+// resets, the reset of ended worlds) fused into one launch, for the
+// quadruped in FP32: the warp-per-leg step of each group of 32 worlds
+// followed by the task layer on them. The worlds are ids[0 .. n_items) (ids
+// nullptr: 0 .. n_items - 1); with a queue (two device ints, zero between
+// launches) one wave of resident CTAs takes the groups. O.done_count must be
+// zero before the launch. Without resets the ended worlds are only listed
+// (O.done_list), for launch_task_reset. The results equal launch_step_warps,
+// launch_task_step (write_obs 2), launch_task_heights and launch_task_reset
+// over O.done_list in turn, bit for bit: the same kernel runs the physics in
+// every form, and the task functions are compiled once.
 cudaError_t launch_control_step(const DevModel<float>& M, const ResetModel& RM, const Worlds<float>& W,
                                 TerrainGeom<float>* tg, TerrainGeomD* tgd, const int* grid_of, double cell,
                                 const TaskParams& P, const TaskState& S, const TaskOut& O, const float* actions,
                                 float* spill, int spill_per_lane, int lane_cap, const int* ids, int n_items, int* queue,
-                                cudaStream_t stream);
+                                bool resets, cudaStream_t stream);
 
 // Starts worlds ids[0 .. n) (device arrays) afresh as new tenants of their
 // slots: level and difficulty, RNG key and RNG counters set, then a task

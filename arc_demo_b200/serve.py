@@ -95,7 +95,9 @@ class Server:
 
     def request(self, session: int, steps: int, actions=None, ou_seed: int = 0, obs: bool = True) -> int:
         """Steps a session; actions (steps x n x 12) or an OU process."""
-        n = self._sizes[session]
+        n = self._sizes.get(session)
+        if n is None:
+            raise RuntimeError(f"session {session} is not open")
         act = None
         if actions is not None:
             act = np.ascontiguousarray(actions, dtype=np.float32)

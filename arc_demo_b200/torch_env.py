@@ -64,11 +64,12 @@ class DeviceVecEnv:
     def set_kernel(self, kernel: int, worlds_per_cta: int = 16) -> None:
         self.sim.set_kernel(kernel, worlds_per_cta)
 
-    def set_fused(self, on: bool) -> None:
-        """With the warp-per-leg kernel, each control step is one fused launch
-        (the default) or the step kernel followed by the task, heights and
-        reset kernels; the results are the same bit for bit."""
-        self.sim._check(self.gpu.lib.arc_env_set_fused(self.sim.ptr, int(bool(on))))
+    def set_fused(self, mode: int) -> None:
+        """With the warp-per-leg kernel: 0 the step kernel, then the task,
+        heights and reset kernels; 1 the step and the task layer fused per
+        group of 32 worlds, the resets after; 2 the resets fused too (one
+        launch per control step). The results are the same bit for bit."""
+        self.sim._check(self.gpu.lib.arc_env_set_fused(self.sim.ptr, int(mode)))
 
     def set_levels(self, levels) -> None:
         """Per-world terrain difficulty levels (the curriculum state)."""

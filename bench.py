@@ -232,20 +232,26 @@ def autotune(env, torch, stream,
     return best, table
 
 
-def autotune_parts(env, torch, stream, one_step, candidates=("1", "1 separate", "2", "4"), steps=6):
-    """How the control step runs (by timing whole control steps, each
-    candidate from the same world and task states): "1", the policy then the
-    whole step as one CUDA graph whose step is one fused launch (each group's
-    physics, rewards, observations and resets in one kernel); "1 separate",
-    the same graph with the step kernel followed by the task, heights and
-    reset kernels; "2", "4", the worlds in that many ranges on their own
-    streams (DeviceVecEnv.step_parts), each range's policy then its step."""
+FORMS = {0: "step kernel, then task, heights and reset kernels",
+         1: "step and task layer fused per group of 32 worlds, then the reset kernel",
+         2: "step, task layer and resets fused: one launch per control step"}
+
+
+def autotune_parts(env, torch, stream, one_step,
+                   candidates=((1, 0), (1, 1), (1, 2), (2, 0), (2, 1), (4, 0), (4, 1)), steps=6):
+    """How the control step runs, by timing whole control steps (policy
+    included), each candidate from the same world and task states: (ranges,
+    form). Ranges 1: the policy, then env.step() as one CUDA graph; 2, 4: the
+    worlds in that many ranges on their own streams (DeviceVecEnv.step_parts),
+    each range's policy then its step. Forms (DeviceVecEnv.set_fused): 0 the
+    step kernel, then the task, heights and reset kernels; 1 the step and the
+    task layer fused per group of 32 worlds, then the reset kernel; 2 the
+    resets fused too."""
     table = {}
     stream.synchronize()
     start, tstart = env.sim.get_state(), env.gpu.get_state()
-    for cand in candidates:
-        parts = int(cand.split()[0])
-        env.set_fused(cand != "1 separate")
+    for parts, form in candidates:
+        env.set_fused(form)
         env.sim.set_state(start)
         env.gpu.set_state(tstart)
         torch.cuda.synchronize()
@@ -257,13 +263,13 @@ def autotune_parts(env, torch, stream, one_step, candidates=("1", "1 separate", 
             one_step(parts)
         e1.record(stream)
         e1.synchronize()
-        table[cand] = round(e0.elapsed_time(e1) / steps, 4)
+        table[f"{parts} ranges, form {form}"] = round(e0.elapsed_time(e1) / steps, 4)
     env.sim.set_state(start)
     env.gpu.set_state(tstart)
     torch.cuda.synchronize()
-    best = min(candidates, key=lambda c: table[c])
-    env.set_fused(best != "1 separate")
-    return int(best.split()[0]), best, table
+    parts, form = min(candidates, key=lambda c: table[f"{c[0]} ranges, form {c[1]}"])
+    env.set_fused(form)
+    return parts, form, table
 
 
 def max_over_ranks(torch, dist, x: float) -> float:
@@ -330,7 +336,8 @@ def run_ours(args) -> dict | None:
                 env.step_parts(part_policy, parts)
 
         if args.parts:
-            parts, form, parts_tune = args.parts, str(args.parts), None
+            parts, form, parts_tune = args.parts, 0, None
+            env.set_fused(0)
         else:
             parts, form, parts_tune = autotune_parts(env, torch, stream, one_step)
         env.reset()
@@ -446,11 +453,12 @@ def run_ours(args) -> dict | None:
     kernel_name = ("warp-per-leg" + (", work queue" if cand != "warps" else "") +
                    (f", {cand[4:]} substeps per launch" if cand.startswith("tile") else "")
                    if cand.startswith(("warps", "tile")) else "leg-parallel")
-    fused = form != "1 separate" and cand.startswith("warps")
-    # our launches per control step: the fused control step (one per range)
-    # or the step, task, heights and reset kernels (per range), the ranges'
-    # merge, the memset of the ended-world count not counted (not a kernel)
-    per_part = 1 if fused else 4
+    form = form if cand.startswith("warps") else 0  # the fused forms need the warp-per-leg kernel
+    # our launches per control step and range: the step, task, heights and
+    # reset kernels (form 0), the fused step and the reset kernel (1), the
+    # fused step alone (2); the ranges' merge; the memset of the ended-world
+    # count is not a kernel
+    per_part = {0: 4, 1: 2, 2: 1}[form]
     launches = (per_part * parts + (1 if parts > 1 else 0)) * K
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "env-steps/s", "n_gpus": world, "steps": K,
@@ -464,8 +472,7 @@ def run_ours(args) -> dict | None:
                    "substeps_per_launch": int(cand[4:]) if cand.startswith("tile") else 20,
                    "autotune_step_kernel_ms": tune,
                    "parts": parts,
-                   "control_step": ("one fused launch per world range (step, rewards, observations, resets)"
-                                    if fused else "step kernel, then task, heights and reset kernels"),
+                   "control_step": FORMS[form],
                    "autotune_control_step_ms": parts_tune,
                    "loop": ("policy then env.step() (one CUDA graph) per control step" if parts == 1 else
                             f"policy and step of {parts} world ranges, each on its own stream "

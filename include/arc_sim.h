@@ -288,9 +288,8 @@ int arc_env_reset(arc_sim *s, const int *ids, int n_ids, void *stream);
  * reset of every world that ended (their pre-reset observation goes to
  * ARC_ENV_TERMINAL_OBS). d_actions == NULL: the ARC_ENV_ACTIONS buffer,
  * through a CUDA graph of the whole step captured on first use. With the
- * warp-per-leg kernel (FP32) the whole step is one kernel launch: each group
- * of 32 worlds is stepped and then gets its rewards, observations and
- * resets in the same kernel (see arc_env_set_fused). */
+ * warp-per-leg kernel (FP32) the step and the task layer can run fused (see
+ * arc_env_set_fused). */
 int arc_env_step(arc_sim *s, const float *d_actions, void *stream);
 
 /* Starts the listed worlds (host ids) afresh for a new tenant: difficulty
@@ -308,11 +307,14 @@ int arc_env_admit(arc_sim *s, const int *ids, int n_ids, const double *difficult
  * ended ones (ARC_ENV_DONE_LIST / DONE_COUNT) reset. Asynchronous on stream. */
 int arc_env_step_ids(arc_sim *s, const int *d_ids, int n_ids, void *stream);
 
-/* on != 0 (the default): with the warp-per-leg kernel, the env's control
- * step (arc_env_step, arc_env_step_part, arc_env_step_host) is one fused
- * launch; 0: the step kernel, then the task, heights and reset kernels. Both
- * give the same results bit for bit. */
-int arc_env_set_fused(arc_sim *s, int on);
+/* How the env's control step (arc_env_step, arc_env_step_part,
+ * arc_env_step_host, arc_env_step_ids) runs with the warp-per-leg kernel:
+ * 0 (the default) the step kernel, then the task, heights and reset kernels;
+ * 1 each group of 32 worlds stepped and then given its rewards,
+ * observations and heights in the same kernel, the ended worlds reset by the
+ * reset kernel after it; 2 the ended worlds reset in that kernel too (one
+ * launch per control step). All three give the same results bit for bit. */
+int arc_env_set_fused(arc_sim *s, int mode);
 
 /*
  * The same control step with host buffers, as ArcVecEnv.step_wait's caller

@@ -126,5 +126,24 @@ def test_slots_budget_ticks_and_errors():
         with pytest.raises(RuntimeError):
             sv.open(np.zeros(101), 4)          # larger than the pool
         sv.close_session(c)
+        assert sv._lib.arc_server_request(sv._ptr, c, 1, None, 0, None, None, None) < 0  # closed
         with pytest.raises(RuntimeError):
-            sv.request(c, 1)                   # closed
+            sv.request(c, 1)
+
+
+def test_session_closed_before_admission_still_runs_its_requests():
+    """A client may close a session while it still waits for slots: its
+    queued requests run, then its slots are freed."""
+    with Server(64, config=CFG) as sv:
+        a = sv.open(np.zeros(60), 1)
+        ra = sv.request(a, 3)
+        b = sv.open(np.zeros(30), 2)           # waits: 4 slots left
+        rb = [sv.request(b, 2) for _ in range(2)]
+        sv.close_session(b)                    # closed before it was admitted
+        sv.wait(ra)
+        sv.close_session(a)
+        for r in rb:
+            (obs, rew, done), _ = sv.wait(r, timeout=60.0)
+            assert np.isfinite(obs).all() and rew.shape == (2, 30)
+        st = sv.stats()
+        assert st["error"] == 0 and st["completed"] == 3
