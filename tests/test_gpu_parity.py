@@ -17,7 +17,13 @@
    and of the restatement against the reference is printed (p50, p95, p99,
    max of each world's worst body), and the kernel's is bounded by the
    restatement's: FP32 arithmetic, not the kernel, sets how fast an FP32
-   rollout leaves the FP64 one. Two workloads: 64 worlds on flat terrain with
+   rollout leaves the FP64 one. The bound is 1.25x while the restatement
+   still follows the reference (its median error below 0.1, a tenth of the
+   body scale); once the median passes that, both FP32 rollouts have
+   decorrelated from the FP64 one (errors of the order of the robot itself,
+   e.g. medians of 0.66 and 0.84 after 100 uneven-terrain steps) and are two
+   samples of the same chaotic spread, whose percentiles over 256 worlds
+   agree to 1.5x. Two workloads: 64 worlds on flat terrain with
    seeds = world index and U[-1, 1] actions from seed 0 (the small plain
    configuration), and 256 worlds with difficulty U[0, 1] and per-joint
    Ornstein-Uhlenbeck actions (theta 0.15, sigma 0.3, clipped to [-1, 1],
@@ -34,6 +40,8 @@ from parity_checks import body_errors, classify_touch_mismatches, report_mismatc
 pytestmark = pytest.mark.gpu
 
 HORIZONS = (1, 5, 10, 30, 100)
+# median relative error past which an FP32 rollout no longer follows the FP64 one
+DECORRELATED = 0.1
 
 
 @pytest.mark.parametrize("kernel", [KERNEL_WARPS, KERNEL_LEGS])
@@ -130,9 +138,10 @@ def test_free_running_rollouts_against_horizon(name):
               f"orientation: kernel {fmt(kq)}   restatement {fmt(rq)}")
     for k, ((kx, kq), (rx, rq)) in table.items():
         for what, kern, rest in (("position", kx, rx), ("orientation", kq, rq)):
+            ratio = 1.25 if np.median(rest) < DECORRELATED else 1.5
             for p in (50, 95):
                 kv, rv = float(np.percentile(kern, p)), float(np.percentile(rest, p))
-                assert kv <= max(1.25 * rv, 2e-6), f"k={k} {what} p{p}: kernel {kv:.2e} vs restatement {rv:.2e}"
+                assert kv <= max(ratio * rv, 2e-6), f"k={k} {what} p{p}: kernel {kv:.2e} vs restatement {rv:.2e}"
     # one control step from the same state stays at FP32 resolution
     (kx, kq), _ = table[1]
     assert np.percentile(kx, 95) <= 1e-5 and np.percentile(kq, 95) <= 1e-5
