@@ -33,15 +33,13 @@ INCLUDE = HERE.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills", f"-I{INCLUDE}", f"-I{CSRC}"]
-# per-file flags: the warp-per-leg FP32 step divides and takes square roots
-# with the full-range approximate instructions (at most 2 ulp), whose errors
-# are far below the FP32 parity bounds its tests hold it to, and flushes
-# denormals to zero (no fix-up code for them: 3% less code and time)
-FILE_FLAGS = {"arc_step_warps.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
-              # the task layer runs the same warp-per-leg step inside its fused
-              # control-step kernel: the same flags, so the two give the same
-              # worlds (its own arithmetic is FP64, which they do not touch)
-              "arc_task.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
+# per-file flags: the warp-per-leg FP32 step (arc_step_warps.cuh, compiled
+# into arc_task.cu's control-step kernel) divides and takes square roots with
+# the full-range approximate instructions (at most 2 ulp), whose errors are
+# far below the FP32 parity bounds its tests hold it to, and flushes denormals
+# to zero (no fix-up code for them: 3% less code and time); the task layer's
+# own arithmetic there is FP64, which these flags do not touch
+FILE_FLAGS = {"arc_task.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
               # the renderer: the same, for code size (its output is 8-bit colour)
               "arc_render.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]}
 

