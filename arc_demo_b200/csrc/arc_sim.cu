@@ -63,6 +63,7 @@ struct arc_sim {
     int* queue = nullptr;        // work queue of the warp-per-leg kernel (two ints)
     bool use_queue = false;
     int fused = 0;  // env control step: 0 separate kernels, 1 fused step and task, 2 and resets (arc_env_set_fused)
+    int step_order = 1;  // env step: 0 index order, 1 each range by difficulty band (arc_env_set_step_order)
     void* lastc = nullptr;     // [n][kMaxContacts][kContactRec] R: the last substep's contacts (recording on)
     int* lastn = nullptr;      // [n] their counts
     int substep_tile = 0;      // warp-per-leg step: substeps per launch (0: the whole control step)
@@ -88,11 +89,14 @@ struct arc_sim {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t graph_stream = nullptr;
-    int graph_kernel = -1, graph_wpc = -1, graph_queue = -1, graph_fused = -1, graph_tile = -1;  // the captured form
+    int graph_kernel = -1, graph_wpc = -1, graph_queue = -1, graph_fused = -1, graph_tile = -1,
+        graph_order = -1;  // the captured form
     void* graph_lastc = nullptr;
     // arc_env_step_host: world indices 0..n-1, per-chunk ended-world lists and
     // counts, the two copy streams and their events
     int* iota = nullptr;
+    int* order = nullptr;         // the step kernels' world order (k_order_count, k_order_place)
+    int* order_counts = nullptr;  // [chunks][bands] worlds per band of each chunk of the order kernels
     int* chunk_done = nullptr;
     int* chunk_count = nullptr;
     int* part_queue = nullptr;  // arc_env_step_part: a work queue (two ints) per part
@@ -276,7 +280,7 @@ void free_all(arc_sim* s)
     for (void* p : s->env_allocs)
         cudaFree(p);
     void* ps[] = {s->rec, s->sph, s->unstable, s->time, s->th, s->toff, s->tg, s->tgd, s->grid_of, s->spill, s->queue,
-                  s->st_in.p, s->st_in2.p, s->st_in3.p, s->st_out.p, s->iota, s->chunk_done, s->chunk_count,
+                  s->st_in.p, s->st_in2.p, s->st_in3.p, s->st_out.p, s->iota, s->order, s->order_counts, s->chunk_done, s->chunk_count,
                   s->part_queue, s->tile_q, s->lastc, s->lastn};
     for (void* p : ps)
         if (p)
@@ -1305,6 +1309,14 @@ int arc_env_set_fused(arc_sim* s, int mode)
     return ARC_OK;
 }
 
+int arc_env_set_step_order(arc_sim* s, int mode)
+{
+    if (mode < 0 || mode > 1)
+        return fail(s, ARC_ERR_ARG, "arc_env_set_step_order: mode 0 or 1");
+    s->step_order = mode;
+    return ARC_OK;
+}
+
 int arc_device_checks(unsigned long long* failures, int* first_site, long long* first_index, int clear)
 {
     unsigned long long total = 0;
@@ -1496,12 +1508,24 @@ int env_control_step(arc_sim* s, const float* actions, const TaskOut& O, const i
 }
 
 // the whole control step of ArcVecEnv.step_wait, as launched into `st`
+int ensure_step_host(arc_sim* s);
+bool order_applies(const arc_sim* s);
+const int* range_ids(arc_sim* s, int first, int count, cudaStream_t st, int slot);
+
 int env_step_launches(arc_sim* s, const float* actions, cudaStream_t st)
 {
+    // the worlds in the step order, or all worlds in index order (NULL)
+    const int* ids = nullptr;
+    if (order_applies(s)) {
+        if (int rc = ensure_step_host(s))
+            return rc;
+        if (!(ids = range_ids(s, 0, s->n, st, 0)))
+            return ARC_ERR_CUDA;
+    }
     if (fused_applies(s))
-        return env_control_step(s, actions, s->to, nullptr, s->n, s->use_queue ? s->queue : nullptr, st);
+        return env_control_step(s, actions, s->to, ids, s->n, s->use_queue ? s->queue : nullptr, st);
     Actuation A{nullptr, actions};
-    int rc = step_any(s, A, st);
+    int rc = step_any(s, A, st, ids, s->n);
     if (rc)
         return rc;
     rc = s->fp64 ? env_task_step<double>(s, actions, true, st) : env_task_step<float>(s, actions, true, st);
@@ -1511,6 +1535,21 @@ int env_step_launches(arc_sim* s, const float* actions, cudaStream_t st)
 }
 
 constexpr int kMaxChunks = 16;
+
+// The step kernels' world order (arc_env_set_step_order): the worlds of a
+// range by difficulty band, hardest first, and by world index within a band.
+// The groups of 32 worlds that the work queue hands out first are then the
+// costliest, and the last, which run while the SMs empty, the cheapest
+// (longest first). A world's results do not depend on which others share its
+// CTA or when it runs, so any order gives the same worlds bit for bit.
+constexpr int kOrderChunk = 1024;  // worlds per CTA of the two order kernels
+constexpr int kOrderBands = 16;
+
+__device__ __forceinline__ int difficulty_band(const double* __restrict__ difficulty, int w)
+{
+    const double d = difficulty[w];
+    return d >= 1.0 ? kOrderBands - 1 : (d > 0.0 ? (int)(d * kOrderBands) : 0);  // NaN: band 0
+}
 
 // World ranges of arc_env_step_host: range c is first[c] .. first[c + 1] - 1.
 struct Ranges {
@@ -1572,6 +1611,87 @@ __global__ void k_merge_done(const int* __restrict__ chunk_done, const int* __re
     }
 }
 
+// The step order of worlds first .. first + count - 1, in two launches over
+// chunks of kOrderChunk worlds, one CTA each. k_order_count: each chunk's
+// worlds per band into counts[chunk][band].
+__global__ void __launch_bounds__(kOrderChunk) k_order_count(int* __restrict__ counts,
+                                                              const double* __restrict__ difficulty, int first,
+                                                              int count)
+{
+    __shared__ int c[kOrderBands];
+    const int t = threadIdx.x, i = blockIdx.x * kOrderChunk + t;
+    if (t < kOrderBands)
+        c[t] = 0;
+    __syncthreads();
+    if (i < count)
+        atomicAdd(&c[difficulty_band(difficulty, first + i)], 1);
+    __syncthreads();
+    if (t < kOrderBands)
+        counts[blockIdx.x * kOrderBands + t] = c[t];
+}
+
+// k_order_place: each chunk's worlds to their places in order[first ..]:
+// bands from the hardest, within a band the chunks in turn and each chunk's
+// worlds by index (a ballot and a warp scan per band).
+__global__ void __launch_bounds__(kOrderChunk) k_order_place(int* __restrict__ order, const int* __restrict__ counts,
+                                                              const double* __restrict__ difficulty, int first,
+                                                              int count)
+{
+    __shared__ int total[kOrderBands], prior[kOrderBands];  // a band's worlds: all, in the chunks before
+    __shared__ int base[kOrderBands];         // where this chunk's worlds of each band start
+    __shared__ int before[kOrderChunk / 32];  // worlds of the band in the warps before
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, chunk = blockIdx.x, i = chunk * kOrderChunk + t;
+    if (warp < kOrderBands) {  // warp b sums band b over the chunks
+        int all = 0, mine = 0;
+        for (int k = lane; k < (int)gridDim.x; k += 32) {
+            const int v = counts[k * kOrderBands + warp];
+            all += v;
+            mine += k < chunk ? v : 0;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            all += __shfl_xor_sync(0xffffffffu, all, o);
+            mine += __shfl_xor_sync(0xffffffffu, mine, o);
+        }
+        if (lane == 0) {
+            total[warp] = all;
+            prior[warp] = mine;
+        }
+    }
+    const int band = i < count ? difficulty_band(difficulty, first + i) : -1;
+    __syncthreads();
+    if (t == 0) {
+        int at = 0;
+        for (int b = kOrderBands - 1; b >= 0; --b) {
+            base[b] = at + prior[b];
+            at += total[b];
+        }
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int b = kOrderBands - 1; b >= 0; --b) {
+        const unsigned m = __ballot_sync(0xffffffffu, band == b);
+        if (lane == 0)
+            before[warp] = __popc(m);
+        __syncthreads();
+        if (warp == 0) {
+            const int c = before[lane];
+            int x = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o)
+                    x += y;
+            }
+            before[lane] = x - c;
+        }
+        __syncthreads();
+        if (band == b)
+            order[first + base[b] + before[warp] + __popc(m & ((1u << lane) - 1u))] = first + i;
+        __syncthreads();
+    }
+}
+
 __global__ void k_iota(int* __restrict__ out, int n)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1585,7 +1705,8 @@ int ensure_step_host(arc_sim* s)
         return ARC_OK;
     // everything is made into locals and handed to s only once all of it
     // exists, so a failure part way leaves s as it was and leaks nothing
-    int *iota = nullptr, *chunk_done = nullptr, *chunk_count = nullptr, *part_queue = nullptr;
+    int *iota = nullptr, *order = nullptr, *order_counts = nullptr, *chunk_done = nullptr, *chunk_count = nullptr,
+        *part_queue = nullptr;
     cudaStream_t copy_in = nullptr, copy_out = nullptr;
     constexpr int kEvents = (int)(sizeof(s->ev) / sizeof(s->ev[0]));
     cudaEvent_t ev[kEvents] = {};
@@ -1596,16 +1717,20 @@ int ensure_step_host(arc_sim* s)
         for (cudaStream_t c : {copy_in, copy_out})
             if (c)
                 cudaStreamDestroy(c);
-        for (int* p : {iota, chunk_done, chunk_count, part_queue})
+        for (int* p : {iota, order, order_counts, chunk_done, chunk_count, part_queue})
             cudaFree(p);
         return ARC_ERR_CUDA;
     };
     if (check(s, cudaMalloc((void**)&chunk_done, sizeof(int) * s->n), "cudaMalloc(chunk lists)") ||
         check(s, cudaMalloc((void**)&chunk_count, sizeof(int) * kMaxChunks), "cudaMalloc(chunk counts)") ||
         check(s, cudaMalloc((void**)&part_queue, sizeof(int) * 2 * kMaxChunks), "cudaMalloc(part queues)") ||
-        check(s, cudaMalloc((void**)&iota, sizeof(int) * s->n), "cudaMalloc(world indices)"))
+        check(s, cudaMalloc((void**)&iota, sizeof(int) * s->n), "cudaMalloc(world indices)") ||
+        check(s, cudaMalloc((void**)&order, sizeof(int) * s->n), "cudaMalloc(step order)") ||
+        check(s, cudaMalloc((void**)&order_counts, sizeof(int) * kOrderBands * (s->n / kOrderChunk + 2 + kMaxChunks)),
+              "cudaMalloc(step order counts)"))
         return release();
     k_iota<<<(s->n + 255) / 256, 256, 0, s->stream>>>(iota, s->n);
+    k_iota<<<(s->n + 255) / 256, 256, 0, s->stream>>>(order, s->n);
     // ready before any stream uses them (arc_env_step_part runs on the caller's)
     if (check(s, cudaGetLastError(), "world indices") ||
         check(s, cudaMemsetAsync(part_queue, 0, sizeof(int) * 2 * kMaxChunks, s->stream), "zero part queues") ||
@@ -1623,8 +1748,38 @@ int ensure_step_host(arc_sim* s)
     s->copy_out = copy_out;
     for (int i = 0; i < kEvents; ++i)
         s->ev[i] = ev[i];
+    s->order = order;
+    s->order_counts = order_counts;
     s->iota = iota;
     return ARC_OK;
+}
+
+// Whether the env's step kernels take the step order: on, and a kernel that
+// steps lists of worlds as it steps whole batches (the leg-parallel kernel
+// steps whole batches only).
+bool order_applies(const arc_sim* s)
+{
+    return s->step_order && s->ts.difficulty && (s->kernel == ARC_KERNEL_WARPS || s->kernel == ARC_KERNEL_PLAIN);
+}
+
+// The world ids the step kernels take for worlds first .. first + count - 1:
+// the range's step order, made into `st` from the worlds' current
+// difficulty, when it applies; else the worlds in index order. NULL on a
+// launch error. Ranges that run side by side (the parts of
+// arc_env_step_part, slot = part, in world order) use disjoint parts of the
+// order and of its counts: range `slot` takes the chunks from its first
+// world's chunk + slot, which the next range's start cannot reach.
+const int* range_ids(arc_sim* s, int first, int count, cudaStream_t st, int slot)
+{
+    if (!order_applies(s) || count <= 0)
+        return s->iota + first;
+    const int chunks = (count + kOrderChunk - 1) / kOrderChunk;
+    int* counts = s->order_counts + (first / kOrderChunk + slot) * kOrderBands;
+    k_order_count<<<chunks, kOrderChunk, 0, st>>>(counts, s->ts.difficulty, first, count);
+    k_order_place<<<chunks, kOrderChunk, 0, st>>>(s->order, counts, s->ts.difficulty, first, count);
+    if (check(s, cudaGetLastError(), "step order kernels"))
+        return nullptr;
+    return s->order + first;
 }
 
 // One control step of worlds first .. first + count - 1 into `st`, their
@@ -1635,12 +1790,15 @@ template <class R> int env_step_chunk(arc_sim* s, int first, int count, int c, c
     TaskOut O = s->to;
     O.done_list = s->chunk_done + first;
     O.done_count = s->chunk_count + c;
+    const int* ids = range_ids(s, first, count, st, part >= 0 ? part : c);
+    if (!ids)
+        return ARC_ERR_CUDA;
     if (fused_applies(s)) {
         int* queue = !s->use_queue ? nullptr : (part >= 0 ? s->part_queue + 2 * part : s->queue);
-        return env_control_step(s, s->actions, O, s->iota + first, count, queue, st);
+        return env_control_step(s, s->actions, O, ids, count, queue, st);
     }
     Actuation A{nullptr, s->actions};
-    if (int rc = step_any(s, A, st, s->iota + first, count, part))
+    if (int rc = step_any(s, A, st, ids, count, part))
         return rc;
     if (check(s, launch_task_step<R>(dev_model<R>(s), view<R>(s), s->tp, s->ts, O, s->actions, 2, st, first, count),
               "task step kernel") ||
@@ -1747,6 +1905,21 @@ int arc_env_step_part(arc_sim* s, int part, int parts, void* stream)
         return ARC_ERR_CUDA;
     return s->fp64 ? env_step_chunk<double>(s, first, count, part, st, part)
                    : env_step_chunk<float>(s, first, count, part, st, part);
+}
+
+int arc_env_get_step_order(arc_sim* s, int* order)
+{
+    if (int rc = env_check(s))
+        return rc;
+    if (!order)
+        return fail(s, ARC_ERR_ARG, "arc_env_get_step_order: NULL order");
+    if (int rc = ensure_step_host(s))
+        return rc;
+    const int* ids = order_applies(s) ? range_ids(s, 0, s->n, s->stream, 0) : s->iota;
+    if (!ids ||
+        check(s, cudaMemcpyAsync(order, ids, sizeof(int) * s->n, cudaMemcpyDeviceToHost, s->stream), "step order"))
+        return ARC_ERR_CUDA;
+    return sync(s, "step order");
 }
 
 int arc_env_merge_parts(arc_sim* s, int parts, void* stream)
@@ -1979,7 +2152,8 @@ int arc_env_step(arc_sim* s, const float* d_actions, void* stream)
     // graph of the whole control step over the ARC_ENV_ACTIONS buffer
     if (s->graph_exec && (s->graph_kernel != s->kernel || s->graph_wpc != s->wpc ||
                           s->graph_queue != (int)s->use_queue || s->graph_fused != s->fused ||
-                          s->graph_tile != s->substep_tile || s->graph_lastc != s->lastc)) {
+                          s->graph_tile != s->substep_tile || s->graph_lastc != s->lastc ||
+                          s->graph_order != s->step_order)) {
         cudaGraphExecDestroy(s->graph_exec);
         cudaGraphDestroy(s->graph);
         s->graph_exec = nullptr;
@@ -2010,6 +2184,7 @@ int arc_env_step(arc_sim* s, const float* d_actions, void* stream)
         s->graph_fused = s->fused;
         s->graph_tile = s->substep_tile;
         s->graph_lastc = s->lastc;
+        s->graph_order = s->step_order;
         return ARC_OK;
     }
     return check(s, cudaGraphLaunch(s->graph_exec, st), "graph launch");

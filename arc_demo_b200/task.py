@@ -109,6 +109,8 @@ def env_lib() -> ctypes.CDLL:
     d("arc_env_reset", _int, _vp, _vp, _int, _vp)
     d("arc_env_step", _int, _vp, _vp, _vp)
     d("arc_env_set_fused", _int, _vp, _int)
+    d("arc_env_set_step_order", _int, _vp, _int)
+    d("arc_env_get_step_order", _int, _vp, _vp)
     d("arc_env_step_host", _int, _vp, _vp, _vp, _vp, _vp, _vp, _int)
     d("arc_env_part_range", _int, _vp, _int, _int, ctypes.POINTER(_int), ctypes.POINTER(_int))
     d("arc_env_step_part", _int, _vp, _int, _int, _vp)

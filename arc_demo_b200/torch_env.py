@@ -71,6 +71,20 @@ class DeviceVecEnv:
         launch per control step). The results are the same bit for bit."""
         self.sim._check(self.gpu.lib.arc_env_set_fused(self.sim.ptr, int(mode)))
 
+    def set_step_order(self, mode: int) -> None:
+        """1 (the default): the step kernels take each range's worlds by
+        difficulty band, hardest first; 0: in index order. The results are
+        the same bit for bit."""
+        self.sim._check(self.gpu.lib.arc_env_set_step_order(self.sim.ptr, int(mode)))
+
+    def step_order(self):
+        """The order (numpy int32 permutation) a whole control step hands the
+        step kernels now."""
+        import numpy as np
+        out = np.empty(self.num_envs, dtype=np.int32)
+        self.sim._check(self.gpu.lib.arc_env_get_step_order(self.sim.ptr, out.ctypes.data))
+        return out
+
     def set_levels(self, levels) -> None:
         """Per-world terrain difficulty levels (the curriculum state)."""
         import numpy as np

@@ -47,9 +47,9 @@ HBM_BYTES_PER_ENV_STEP = 3.9e3  # algorithmic HBM traffic of one env-step (state
 LAT_STEPS = 300  # control steps of the step-latency sample
 # DRAM bytes (read + write) one world costs a launch of the warp-per-leg step
 # kernel: ncu's dram__bytes_read.sum + dram__bytes_write.sum over a
-# 16,384-world launch (42.24 MB + 0.17 MB), divided by the worlds; each world
+# 16,384-world launch (42.19 MB + 3.68 MB), divided by the worlds; each world
 # reads its own record and terrain cells, so the traffic scales with them.
-WARPS_DRAM_BYTES_PER_WORLD = (42.240e6 + 0.175e6) / 16384
+WARPS_DRAM_BYTES_PER_WORLD = (42.195e6 + 3.681e6) / 16384
 
 # the renderer's workload: frames of the reference's rgb_array size
 # (arc/env.py:43), 4 rays per pixel, for a batch of worlds per launch
@@ -395,11 +395,21 @@ def run_ours(args) -> dict | None:
         lib, ptr = env.sim._lib, env.sim.ptr
         a = ctypes.c_void_p(env.actions.data_ptr())
         st = ctypes.c_void_p(stream.cuda_stream)
+        # the worlds in the order the env's step hands them to the kernels
+        # (by difficulty band, hardest first), which both kernels are timed in
+        order = torch.from_numpy(env.step_order()).to("cuda")
+        ids = ctypes.c_void_p(order.data_ptr())
+
+        def step_kernel():
+            if env.sim.kernel()[0] in (KERNEL_WARPS, KERNEL_PLAIN):
+                lib.arc_sim_step_ids(ptr, ids, n, None, a, st)
+            else:  # the leg-parallel kernel steps whole batches, in index order
+                lib.arc_sim_step_actions(ptr, a, st)
         M = 10
         k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         k0.record(stream)
         for _ in range(M):
-            lib.arc_sim_step_actions(ptr, a, st)
+            step_kernel()
         k1.record(stream)
         k1.synchronize()
         step_kernel_ms = k0.elapsed_time(k1) / M
@@ -421,7 +431,7 @@ def run_ours(args) -> dict | None:
             q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             q0.record(stream)
             for _ in range(3):
-                lib.arc_sim_step_actions(ptr, a, st)
+                step_kernel()
             q1.record(stream)
             q1.synchronize()
             plain_kernel_ms = q0.elapsed_time(q1) / 3
@@ -484,6 +494,7 @@ def run_ours(args) -> dict | None:
                    "autotune_step_kernel_ms": tune,
                    "parts": parts,
                    "control_step": FORMS[form],
+                   "step_order": "each range's worlds by difficulty band, hardest first (arc_env_set_step_order)",
                    "autotune_control_step_ms": parts_tune,
                    "loop": ("policy then env.step() (one CUDA graph) per control step" if parts == 1 else
                             f"policy and step of {parts} world ranges, each on its own stream "

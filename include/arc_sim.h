@@ -316,6 +316,20 @@ int arc_env_step_ids(arc_sim *s, const int *d_ids, int n_ids, void *stream);
  * launch per control step). All three give the same results bit for bit. */
 int arc_env_set_fused(arc_sim *s, int mode);
 
+/* The order in which the env's control step hands worlds to the step
+ * kernels (warp-per-leg and plain): 1 (the default) the worlds of each
+ * range stepped (all worlds, a part of arc_env_step_part, a chunk of
+ * arc_env_step_host) by difficulty band (16 bands, hardest first; by index
+ * within a band), made from the current difficulties every step, so that
+ * the costliest groups of 32 worlds go first and the cheapest run while the
+ * GPU empties; 0 index order. A world's results do not depend on the order:
+ * both modes give the same worlds bit for bit. */
+int arc_env_set_step_order(arc_sim *s, int mode);
+
+/* The order (N world indices, a permutation) that a whole control step
+ * hands the step kernels now; synchronous. */
+int arc_env_get_step_order(arc_sim *s, int *order);
+
 /*
  * The same control step with host buffers, as ArcVecEnv.step_wait's caller
  * sees it (arc/env.py:99-117): h_actions (N x 12 float32) in; observations
