@@ -1632,14 +1632,15 @@ __global__ void __launch_bounds__(kOrderChunk) k_order_count(int* __restrict__ c
 
 // k_order_place: each chunk's worlds to their places in order[first ..]:
 // bands from the hardest, within a band the chunks in turn and each chunk's
-// worlds by index (a ballot and a warp scan per band).
+// worlds by index (per band: a ballot per warp, then a scan over the warps).
 __global__ void __launch_bounds__(kOrderChunk) k_order_place(int* __restrict__ order, const int* __restrict__ counts,
                                                               const double* __restrict__ difficulty, int first,
                                                               int count)
 {
+    constexpr int kWarpsPerChunk = kOrderChunk / 32;
     __shared__ int total[kOrderBands], prior[kOrderBands];  // a band's worlds: all, in the chunks before
-    __shared__ int base[kOrderBands];         // where this chunk's worlds of each band start
-    __shared__ int before[kOrderChunk / 32];  // worlds of the band in the warps before
+    __shared__ int base[kOrderBands];                      // where this chunk's worlds of each band start
+    __shared__ int before[kWarpsPerChunk][kOrderBands + 1];  // a band's worlds in a warp, then in the warps before
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5, chunk = blockIdx.x, i = chunk * kOrderChunk + t;
     if (warp < kOrderBands) {  // warp b sums band b over the chunks
         int all = 0, mine = 0;
@@ -1659,6 +1660,15 @@ __global__ void __launch_bounds__(kOrderChunk) k_order_place(int* __restrict__ o
         }
     }
     const int band = i < count ? difficulty_band(difficulty, first + i) : -1;
+    unsigned same = 0;  // the lanes of this warp in this thread's band
+#pragma unroll
+    for (int b = 0; b < kOrderBands; ++b) {
+        const unsigned m = __ballot_sync(0xffffffffu, band == b);
+        if (lane == b)
+            before[warp][b] = __popc(m);
+        if (band == b)
+            same = m;
+    }
     __syncthreads();
     if (t == 0) {
         int at = 0;
@@ -1667,29 +1677,20 @@ __global__ void __launch_bounds__(kOrderChunk) k_order_place(int* __restrict__ o
             at += total[b];
         }
     }
-    __syncthreads();
-#pragma unroll 1
-    for (int b = kOrderBands - 1; b >= 0; --b) {
-        const unsigned m = __ballot_sync(0xffffffffu, band == b);
-        if (lane == 0)
-            before[warp] = __popc(m);
-        __syncthreads();
-        if (warp == 0) {
-            const int c = before[lane];
-            int x = c;
+    if (warp < kOrderBands) {  // warp b: band b's exclusive scan over the chunk's warps
+        const int c = before[lane][warp];
+        int x = c;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o)
-                    x += y;
-            }
-            before[lane] = x - c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o)
+                x += y;
         }
-        __syncthreads();
-        if (band == b)
-            order[first + base[b] + before[warp] + __popc(m & ((1u << lane) - 1u))] = first + i;
-        __syncthreads();
+        before[lane][warp] = x - c;
     }
+    __syncthreads();
+    if (band >= 0)
+        order[first + base[band] + before[warp][band] + __popc(same & ((1u << lane) - 1u))] = first + i;
 }
 
 __global__ void k_iota(int* __restrict__ out, int n)
