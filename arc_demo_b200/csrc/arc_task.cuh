@@ -99,8 +99,8 @@ cudaError_t launch_task_reset(const DevModel<R>& M, const ResetModel& RM, const 
 // zero before the launch. Without resets the ended worlds are only listed
 // (O.done_list), for launch_task_reset. The results equal launch_step_warps,
 // launch_task_step (write_obs 2), launch_task_heights and launch_task_reset
-// over O.done_list in turn, bit for bit: the same kernel runs the physics in
-// every form, and the task functions are compiled once.
+// over O.done_list in turn to FP32 rounding: the task functions are compiled
+// once, and the physics is the same source compiled into this form's kernel.
 cudaError_t launch_control_step(const DevModel<float>& M, const ResetModel& RM, const Worlds<float>& W,
                                 TerrainGeom<float>* tg, TerrainGeomD* tgd, const int* grid_of, double cell,
                                 const TaskParams& P, const TaskState& S, const TaskOut& O, const float* actions,

@@ -68,7 +68,8 @@ class DeviceVecEnv:
         """With the warp-per-leg kernel: 0 the step kernel, then the task,
         heights and reset kernels; 1 the step and the task layer fused per
         group of 32 worlds, the resets after; 2 the resets fused too (one
-        launch per control step). The results are the same bit for bit."""
+        launch per control step). Forms 1 and 2 agree with form 0 to FP32
+        rounding (their physics is compiled into their own kernel)."""
         self.sim._check(self.gpu.lib.arc_env_set_fused(self.sim.ptr, int(mode)))
 
     def set_step_order(self, mode: int) -> None:

@@ -313,7 +313,10 @@ int arc_env_step_ids(arc_sim *s, const int *d_ids, int n_ids, void *stream);
  * 1 each group of 32 worlds stepped and then given its rewards,
  * observations and heights in the same kernel, the ended worlds reset by the
  * reset kernel after it; 2 the ended worlds reset in that kernel too (one
- * launch per control step). All three give the same results bit for bit. */
+ * launch per control step). The task layer's results are the same in all
+ * three; the physics of forms 1 and 2 is compiled into their own kernel and
+ * agrees with form 0's to FP32 rounding (form 0, the fastest, keeps the
+ * task code out of the step kernel). */
 int arc_env_set_fused(arc_sim *s, int mode);
 
 /* The order in which the env's control step hands worlds to the step
