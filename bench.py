@@ -47,9 +47,9 @@ HBM_BYTES_PER_ENV_STEP = 3.9e3  # algorithmic HBM traffic of one env-step (state
 LAT_STEPS = 300  # control steps of the step-latency sample
 # DRAM bytes (read + write) one world costs a launch of the warp-per-leg step
 # kernel: ncu's dram__bytes_read.sum + dram__bytes_write.sum over a
-# 16,384-world launch (42.19 MB + 3.68 MB), divided by the worlds; each world
+# 16,384-world launch (42.24 MB + 0.00 MB), divided by the worlds; each world
 # reads its own record and terrain cells, so the traffic scales with them.
-WARPS_DRAM_BYTES_PER_WORLD = (42.195e6 + 3.681e6) / 16384
+WARPS_DRAM_BYTES_PER_WORLD = (42.242e6 + 192.0) / 16384
 
 # the renderer's workload: frames of the reference's rgb_array size
 # (arc/env.py:43), 4 rays per pixel, for a batch of worlds per launch
