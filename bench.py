@@ -488,11 +488,12 @@ def run_ours(args) -> dict | None:
                    (f", {cand[4:]} substeps per launch" if cand.startswith("tile") else "")
                    if cand.startswith(("warps", "tile")) else "leg-parallel")
     form = form if cand.startswith("warps") else 0  # the fused forms need the warp-per-leg kernel
-    # our launches per control step and range: the step, task, heights and
-    # reset kernels (form 0), the fused step and the reset kernel (1), the
-    # fused step alone (2); the ranges' merge; the memset of the ended-world
-    # count is not a kernel
-    per_part = {0: 4, 1: 2, 2: 1}[form]
+    # our launches per control step and range: the step order's two kernels
+    # (with the warp-per-leg kernel), then the step, task, heights and reset
+    # kernels (form 0), the fused step and the reset kernel (1), the fused
+    # step alone (2); the ranges' merge; the memset of the ended-world count
+    # is not a kernel
+    per_part = {0: 4, 1: 2, 2: 1}[form] + (2 if cand.startswith(("warps", "tile")) else 0)
     launches = (per_part * parts + (1 if parts > 1 else 0)) * K
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "env-steps/s", "n_gpus": world, "steps": K,
