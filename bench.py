@@ -247,10 +247,10 @@ FORMS = {0: "step kernel, then task, heights and reset kernels",
 
 
 def autotune_parts(env, torch, stream, one_step,
-                   candidates=((1, 0), (1, 1), (1, 2), (2, 0), (2, 1), (4, 0), (4, 1)), steps=6):
+                   candidates=((1, 0), (1, 1), (1, 2), (2, 0), (2, 1), (4, 0), (4, 1), (8, 0)), steps=6):
     """How the control step runs, by timing whole control steps (policy
     included), each candidate from the same world and task states: (ranges,
-    form). Ranges 1: the policy, then env.step() as one CUDA graph; 2, 4: the
+    form). Ranges 1: the policy, then env.step() as one CUDA graph; 2, 4, 8: the
     worlds in that many ranges on their own streams (DeviceVecEnv.step_parts),
     each range's policy then its step. Forms (DeviceVecEnv.set_fused): 0 the
     step kernel, then the task, heights and reset kernels; 1 the step and the
