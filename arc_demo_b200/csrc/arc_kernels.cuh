@@ -66,6 +66,11 @@ template <class R> size_t fast_smem_bytes(int stride, int worlds_per_cta);
 cudaError_t launch_step_warps(const DevModel<float>& M, const Worlds<float>& W, const Actuation& A, float* spill,
                               int spill_per_lane, int lane_cap, const int* ids, int n_items, int* queue,
                               cudaStream_t stream, int tile = 0, float* tile_q = nullptr);
+// The same step in FP64 (arc_step_warps64.cu): two CTAs per SM (its bodies
+// take twice the shared memory), the whole control step in one launch.
+cudaError_t launch_step_warps64(const DevModel<double>& M, const Worlds<double>& W, const Actuation& A,
+                                double* spill, int spill_per_lane, int lane_cap, const int* ids, int n_items,
+                                int* queue, cudaStream_t stream);
 constexpr int kFastOnChipContacts = 2;
 constexpr int kWarpsOnChipContacts = 1;  // keeps four CTAs of the warp-per-leg kernel per SM
 // the fewest on-chip records of any kernel: a spill area of lane_cap minus

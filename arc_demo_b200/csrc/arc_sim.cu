@@ -580,17 +580,23 @@ template <class R> const DevModel<R>& dev_model(const arc_sim* s);
 template <> const DevModel<float>& dev_model<float>(const arc_sim* s) { return s->mf; }
 template <> const DevModel<double>& dev_model<double>(const arc_sim* s) { return s->md; }
 
-template <class R> cudaError_t launch_warps_if_fp32(arc_sim*, const DevModel<R>&, const Worlds<R>&, const Actuation&,
-                                                   const int*, int, int*, cudaStream_t)
-{
-    return cudaErrorNotSupported;
-}
-template <> cudaError_t launch_warps_if_fp32<float>(arc_sim* s, const DevModel<float>& M, const Worlds<float>& W,
-                                                    const Actuation& A, const int* ids, int n_items, int* queue,
-                                                    cudaStream_t st)
+// the warp-per-leg step in the sim's precision (FP64: the whole control
+// step in one launch; substep tiles are FP32 only)
+template <class R> cudaError_t launch_warps(arc_sim*, const DevModel<R>&, const Worlds<R>&, const Actuation&,
+                                           const int*, int, int*, cudaStream_t);
+template <> cudaError_t launch_warps<float>(arc_sim* s, const DevModel<float>& M, const Worlds<float>& W,
+                                            const Actuation& A, const int* ids, int n_items, int* queue,
+                                            cudaStream_t st)
 {
     return launch_step_warps(M, W, A, static_cast<float*>(s->spill), s->spill_per_lane, s->lane_cap, ids, n_items,
                              queue, st, s->substep_tile, s->tile_q);
+}
+template <> cudaError_t launch_warps<double>(arc_sim* s, const DevModel<double>& M, const Worlds<double>& W,
+                                             const Actuation& A, const int* ids, int n_items, int* queue,
+                                             cudaStream_t st)
+{
+    return launch_step_warps64(M, W, A, static_cast<double*>(s->spill), s->spill_per_lane, s->lane_cap, ids,
+                               n_items, queue, st);
 }
 
 // ids: device list of n_ids distinct worlds to step (NULL: all worlds).
@@ -604,10 +610,10 @@ template <class R> int step_impl(arc_sim* s, const Actuation& A, cudaStream_t st
     const Worlds<R> W = view<R>(s);
     const DevModel<R>& M = dev_model<R>(s);
     const int n_items = ids ? n_ids : s->n;
-    const bool warps_ok = !s->fp64 && M.leaper && s->substeps <= kFastMaxSubsteps;
+    const bool warps_ok = M.leaper && s->substeps <= kFastMaxSubsteps;
     cudaError_t e;
     if (warps_ok && (s->kernel == ARC_KERNEL_WARPS || (ids && s->kernel == ARC_KERNEL_LEGS)))
-        e = launch_warps_if_fp32<R>(s, M, W, A, ids, n_items, queue, st);
+        e = launch_warps<R>(s, M, W, A, ids, n_items, queue, st);
     else if (!ids && s->kernel == ARC_KERNEL_LEGS && M.leaper && s->substeps <= kFastMaxSubsteps)
         e = launch_step_fast<R>(M, W, A, static_cast<R*>(s->spill), s->spill_per_lane, s->lane_cap, s->wpc, st);
     else
@@ -977,8 +983,8 @@ int arc_sim_set_kernel(arc_sim* s, int kernel, int worlds_per_cta)
             return fail(s, ARC_ERR_UNSUPPORTED, "worlds_per_cta needs more than 227 KB of shared memory");
         s->wpc = worlds_per_cta;
     } else if (kernel == ARC_KERNEL_WARPS) {
-        if (!s->model.leaper || s->fp64)
-            return fail(s, ARC_ERR_UNSUPPORTED, "warp-per-leg kernel needs the quadruped in FP32");
+        if (!s->model.leaper)
+            return fail(s, ARC_ERR_UNSUPPORTED, "warp-per-leg kernel needs the quadruped's topology");
     } else if (kernel != ARC_KERNEL_PLAIN) {
         return fail(s, ARC_ERR_ARG, "unknown kernel");
     }

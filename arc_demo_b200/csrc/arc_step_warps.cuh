@@ -49,7 +49,13 @@ constexpr int kWorlds = 32; // one per lane
 constexpr int kThreads = kWarps * kWorlds;
 constexpr int kOnChip = kWarpsOnChipContacts;
 
+// the precision of the step: FP32 (arc_task.cu's control-step kernel) or,
+// where the including file defines ARC_WARPS_FP64, FP64 (arc_step_warps64.cu)
+#ifdef ARC_WARPS_FP64
+using F = double;
+#else
 using F = float;
+#endif
 using V = V3<F>;
 using Q = Q4<F>;
 using P = Pose<F>;

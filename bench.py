@@ -15,12 +15,12 @@ observations, resets; plus the policy forward that produces its actions.
 
 Prints one JSON line (rank 0). `value` is device-resident throughput: either
 the policy, then the step as one CUDA graph of the library's kernels, or the
-worlds in 2 or 4 ranges on their own streams, each range's policy then its
+worlds in 2, 4 or 8 ranges on their own streams, each range's policy then its
 step (DeviceVecEnv.step_parts), whichever a short timing picks; `e2e` is the
 same loop through the host-buffer API (actions copied
 in, observations/rewards/dones copied out every step). `--impl reference`
 times the reference's own CPU path (its csrc/ built by oracle/Makefile, run
-with OpenMP on every host core) plus the task layer, on a bounded sample.
+with OpenMP on every host core) plus the task layer, over all the worlds.
 """
 
 from __future__ import annotations
@@ -78,7 +78,7 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--kernel", choices=["auto", "warps"], default="auto")
     p.add_argument("--parts", type=int, default=0,
-                   help="policy + step in this many world ranges on their own streams (0: autotune over 1, 2, 4)")
+                   help="policy + step in this many world ranges on their own streams (0: autotune over 1, 2, 4, 8)")
     p.add_argument("--workload", choices=["step", "render"], default="step",
                    help="step: the world step (the headline); render: frames of the headless renderer")
     p.add_argument("--render-worlds", type=int, default=RENDER_WORLDS)
@@ -736,36 +736,59 @@ def leg_grid_sizes(torch, n=16384, steps=40, warmup=5) -> dict:
 
 def leg_fp64(torch, n, steps=6, warmup=3) -> dict:
     """The step in FP64 (the reference's precision) at the headline's world
-    count: the leg-parallel FP64 kernel, timed alone from settled states."""
+    count: the leg-parallel FP64 kernel at 8 and 16 worlds per CTA and the
+    FP64 warp-per-leg kernel (one CTA per group, work queue), each timed alone
+    from the same settled states; then the control step with the fastest."""
     import ctypes
-    from arc_demo_b200.native import KERNEL_LEGS
+    from arc_demo_b200.native import KERNEL_LEGS, KERNEL_WARPS
     from arc_demo_b200.task import TaskConfig
     from arc_demo_b200.torch_env import DeviceVecEnv
     env = DeviceVecEnv(n, TaskConfig(curriculum=False), seed=3, fp64=True)
     env.set_levels(levels_for(n, 17))
     stream = torch.cuda.Stream()
+    names = {"legs8": "leg-parallel FP64, 8 worlds per CTA", "legs16": "leg-parallel FP64, 16 worlds per CTA",
+             "warps": "warp-per-leg FP64", "warps+queue": "warp-per-leg FP64, work queue"}
+
+    def apply(cand):
+        env.sim.set_work_queue(cand == "warps+queue")
+        if cand.startswith("legs"):
+            env.set_kernel(KERNEL_LEGS, int(cand[4:]))
+        else:
+            env.set_kernel(KERNEL_WARPS)
     with torch.cuda.stream(stream):
         env.reset()
-        best = None
-        for wpc in (8, 16):
-            env.set_kernel(KERNEL_LEGS, wpc)
-            torch.nn.init.uniform_(env.actions, -1.0, 1.0)
-            for _ in range(warmup):
-                env.step()
-            lib, ptr = env.sim._lib, env.sim.ptr
-            a, h = ctypes.c_void_p(env.actions.data_ptr()), ctypes.c_void_p(stream.cuda_stream)
+        torch.nn.init.uniform_(env.actions, -1.0, 1.0)
+        apply("legs8")
+        for _ in range(warmup):
+            env.step()
+        stream.synchronize()
+        start, tstart = env.sim.get_state(), env.gpu.get_state()
+        lib, ptr = env.sim._lib, env.sim.ptr
+        a, h = ctypes.c_void_p(env.actions.data_ptr()), ctypes.c_void_p(stream.cuda_stream)
+        table = {}
+        for cand in names:
+            env.sim.set_state(start)
+            torch.cuda.synchronize()
+            apply(cand)
+            lib.arc_sim_step_actions(ptr, a, h)  # first launch: per-device set-up
+            env.sim.set_state(start)
+            torch.cuda.synchronize()
             ms, _ = timed_loop(torch, stream, lambda: lib.arc_sim_step_actions(ptr, a, h), steps)
-            if best is None or ms < best[1]:
-                best = (wpc, ms)
-        wpc, ms = best
-        env.set_kernel(KERNEL_LEGS, wpc)
+            table[cand] = round(ms / steps, 4)
+        best = min(table, key=table.get)
+        env.sim.set_state(start)
+        env.gpu.set_state(tstart)
+        torch.cuda.synchronize()
+        apply(best)
         step_ms, _ = timed_loop(torch, stream, lambda: env.step(), steps)
     env.close()
-    return {"worlds": n, "kernel": f"leg-parallel FP64, {wpc} worlds per CTA",
-            "step_kernel_ms": round(ms / steps, 4), "env_steps_per_s_step_kernel": round(n * steps / (ms * 1e-3), 1),
+    ms = table[best] * steps
+    return {"worlds": n, "kernel": names[best], "step_kernel_ms_by_kernel": table,
+            "step_kernel_ms": table[best], "env_steps_per_s_step_kernel": round(n * steps / (ms * 1e-3), 1),
             "control_step_ms": round(step_ms / steps, 4),
             "env_steps_per_s_control_step": round(n * steps / (step_ms * 1e-3), 1),
-            "note": "actions fixed (uniform random); control step = step, task, heights, reset in one graph"}
+            "note": "actions fixed (uniform random); every kernel from the same states 3 steps after a reset; "
+                    "control step = step, task, heights, reset in one graph"}
 
 
 def leg_serving(seconds=3.0, clients=8, rates=(200.0, 50.0), tick_cap=131072) -> dict:

@@ -104,7 +104,8 @@ const arc_world *arc_sim_world(const arc_sim *s, int i);
 /* kernels */
 #define ARC_KERNEL_PLAIN 0      /* one thread per world */
 #define ARC_KERNEL_LEGS 1       /* four lanes per world (one per leg), shared-memory staging */
-#define ARC_KERNEL_WARPS 2      /* FP32: four warps per 32 worlds (one warp per leg), state in shared memory */
+#define ARC_KERNEL_WARPS 2      /* four warps per 32 worlds (one warp per leg), state in shared memory;
+                                   FP32, and FP64 with two CTAs per SM and no substep tiles */
 
 arc_sim *arc_sim_create_ex(int n_worlds, double dt, int substeps, int grid, double cell, unsigned flags);
 
@@ -188,8 +189,8 @@ int arc_sim_synchronize(const arc_sim *s);
 /* Steps only the n_ids worlds d_ids[0..n_ids) (device ints, distinct; ids
  * outside 0..N-1 are skipped), with exactly one of d_targets (N x 12 FP64)
  * or d_actions (N x 12 FP32, as arc_sim_step_actions), read at the listed
- * rows only. FP32 quadruped batches use the warp-per-leg kernel, others the
- * plain one. */
+ * rows only. Quadruped batches use the warp-per-leg kernel (FP32 or FP64)
+ * unless the plain one is selected, other models the plain one. */
 int arc_sim_step_ids(arc_sim *s, const int *d_ids, int n_ids, const double *d_targets, const float *d_actions,
                      void *stream);
 /* observe of the listed worlds (device ids) into device buffers whose row k
@@ -199,7 +200,7 @@ int arc_sim_observe_ids(const arc_sim *s, const int *d_ids, int n_ids, double *r
 /* on != 0: the warp-per-leg kernel runs one wave of resident CTAs that take
  * groups of 32 worlds from a device work queue, instead of one CTA per group */
 int arc_sim_set_work_queue(arc_sim *s, int on);
-/* Substep tiling of the warp-per-leg kernel: tile in 1 .. substeps - 1 runs
+/* Substep tiling of the FP32 warp-per-leg kernel: tile in 1 .. substeps - 1 runs
  * each control step as launches of `tile` substeps, the state going through
  * device memory between them (the same worlds bit for bit); 0 (the default)
  * or >= substeps: the whole control step in one launch, the state on chip

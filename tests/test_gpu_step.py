@@ -97,7 +97,7 @@ def test_reset_matches_oracle(fp64):
 
 
 @pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
-@pytest.mark.parametrize("kernel", [KERNEL_PLAIN, KERNEL_LEGS])
+@pytest.mark.parametrize("kernel", [KERNEL_PLAIN, KERNEL_LEGS, KERNEL_WARPS])
 def test_fp64_teacher_forced_vs_reference(kernel):
     ref, seeds, diffs, rng = diverse_states(N)
     g = Sim(N, fp64=True)
@@ -358,14 +358,15 @@ def _device_buffers(ids, targets):
     return d_ids, d_t
 
 
-@pytest.mark.parametrize("queue", [False, True])
-def test_subset_step_equals_batch_step(queue):
+@pytest.mark.parametrize("queue,fp64", [(False, False), (True, False), (False, True), (True, True)])
+def test_subset_step_equals_batch_step(queue, fp64):
     """Stepping a list of worlds gives, for those worlds, exactly what the
     whole-batch step gives (worlds never interact and run the same code),
-    and leaves the other worlds untouched; with or without the work queue."""
+    and leaves the other worlds untouched; with or without the work queue,
+    in FP32 and FP64."""
     n = 200
     seeds, diffs = seeds_diffs(n, 21)
-    a, b = Sim(n), Sim(n)
+    a, b = Sim(n, fp64=fp64), Sim(n, fp64=fp64)
     for s in (a, b):
         s.set_kernel(KERNEL_WARPS)
         s.reset(np.arange(n), seeds, diffs)
@@ -386,13 +387,14 @@ def test_subset_step_equals_batch_step(queue):
         assert np.array_equal(sa[rest], before[rest])
 
 
-def test_work_queue_matches_one_cta_per_group():
+@pytest.mark.parametrize("fp64", [False, True])
+def test_work_queue_matches_one_cta_per_group(fp64):
     """The persistent form (resident CTAs taking groups from a queue, reset
     by the last CTA) steps every world exactly as one CTA per group does,
-    launch after launch."""
+    launch after launch, in FP32 and FP64."""
     n = 70 * 32 + 5
     seeds, diffs = seeds_diffs(n, 22)
-    a, b = Sim(n), Sim(n)
+    a, b = Sim(n, fp64=fp64), Sim(n, fp64=fp64)
     for s in (a, b):
         s.set_kernel(KERNEL_WARPS)
         s.reset(np.arange(n), seeds, diffs)
@@ -498,6 +500,7 @@ def contact_lists(world_fn, n):
 
 @pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
 @pytest.mark.parametrize("fp64,kernel,cell", [(True, KERNEL_PLAIN, 0.4), (True, KERNEL_LEGS, 0.4),
+                                              (True, KERNEL_WARPS, 0.4), (True, KERNEL_WARPS, 0.05),
                                               (False, KERNEL_WARPS, 0.4), (False, KERNEL_WARPS, 0.05),
                                               (False, KERNEL_LEGS, 0.4)])
 def test_world_contact_list_matches_reference(fp64, kernel, cell):
