@@ -346,11 +346,9 @@ arc_sim* create_with_model(const ModelHost& model, int n, double dt, int substep
     s->fp64 = (flags & ARC_SIM_FP64) != 0;
     s->model = model;
     rebuild_models(s);
-    // the fastest form that steps the model: warp-per-leg (FP32 quadruped),
-    // leg-parallel (FP64 quadruped), plain (any model)
-    s->kernel = (flags & ARC_SIM_PLAIN) || !s->model.leaper ? ARC_KERNEL_PLAIN
-                : s->fp64                                 ? ARC_KERNEL_LEGS
-                                                          : ARC_KERNEL_WARPS;
+    // the fastest form that steps the model: warp-per-leg (the quadruped, in
+    // FP32 or FP64), plain (any model)
+    s->kernel = (flags & ARC_SIM_PLAIN) || !s->model.leaper ? ARC_KERNEL_PLAIN : ARC_KERNEL_WARPS;
     const int rs = real_size(s);
     s->off_sphere = s->model.nb * kBodyRec;
     s->off_joint = s->off_sphere + s->model.ns * kSphereRec;
