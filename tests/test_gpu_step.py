@@ -321,6 +321,20 @@ def test_observe_heights_terrain_at_match_oracle():
     # FP64 sample points on both sides; a libm ulp in the heading can move a
     # point across a cell boundary only on an exact tie
     assert mism <= 1e-4
+    # each mismatching sample lies at a cell edge: its point, recomputed here
+    # in FP64 as csrc/arc_sim.c:185-203 computes it (heading from the torso's
+    # forward axis), is within 1e-9 m of a column boundary of the 64 x 64,
+    # 0.4 m grid centred on the origin
+    st = g.get_state()
+    for w, k in zip(*np.nonzero(hg.reshape(n, len(offs)) != ho.reshape(n, len(offs)))):
+        qw, qx, qy, qz = st[w, 3:7]
+        yaw = np.arctan2(2.0 * (qx * qy + qw * qz), 1.0 - 2.0 * (qy * qy + qz * qz))
+        f, l = offs[k]
+        px = st[w, 0] + np.cos(yaw) * f - np.sin(yaw) * l
+        py = st[w, 1] + np.sin(yaw) * f + np.cos(yaw) * l
+        u = (np.array([px, py]) + 0.5 * 64 * 0.4) / 0.4
+        edge = np.abs(u - np.round(u)).min() * 0.4
+        assert edge <= 1e-9, (w, k, edge)
     ids = rng.integers(0, n, 500).astype(np.int32)
     xy = rng.uniform(-14, 14, (500, 2))
     assert np.array_equal(g.terrain_at(ids, xy), o.terrain_at(ids, xy))
