@@ -1297,6 +1297,8 @@ int arc_sim_set_substep_tile(arc_sim* s, int tile)
 {
     if (tile < 0)
         return fail(s, ARC_ERR_ARG, "arc_sim_set_substep_tile: tile < 0");
+    if (s->fp64 && tile > 0 && tile < s->substeps)
+        return fail(s, ARC_ERR_UNSUPPORTED, "arc_sim_set_substep_tile: substep tiles are FP32 only");
     if (tile > 0 && tile < s->substeps && !s->tile_q &&
         check(s, cudaMalloc((void**)&s->tile_q, sizeof(float) * 13 * 4 * (size_t)std::max(s->n, 1)),
               "cudaMalloc(tile quaternions)"))

@@ -204,7 +204,7 @@ int arc_sim_set_work_queue(arc_sim *s, int on);
  * each control step as launches of `tile` substeps, the state going through
  * device memory between them (the same worlds bit for bit); 0 (the default)
  * or >= substeps: the whole control step in one launch, the state on chip
- * throughout. */
+ * throughout. FP64 sims refuse tiles (ARC_ERR_UNSUPPORTED). */
 int arc_sim_set_substep_tile(arc_sim *s, int tile);
 /* on != 0: the step kernels keep each world's contact list of the last
  * substep on the device (128 records a world: 4 KB in FP32, 8 KB in FP64),

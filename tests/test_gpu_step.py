@@ -401,6 +401,43 @@ def test_subset_step_equals_batch_step(queue, fp64):
         assert np.array_equal(sa[rest], before[rest])
 
 
+@pytest.mark.parametrize("tile,queue", [(1, True), (2, False), (5, True), (7, True), (10, False)])
+def test_substep_tiles_equal_one_launch(tile, queue):
+    """The FP32 warp-per-leg control step as launches of `tile` substeps (7
+    leaves a short last tile), the state going through device memory between
+    them, steps every world bit for bit as one launch does, with the last
+    substep's contact list recorded in the last tile; FP64 sims refuse tiles."""
+    import ctypes
+    from oracle.oracle import World
+
+    n = 300
+    seeds, diffs = seeds_diffs(n, 23)
+    a, b = Sim(n), Sim(n)
+    for s in (a, b):
+        s.set_kernel(KERNEL_WARPS)
+        s.set_work_queue(queue)
+        s._lib.arc_sim_world.restype = ctypes.POINTER(World)
+        s._lib.arc_sim_world.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        s._lib.arc_sim_world(s.ptr, 0)  # the first call turns contact recording on
+        s.reset(np.arange(n), seeds, diffs)
+    a.set_substep_tile(tile)
+    rng = np.random.default_rng(5)
+    for _ in range(4):
+        t = a.default_angles + 0.6 * rng.uniform(-1, 1, (n, 12))
+        a.step(t)
+        b.step(t)
+        assert np.array_equal(a.get_state(), b.get_state())
+    la = contact_lists(lambda i: a._lib.arc_sim_world(a.ptr, i).contents, n)
+    lb = contact_lists(lambda i: b._lib.arc_sim_world(b.ptr, i).contents, n)
+    assert sum(len(x[0]) for x in la) > n // 2  # the lists are not empty
+    for (ba, va), (bb, vb) in zip(la, lb):
+        assert np.array_equal(ba, bb) and np.array_equal(va, vb)
+    f = Sim(8, fp64=True)
+    with pytest.raises(RuntimeError):
+        f.set_substep_tile(5)
+    f.set_substep_tile(0)  # the whole step stays allowed
+
+
 @pytest.mark.parametrize("fp64", [False, True])
 def test_work_queue_matches_one_cta_per_group(fp64):
     """The persistent form (resident CTAs taking groups from a queue, reset
