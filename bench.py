@@ -522,6 +522,10 @@ def run_ours(args) -> dict | None:
         "plain_kernel": plain,
         "speedup_vs_plain": round(plain["ms_per_step"] / (ms_total / K), 2) if plain else None,
         "speedup_vs_plain_step_kernel": round(plain["step_kernel_ms"] / step_kernel_ms, 2) if plain else None,
+        "speedup_vs_plain_meaning": ("speedup_vs_plain: the whole control step, the FP32 MLP policy and the task "
+                                     "kernels included (the same in both loops); speedup_vs_plain_step_kernel: "
+                                     "the batched step kernel alone against the plain per-world kernel, both on "
+                                     "the states after their loops, each in its faster step order"),
         "control_step_ms_without_policy": round(control_step_ms, 4),
         "roofline": {"bound": "fp32", "achieved": round(achieved / 1e12, 3),
                      "peak": round(peak.value / 1e12, 3), "unit": "TFLOP/s",
