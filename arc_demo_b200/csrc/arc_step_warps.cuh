@@ -32,10 +32,11 @@
 // starts from).
 //
 // This header holds the step of one group, `step_group`, which the control
-// step kernel of arc_task.cu runs, alone (the physics step) or followed by
-// the task layer on the group's worlds (the fused control step). Everything
-// here has internal linkage: the operation lists live in that translation
-// unit's constant bank.
+// step kernel of arc_task.cu runs in FP32, alone (the physics step) or
+// followed by the task layer on the group's worlds (the fused control step),
+// and arc_step_warps64.cu's kernel runs in FP64 (ARC_WARPS_FP64). Everything
+// here has internal linkage: each including translation unit has its own
+// copy, its operation lists in its own constant bank.
 #pragma once
 
 #include "arc_kernels.cuh"
